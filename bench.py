@@ -1,0 +1,476 @@
+"""Throughput benchmark of the B200 force evaluation + leapfrog step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Default workload (``bh_collision_1m``): plain Barnes-Hut on two Plummer
+spheres of 500k particles (a = 1, M = 1/2 each, centres 10 apart on x,
+relative velocity 0.3 on y), eps = 0.01, theta = 0.7, leapfrog KDK at
+dt = 1e-3 — one step = one kick-drift-force-kick of all N particles.
+Metric: particle-steps/s (N x steps / device time).
+
+Other workloads (parity configs, selectable): ``allpairs_plummer_16k``,
+``allpairs_precision_262k``.
+
+Timing: W untimed warm-up steps; then K steps, each a 1-step device-resident
+advance bracketed by CUDA events recorded by the library on its own stream;
+a 256 MiB buffer is written between timed steps to flush the 126 MB L2.
+Under torchrun (N > 1) every rank advances its own replica (no data-path
+collective: the path is single-GPU; "replicas only"), the step time is the
+max over ranks and `value` sums the ranks' particle-steps.
+
+`e2e`: the same metric through the reference-facing plugin call
+n_body_sim_pro_barnes_hut_compute_acceleration_cuda(view, ...) on pinned host
+arrays inside a host leapfrog loop: every step copies positions + masses to
+the device and accelerations back.
+
+`cpu_baseline` / `--impl reference`: the reference engine compiled from its
+own sources (oracle/_ref) timed on this host's cores on the same initial
+conditions (a bounded sample of steps).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "bh_collision_1m": dict(n=1_000_000, algorithm="barnes_hut", theta=0.7, eps=0.01, dt=1e-3,
+                            ic="collision", steps=10, order=1),
+    "allpairs_plummer_16k": dict(n=16384, algorithm="all_pairs", eps=0.01, dt=1e-3,
+                                 ic="plummer", steps=3),
+    "allpairs_precision_262k": dict(n=262144, algorithm="all_pairs", eps=1e-3, dt=1e-4,
+                                    ic="uniform_log_mass", steps=3),
+}
+
+FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
+FLOPS_PAIR = 20          # standard convention per softened pair interaction
+FLOPS_QUAD = 58          # monopole + trace-free quadrupole per accepted cell
+
+
+# ---------------------------------------------------------------------------
+# initial conditions (numpy; statistically the reference's Plummer preset,
+# src/c/generation/presets.c:144-202, not its RNG stream)
+# ---------------------------------------------------------------------------
+
+def plummer_block(rng, n, a, mass, centre):
+    u = 1.0 - rng.random(n)
+    r = a / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pos = r[:, None] * d + np.asarray(centre)
+    sigma = np.sqrt(mass / (6.0 * np.sqrt(a * a + r * r)))
+    vel = rng.standard_normal((n, 3)) * sigma[:, None]
+    vel -= vel.mean(axis=0)
+    return pos, vel, np.full(n, mass / n)
+
+
+def initial_conditions(kind, n, seed=42):
+    rng = np.random.default_rng(seed)
+    if kind == "plummer":
+        return plummer_block(rng, n, 1.0, 1.0, (0.0, 0.0, 0.0))
+    if kind == "collision":
+        h = n // 2
+        p1, v1, m1 = plummer_block(rng, h, 1.0, 0.5, (-5.0, 0.0, 0.0))
+        p2, v2, m2 = plummer_block(rng, n - h, 1.0, 0.5, (5.0, 0.0, 0.0))
+        v1[:, 1] -= 0.15
+        v2[:, 1] += 0.15
+        return np.vstack([p1, p2]), np.vstack([v1, v2]), np.concatenate([m1, m2])
+    if kind == "uniform_log_mass":
+        pos = rng.random((n, 3))
+        m = 10.0 ** rng.uniform(-3.0, 0.0, n)
+        return pos, np.zeros((n, 3)), m / m.sum()
+    raise ValueError(kind)
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, f[4:8]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def fp32_peak_tflops(sm_count, mhz):
+    return sm_count * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier_sync(world):
+    import torch
+
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(value, world):
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline (the reference engine compiled from its sources)
+# ---------------------------------------------------------------------------
+
+def reference_steps(wl, pos, vel, mass, steps, threads):
+    """Time `steps` leapfrog steps of the reference engine on this host:
+    n_body_sim_pro_integrator_advance with its Barnes-Hut (or OpenMP AVX all-pairs)
+    force function.  Returns seconds per step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if not O.ref_available():
+        raise RuntimeError("oracle/_ref not built")
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    R = O.ref()
+    p = O.Particles.zeros(mass.shape[0])
+    p.x[:], p.y[:], p.z[:] = pos.T
+    p.vx[:], p.vy[:], p.vz[:] = vel.T
+    p.m[:] = mass
+    g = O.Gravity()
+    R.n_body_sim_pro_gravity_init(C.byref(g), 1.0, wl["eps"])
+    err = O.Error()
+    v = p.view()
+    ctx = None
+    if wl["algorithm"] == "barnes_hut":
+        ctx = R.n_body_sim_pro_barnes_hut_tree_create(C.byref(err))
+        R.n_body_sim_pro_barnes_hut_tree_set_theta(ctx, wl["theta"])
+        fn = R.n_body_sim_pro_barnes_hut_compute_acceleration
+    else:
+        fn = R.n_body_sim_pro_gravity_compute_acceleration_openmp_avx512
+    force = C.cast(fn, C.c_void_p)
+    if fn(C.byref(v), C.byref(g), ctx, C.byref(err)) != 0:  # initial forces
+        raise RuntimeError(err.message)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        rc = R.n_body_sim_pro_integrator_advance(C.byref(v), C.byref(g), 1, wl["dt"], force, ctx,
+                                                 C.byref(err))
+        if rc != 0:
+            raise RuntimeError(err.message)
+    dt = (time.perf_counter() - t0) / steps
+    if ctx is not None:
+        R.n_body_sim_pro_barnes_hut_tree_destroy(ctx)
+    return dt
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, wl, world, rank, local):
+    import torch
+
+    import n_body_sim_pro_b200 as nb
+
+    n = wl["n"]
+    pos, vel, mass = initial_conditions(wl["ic"], n, seed=42 + rank)
+    g = nb.gravity_init(1.0, wl["eps"])
+    algo = nb.Algorithm.BARNES_HUT if wl["algorithm"] == "barnes_hut" else nb.Algorithm.ALL_PAIRS
+    ctx = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1))
+    system = nb.ParticleSystem.from_arrays(pos, vel, mass)
+    ctx.upload(system)
+    ctx.compute_acceleration(g, algo)
+    q0, pe0 = ctx.diagnostics(g, potential=True) if n <= 2_000_000 else (ctx.diagnostics(g), None)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        ctx.advance(g, wl["dt"], 1, algo)
+    barrier_sync(world)
+    launches0 = nb.kernel_launches()
+    step_ms, walk_ms, stats_acc = [], [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ctx.advance(g, wl["dt"], 1, algo)
+            t = ctx.timings()
+            step_ms.append(t["total_ms"])
+            walk_ms.append(t["walk_ms"])
+            stats_acc.append(ctx.stats())
+    launches = nb.kernel_launches() - launches0
+    barrier_sync(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+
+    # accuracy of the final state: forces vs the FP64 device oracle on 4096 targets
+    ctx.compute_acceleration(g, algo)
+    final = nb.ParticleSystem.zeros(n)
+    ctx.download(final)
+    targets = np.random.default_rng(7).choice(n, min(4096, n), replace=False)
+    ref = ctx.reference_acceleration(g, targets)
+    acc = final.acc()[targets]
+    rms = float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
+    max_rel = float(np.max(np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+    drift = None
+    if pe0 is not None:
+        q1, pe1 = ctx.diagnostics(g, potential=True)
+        drift = float(abs((q1[0] + pe1) - (q0[0] + pe0)) / abs(q0[0] + pe0))
+
+    # dominant kernel roofline
+    peaks, peak_kind = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    clk = clocks.summary()
+    mhz_load = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
+    if wl["algorithm"] == "barnes_hut":
+        approx = np.mean([s["accepted_approximations"] for s in stats_acc])
+        exact = np.mean([s["exact_interactions"] for s in stats_acc])
+        flops = FLOPS_PAIR * exact + (FLOPS_PAIR if wl.get("order", 1) == 1 else FLOPS_QUAD) * approx
+        kernel_ms = float(np.mean(walk_ms))
+        kernel = "walk_kernel"
+        interactions = approx + exact
+    else:
+        flops = FLOPS_PAIR * float(n) * float(n)
+        kernel_ms = float(np.mean(walk_ms)) if np.mean(walk_ms) > 0 else total_ms / args.steps
+        kernel = "allpairs_force_kernel"
+        interactions = float(n) * n
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": kernel, "achieved": round(achieved, 3),
+                "peak": round(peak_max, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak_max, 4),
+                "frac_at_load_clock": round(achieved / fp32_peak_tflops(sm_count, mhz_load), 4),
+                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x {peaks.get('sm_max_mhz', 1965.0)} MHz "
+                             f"(sm_max_mhz of {peak_kind} MEASURED_PEAKS.json)",
+                "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4),
+                "traffic": None}
+
+    # e2e through the plugin call on pinned host arrays
+    e2e = None
+    if rank == 0 or world > 1:
+        e2e = run_e2e(nb, wl, pos, vel, mass, min(args.steps, 5), algo, ctx)
+
+    ctx.close()
+    value = world * n * args.steps / (total_ms * 1e-3)
+    return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
+                roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
+                interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
+                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms))
+
+
+def ctx_timings_summary(step_ms, walk_ms):
+    return {"step_ms_mean": round(float(np.mean(step_ms)), 4),
+            "walk_ms_mean": round(float(np.mean(walk_ms)), 4)}
+
+
+def run_e2e(nb, wl, pos, vel, mass, steps, algo, ctx):
+    import torch
+
+    n = wl["n"]
+    alloc = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    s = nb.ParticleSystem.zeros(n, allocator=alloc)
+    s.x[:], s.y[:], s.z[:] = pos.T
+    s.vx[:], s.vy[:], s.vz[:] = vel.T
+    s.m[:] = mass
+    g = nb.gravity_init(1.0, wl["eps"])
+    force = (nb.n_body_sim_pro_barnes_hut_compute_acceleration_cuda if algo == nb.Algorithm.BARNES_HUT
+             else nb.n_body_sim_pro_gravity_compute_acceleration_cuda)
+    c2 = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1))
+    force(s, g, c2)
+    h, dt = 0.5 * wl["dt"], wl["dt"]
+    for _ in range(2):  # warm-up of the plugin path
+        force(s, g, c2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        # integrator.c:47-85 on the host, force on the device
+        s.vx += s.ax * h
+        s.vy += s.ay * h
+        s.vz += s.az * h
+        s.x += s.vx * dt
+        s.y += s.vy * dt
+        s.z += s.vz * dt
+        force(s, g, c2)
+        s.vx += s.ax * h
+        s.vy += s.ay * h
+        s.vz += s.az * h
+    elapsed = time.perf_counter() - t0
+    c2.close()
+    return {"value": n * steps / elapsed, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n,
+            "steps": steps, "path": "host leapfrog + plugin force call, pinned host arrays",
+            "timer": "host wall clock"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="bh_collision_1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    wl = WORKLOADS[args.workload]
+    if args.steps is None:
+        args.steps = wl["steps"]
+    args.warmup = max(args.warmup, 3)
+    metric = "particle-steps/s"
+    config = {"workload": args.workload, "particles": wl["n"], "algorithm": wl["algorithm"],
+              "theta": wl.get("theta"), "softening": wl["eps"], "timestep": wl["dt"],
+              "integrator": "leapfrog_kdk", "multipole_order": wl.get("order"),
+              "initial_conditions": wl["ic"], "l2": "256 MiB write between timed steps",
+              "parallelism": f"replicas x{args.gpus}"}
+
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        pos, vel, mass = initial_conditions(wl["ic"], wl["n"], seed=42)
+        steps = max(1, min(args.steps, 3))
+        for _ in range(1):  # one untimed warm-up step
+            reference_steps(wl, pos, vel, mass, 1, threads)
+        sec = reference_steps(wl, pos, vel, mass, steps, threads)
+        v = wl["n"] / sec
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": metric,
+                "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": sec * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": metric, "cores": threads, "kind": "reference",
+                                 "sample": f"{steps} leapfrog steps of the full {wl['n']}-particle "
+                                           f"system (reference engine, OMP_NUM_THREADS={threads}, "
+                                           f"{cpu_model()})"},
+                "e2e": {"value": v, "unit": metric, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    world, rank, local = dist_setup(args.gpus)
+    r = run_ours(args, wl, world, rank, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            pos, vel, mass = initial_conditions(wl["ic"], wl["n"], seed=42)
+            threads = os.cpu_count() or 1
+            sec = reference_steps(wl, pos, vel, mass, 1, threads)
+            cpu = {"value": wl["n"] / sec, "unit": metric, "cores": threads, "kind": "reference",
+                   "sample": f"1 leapfrog step of the full {wl['n']}-particle system, reference "
+                             f"engine (oracle/_ref) with OMP_NUM_THREADS={threads} on {cpu_model()}"}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": metric, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {"metric": metric, "value": r["value"], "unit": metric, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32-force/f64-state",
+                "data": "synthetic", "config": config,
+                "accuracy": {"rms_rel_force_err": r["rms"], "max_rel_force_err": r["max_rel"],
+                             "energy_drift": r["drift"], "oracle": "FP64 device direct sum, "
+                             "4096 seeded targets, final state"},
+                "interactions_per_s": r["interactions_per_s"], "stats": r["stats"],
+                "phase_ms": r["timings"], "roofline": r["roofline"], "cpu_baseline": cpu,
+                "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"]}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

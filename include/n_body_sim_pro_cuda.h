@@ -1,0 +1,305 @@
+/*
+ * n_body_sim_pro_cuda.h — B200 (sm_100a) force evaluation and time step for the
+ * n_body_sim_pro C engine, exposed as a C ABI.
+ *
+ * The library adds two algorithms behind the engine's existing force-kernel
+ * plugin type
+ *
+ *   typedef NBodySimProStatus (*NBodySimProForceFunction)(
+ *       const NBodySimProParticleSystemView*, const NBodySimProGravity*,
+ *       void* context, NBodySimProError*);      (physics/integrator.h:47-49)
+ *
+ *   cuda             n_body_sim_pro_gravity_compute_acceleration_cuda
+ *   barnes_hut_cuda  n_body_sim_pro_barnes_hut_compute_acceleration_cuda
+ *
+ * plus a device-resident stepping API (upload once, advance many fused
+ * kick-drift-kick steps on the GPU, download) for throughput.
+ *
+ * Conventions (all follow the reference engine):
+ *   - every function returns NBodySimProStatus and fills the optional
+ *     NBodySimProError* (NULL allowed) like n_body_sim_pro_error_set
+ *     (src/c/core/status.c:29);
+ *   - NULL view / gravity -> N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT
+ *     (src/c/physics/gravity.c:19-23);
+ *   - accelerations are OVERWRITTEN, never accumulated (physics/gravity.h:43-44);
+ *   - no CPU fallback: without a usable CUDA device the functions return
+ *     N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM.
+ *
+ * Numerics: forces in FP32 on positions relative to the FP64 centre of mass,
+ * with compensated (TwoSum) accumulation; positions, velocities, the drift,
+ * the kick and all diagnostics in FP64.
+ *
+ * The reference's own types are re-declared here, layout-identical, for
+ * callers that do not have the engine's headers.  When the engine's headers
+ * are included BEFORE this one, their include guards suppress these copies.
+ */
+#ifndef N_BODY_SIM_PRO_CUDA_H
+#define N_BODY_SIM_PRO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define N_BODY_SIM_PRO_CUDA_API
+#else
+#define N_BODY_SIM_PRO_CUDA_API __attribute__((visibility("default")))
+#endif
+
+/* ---- reference types (layout-identical copies) ---------------------------- */
+
+#ifndef N_BODY_SIM_PRO_CORE_STATUS_H
+/* include/n_body_sim_pro/core/status.h:18-35 */
+typedef enum NBodySimProStatus {
+    N_BODY_SIM_PRO_STATUS_OK = 0,
+    N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+    N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY,
+    N_BODY_SIM_PRO_STATUS_INVALID_STATE,
+    N_BODY_SIM_PRO_STATUS_NOT_IMPLEMENTED,
+    N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM,
+    N_BODY_SIM_PRO_STATUS_OVERFLOW,
+    N_BODY_SIM_PRO_STATUS_IO_ERROR,
+    N_BODY_SIM_PRO_STATUS_INSUFFICIENT_MEMORY
+} NBodySimProStatus;
+
+typedef struct NBodySimProError {
+    NBodySimProStatus status;
+    const char* source_file;
+    int source_line;
+    char message[256];
+} NBodySimProError;
+#endif
+
+#ifndef N_BODY_SIM_PRO_CORE_PARTICLE_SYSTEM_H
+/* include/n_body_sim_pro/core/particle_system.h:38-50 */
+typedef struct NBodySimProParticleSystemView {
+    size_t particle_count;
+    double* positions_x;
+    double* positions_y;
+    double* positions_z;
+    double* velocities_x;
+    double* velocities_y;
+    double* velocities_z;
+    double* accelerations_x;
+    double* accelerations_y;
+    double* accelerations_z;
+    double* masses;
+} NBodySimProParticleSystemView;
+#endif
+
+#ifndef N_BODY_SIM_PRO_PHYSICS_GRAVITY_H
+/* include/n_body_sim_pro/physics/gravity.h:25-29 */
+typedef struct NBodySimProGravity {
+    double gravitational_constant;
+    double softening_length;
+    double softening_squared;
+} NBodySimProGravity;
+#endif
+
+#ifndef N_BODY_SIM_PRO_PHYSICS_INTEGRATOR_H
+/* include/n_body_sim_pro/physics/integrator.h:31-35 */
+typedef enum NBodySimProIntegratorType {
+    N_BODY_SIM_PRO_INTEGRATOR_EULER,
+    N_BODY_SIM_PRO_INTEGRATOR_LEAPFROG,
+    N_BODY_SIM_PRO_INTEGRATOR_VELOCITY_VERLET
+} NBodySimProIntegratorType;
+#endif
+
+#ifndef N_BODY_SIM_PRO_BARNES_HUT_BARNES_HUT_H
+/* include/n_body_sim_pro/barnes_hut/barnes_hut.h:31-40 */
+typedef struct NBodySimProBarnesHutStats {
+    size_t node_count;
+    size_t leaf_count;
+    size_t internal_node_count;
+    size_t accepted_approximations;
+    size_t exact_interactions;
+    size_t maximum_depth;
+    double build_time_seconds;
+    double evaluation_time_seconds;
+} NBodySimProBarnesHutStats;
+#endif
+
+#ifndef N_BODY_SIM_PRO_DIAGNOSTICS_NUMERICS_H
+/* include/n_body_sim_pro/diagnostics/numerics.h:22-34 */
+typedef struct NBodySimProDiagnosticsQuantities {
+    double kinetic_energy;
+    double total_mass;
+    double total_momentum_x;
+    double total_momentum_y;
+    double total_momentum_z;
+    double total_angular_momentum_x;
+    double total_angular_momentum_y;
+    double total_angular_momentum_z;
+    double center_of_mass_x;
+    double center_of_mass_y;
+    double center_of_mass_z;
+} NBodySimProDiagnosticsQuantities;
+#endif
+
+/* ---- context ----------------------------------------------------------------- */
+
+/*
+ * Algorithm state for the CUDA force functions: device buffers, the CUDA
+ * stream, Barnes-Hut parameters, the all-pairs tile autotune cache and the
+ * statistics of the last evaluation.  Plays the role of the reference's
+ * NBodySimProBarnesHutTree context (barnes_hut/barnes_hut.h:28-43) for both
+ * CUDA algorithms.  One context must not be used from two host threads at once.
+ */
+typedef struct NBodySimProCudaContext NBodySimProCudaContext;
+
+typedef enum NBodySimProCudaAlgorithm {
+    N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS = 0,
+    N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT = 1
+} NBodySimProCudaAlgorithm;
+
+/* Per-phase device time of the most recent evaluation, milliseconds (CUDA events). */
+typedef struct NBodySimProCudaTimings {
+    double bounds_ms;      /* bbox + centre-of-mass reduction */
+    double keys_ms;        /* Morton keys */
+    double sort_ms;        /* radix sort of keys + permutation */
+    double build_ms;       /* gather + octree build */
+    double moments_ms;     /* monopole / quadrupole pass */
+    double walk_ms;        /* tree walk (Barnes-Hut) or all-pairs tiles */
+    double integrate_ms;   /* kick / drift / scatter epilogue */
+    double total_ms;
+} NBodySimProCudaTimings;
+
+/* Replaces n_body_sim_pro_barnes_hut_tree_create (barnes_hut/barnes_hut.h:43).
+ * Selects the current CUDA device; NULL + UNSUPPORTED_PLATFORM when none. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProCudaContext* n_body_sim_pro_cuda_context_create(
+    NBodySimProError* error);
+
+/* Replaces n_body_sim_pro_barnes_hut_tree_destroy (barnes_hut/barnes_hut.h:46). NULL-safe. */
+N_BODY_SIM_PRO_CUDA_API void n_body_sim_pro_cuda_context_destroy(NBodySimProCudaContext* context);
+
+/* Replace n_body_sim_pro_barnes_hut_tree_set_theta / _theta (barnes_hut/barnes_hut.h:49-50).
+ * Default 0.7 (src/c/barnes_hut/barnes_hut.c:28). */
+N_BODY_SIM_PRO_CUDA_API void n_body_sim_pro_cuda_context_set_theta(NBodySimProCudaContext* context,
+                                                                   double theta);
+N_BODY_SIM_PRO_CUDA_API double n_body_sim_pro_cuda_context_theta(
+    const NBodySimProCudaContext* context);
+
+/* Multipole order of accepted cells: 1 = monopole (the reference's
+ * barnes_hut.c:600-612), 2 = monopole + trace-free quadrupole (default 1). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_multipole_order(
+    NBodySimProCudaContext* context, int order, NBodySimProError* error);
+
+/* Largest particle count of a Barnes-Hut leaf bucket, 1..64 (default 16). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_capacity(
+    NBodySimProCudaContext* context, int capacity, NBodySimProError* error);
+
+/* Replaces n_body_sim_pro_barnes_hut_tree_stats (barnes_hut/barnes_hut.h:116-117):
+ * 0 on success, non-zero when an argument is NULL. */
+N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_stats(
+    const NBodySimProCudaContext* context, NBodySimProBarnesHutStats* stats);
+
+/* Device-event phase timings of the last evaluation or advance. 0 on success. */
+N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_timings(
+    const NBodySimProCudaContext* context, NBodySimProCudaTimings* timings);
+
+/* ---- force functions (NBodySimProForceFunction) -------------------------------- */
+
+/*
+ * `cuda` algorithm: exact softened all-pairs sum (j == i excluded) on the GPU,
+ * semantics of n_body_sim_pro_gravity_compute_acceleration_reference
+ * (physics/gravity.h:46-59, src/c/physics/gravity.c:15-70).  `context` is an
+ * NBodySimProCudaContext*, or NULL for a lazily created process-wide context.
+ * Copies positions/masses to the device and accelerations back every call.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_gravity_compute_acceleration_cuda(
+    const NBodySimProParticleSystemView* view, const NBodySimProGravity* gravity, void* context,
+    NBodySimProError* error);
+
+/*
+ * `barnes_hut_cuda` algorithm: GPU Barnes-Hut with the reference's opening
+ * criterion (2h)^2 < theta^2 d^2 to the cell centre of mass
+ * (src/c/barnes_hut/barnes_hut.c:596-599), replacing
+ * n_body_sim_pro_barnes_hut_compute_acceleration (barnes_hut/barnes_hut.h:61-63).
+ * `context` must be an NBodySimProCudaContext* (NULL: the process-wide one).
+ * Empty system -> INVALID_ARGUMENT (barnes_hut.c:446-451).
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_barnes_hut_compute_acceleration_cuda(
+    const NBodySimProParticleSystemView* view, const NBodySimProGravity* gravity, void* context,
+    NBodySimProError* error);
+
+/* ---- device-resident stepping ---------------------------------------------------- */
+
+/* Copy positions, velocities, masses and accelerations of `view` to the device. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_upload(
+    NBodySimProCudaContext* context, const NBodySimProParticleSystemView* view,
+    NBodySimProError* error);
+
+/* Copy the device state back into `view` (same particle count as uploaded). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_download(
+    NBodySimProCudaContext* context, const NBodySimProParticleSystemView* view,
+    NBodySimProError* error);
+
+/* Recompute the accelerations of the resident state (the "initial forces"
+ * step the integrators require, physics/integrator.h:26-28). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_compute_acceleration(
+    NBodySimProCudaContext* context, const NBodySimProGravity* gravity,
+    NBodySimProCudaAlgorithm algorithm, NBodySimProError* error);
+
+/*
+ * `steps` timesteps of n_body_sim_pro_integrator_advance semantics
+ * (physics/integrator.h:58-64, src/c/physics/integrator.c:141-172) on the
+ * resident state, the force pass fused with the kick/drift epilogues.
+ * Leapfrog / velocity Verlet need valid accelerations first (upload them or
+ * call n_body_sim_pro_cuda_compute_acceleration).  timestep <= 0 -> INVALID_ARGUMENT.
+ * Returns when the work is enqueued AND finished (it synchronises once).
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_advance(
+    NBodySimProCudaContext* context, const NBodySimProGravity* gravity,
+    NBodySimProIntegratorType integrator, double timestep, int steps,
+    NBodySimProCudaAlgorithm algorithm, NBodySimProError* error);
+
+/*
+ * Conservation diagnostics of the resident state in FP64 on the device:
+ * n_body_sim_pro_diagnostics_compute_global (src/c/diagnostics/numerics.c:5-81)
+ * and, when `potential_energy` is non-NULL, the O(N^2) softened potential
+ * energy (numerics.c:83-116).
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_diagnostics(
+    NBodySimProCudaContext* context, const NBodySimProGravity* gravity,
+    NBodySimProDiagnosticsQuantities* quantities, double* potential_energy,
+    NBodySimProError* error);
+
+/*
+ * FP64 exact accelerations of `count` resident target particles (indices in
+ * `targets`) over all resident sources, with the pair arithmetic of
+ * src/c/physics/gravity.c:46-61: the precision-report oracle on the device.
+ * out[3*t + c]; host pointers.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_reference_acceleration(
+    NBodySimProCudaContext* context, const NBodySimProGravity* gravity, const int64_t* targets,
+    size_t count, double* out, NBodySimProError* error);
+
+/*
+ * Morton order of the resident positions as the Barnes-Hut build computes it:
+ * keys_sorted[i] and permutation[i] (original index) for sorted position i,
+ * root[4] = centre xyz and half size.  Bit-exact with the reference's
+ * morton_axis_code / morton_key / radix_sort_morton_keys
+ * (src/c/barnes_hut/barnes_hut.c:286-339, :453-483).  Any argument may be NULL.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_morton_order(
+    NBodySimProCudaContext* context, uint64_t* keys_sorted, uint64_t* permutation, double* root,
+    NBodySimProError* error);
+
+/* Wait for all work queued on the context's stream. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_synchronize(
+    NBodySimProCudaContext* context, NBodySimProError* error);
+
+/* Name of the library's GPU architecture target ("sm_100a"). */
+N_BODY_SIM_PRO_CUDA_API const char* n_body_sim_pro_cuda_architecture(void);
+
+/* Number of CUDA kernels this process has launched through the library. */
+N_BODY_SIM_PRO_CUDA_API unsigned long long n_body_sim_pro_cuda_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N_BODY_SIM_PRO_CUDA_H */

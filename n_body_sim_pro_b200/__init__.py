@@ -1,0 +1,403 @@
+"""n_body_sim_pro_b200 — B200-native force evaluation and time step.
+
+Python mirror of the C ABI in include/n_body_sim_pro_cuda.h (the library
+libn_body_sim_pro_cuda.so is built in-tree by ``n_body_sim_pro_b200.build``).
+Names follow the reference engine's C API:
+
+    n_body_sim_pro_gravity_compute_acceleration_cuda(view, gravity, context)
+    n_body_sim_pro_barnes_hut_compute_acceleration_cuda(view, gravity, context)
+
+are the two new ``NBodySimProForceFunction`` algorithms (``cuda`` and
+``barnes_hut_cuda``); :class:`CudaContext` wraps ``NBodySimProCudaContext``
+(the device-resident state, stepping and diagnostics).
+
+There is no CPU fallback: importing works without a GPU, but every compute
+call raises :class:`CudaError` with ``UNSUPPORTED_PLATFORM`` when no B200 is
+present, and :func:`library` raises if the shared library was not built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from enum import IntEnum
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libn_body_sim_pro_cuda.so")
+
+
+class Status(IntEnum):
+    """NBodySimProStatus (include/n_body_sim_pro/core/status.h:18-28)."""
+
+    OK = 0
+    INVALID_ARGUMENT = 1
+    OUT_OF_MEMORY = 2
+    INVALID_STATE = 3
+    NOT_IMPLEMENTED = 4
+    UNSUPPORTED_PLATFORM = 5
+    OVERFLOW = 6
+    IO_ERROR = 7
+    INSUFFICIENT_MEMORY = 8
+
+
+class Integrator(IntEnum):
+    """NBodySimProIntegratorType (include/n_body_sim_pro/physics/integrator.h:31-35)."""
+
+    EULER = 0
+    LEAPFROG = 1
+    VELOCITY_VERLET = 2
+
+
+class Algorithm(IntEnum):
+    ALL_PAIRS = 0
+    BARNES_HUT = 1
+
+
+class View(C.Structure):
+    """NBodySimProParticleSystemView (include/n_body_sim_pro/core/particle_system.h:38-50)."""
+
+    _fields_ = [("particle_count", C.c_size_t)] + [
+        (name, C.POINTER(C.c_double))
+        for name in ("positions_x", "positions_y", "positions_z", "velocities_x",
+                     "velocities_y", "velocities_z", "accelerations_x", "accelerations_y",
+                     "accelerations_z", "masses")
+    ]
+
+
+class Gravity(C.Structure):
+    """NBodySimProGravity (include/n_body_sim_pro/physics/gravity.h:25-29)."""
+
+    _fields_ = [("gravitational_constant", C.c_double), ("softening_length", C.c_double),
+                ("softening_squared", C.c_double)]
+
+
+def gravity_init(gravitational_constant: float, softening_length: float) -> Gravity:
+    """n_body_sim_pro_gravity_init (src/c/physics/gravity.c:5-13)."""
+    return Gravity(gravitational_constant, softening_length, softening_length * softening_length)
+
+
+class Error(C.Structure):
+    """NBodySimProError (include/n_body_sim_pro/core/status.h:30-35)."""
+
+    _fields_ = [("status", C.c_int), ("source_file", C.c_char_p), ("source_line", C.c_int),
+                ("message", C.c_char * 256)]
+
+
+class BarnesHutStats(C.Structure):
+    """NBodySimProBarnesHutStats (include/n_body_sim_pro/barnes_hut/barnes_hut.h:31-40)."""
+
+    _fields_ = [(n, C.c_size_t) for n in ("node_count", "leaf_count", "internal_node_count",
+                                          "accepted_approximations", "exact_interactions",
+                                          "maximum_depth")] + [
+        ("build_time_seconds", C.c_double), ("evaluation_time_seconds", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class DiagnosticsQuantities(C.Structure):
+    """NBodySimProDiagnosticsQuantities (include/n_body_sim_pro/diagnostics/numerics.h:22-34)."""
+
+    _fields_ = [(n, C.c_double) for n in (
+        "kinetic_energy", "total_mass", "total_momentum_x", "total_momentum_y",
+        "total_momentum_z", "total_angular_momentum_x", "total_angular_momentum_y",
+        "total_angular_momentum_z", "center_of_mass_x", "center_of_mass_y", "center_of_mass_z")]
+
+    def as_array(self) -> np.ndarray:
+        return np.array([getattr(self, f) for f, _ in self._fields_], dtype=np.float64)
+
+
+class Timings(C.Structure):
+    """NBodySimProCudaTimings: per-phase device milliseconds of the last call."""
+
+    _fields_ = [(n, C.c_double) for n in ("bounds_ms", "keys_ms", "sort_ms", "build_ms",
+                                          "moments_ms", "walk_ms", "integrate_ms", "total_ms")]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class CudaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{Status(status).name}: {message}")
+        self.status = Status(status)
+
+
+EXPORTS = (
+    "n_body_sim_pro_cuda_context_create", "n_body_sim_pro_cuda_context_destroy",
+    "n_body_sim_pro_cuda_context_set_theta", "n_body_sim_pro_cuda_context_theta",
+    "n_body_sim_pro_cuda_context_set_multipole_order",
+    "n_body_sim_pro_cuda_context_set_leaf_capacity", "n_body_sim_pro_cuda_context_stats",
+    "n_body_sim_pro_cuda_context_timings", "n_body_sim_pro_gravity_compute_acceleration_cuda",
+    "n_body_sim_pro_barnes_hut_compute_acceleration_cuda", "n_body_sim_pro_cuda_upload",
+    "n_body_sim_pro_cuda_download", "n_body_sim_pro_cuda_compute_acceleration",
+    "n_body_sim_pro_cuda_advance", "n_body_sim_pro_cuda_diagnostics",
+    "n_body_sim_pro_cuda_reference_acceleration", "n_body_sim_pro_cuda_morton_order",
+    "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
+    "n_body_sim_pro_cuda_kernel_launches",
+)
+
+
+def kernel_launches() -> int:
+    """CUDA kernels this process has launched through the library."""
+    return int(library().n_body_sim_pro_cuda_kernel_launches())
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Load the in-tree shared library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m n_body_sim_pro_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    pv, pg, pe, vp = C.POINTER(View), C.POINTER(Gravity), C.POINTER(Error), C.c_void_p
+    st = C.c_int
+    sig = {
+        "n_body_sim_pro_cuda_context_create": (vp, [pe]),
+        "n_body_sim_pro_cuda_context_destroy": (None, [vp]),
+        "n_body_sim_pro_cuda_context_set_theta": (None, [vp, C.c_double]),
+        "n_body_sim_pro_cuda_context_theta": (C.c_double, [vp]),
+        "n_body_sim_pro_cuda_context_set_multipole_order": (st, [vp, C.c_int, pe]),
+        "n_body_sim_pro_cuda_context_set_leaf_capacity": (st, [vp, C.c_int, pe]),
+        "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
+        "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
+        "n_body_sim_pro_gravity_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
+        "n_body_sim_pro_barnes_hut_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
+        "n_body_sim_pro_cuda_upload": (st, [vp, pv, pe]),
+        "n_body_sim_pro_cuda_download": (st, [vp, pv, pe]),
+        "n_body_sim_pro_cuda_compute_acceleration": (st, [vp, pg, C.c_int, pe]),
+        "n_body_sim_pro_cuda_advance": (st, [vp, pg, C.c_int, C.c_double, C.c_int, C.c_int, pe]),
+        "n_body_sim_pro_cuda_diagnostics": (st, [vp, pg, C.POINTER(DiagnosticsQuantities),
+                                                 C.POINTER(C.c_double), pe]),
+        "n_body_sim_pro_cuda_reference_acceleration": (st, [vp, pg, C.POINTER(C.c_int64),
+                                                            C.c_size_t, C.POINTER(C.c_double), pe]),
+        "n_body_sim_pro_cuda_morton_order": (st, [vp, C.POINTER(C.c_uint64),
+                                                  C.POINTER(C.c_uint64), C.POINTER(C.c_double),
+                                                  pe]),
+        "n_body_sim_pro_cuda_synchronize": (st, [vp, pe]),
+        "n_body_sim_pro_cuda_architecture": (C.c_char_p, []),
+        "n_body_sim_pro_cuda_kernel_launches": (C.c_ulonglong, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype, f.argtypes = res, args
+    _lib = L
+    return L
+
+
+def _check(status: int, err: Error) -> None:
+    if status != Status.OK:
+        raise CudaError(status, err.message.decode(errors="replace"))
+
+
+# ---------------------------------------------------------------------------
+# particle storage
+# ---------------------------------------------------------------------------
+
+_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+
+
+@dataclass
+class ParticleSystem:
+    """SoA float64 storage with the reference's field set; ``view()`` gives the
+    NBodySimProParticleSystemView the C ABI takes.  Arrays may be numpy arrays
+    in pinned memory (see :func:`pinned_empty`)."""
+
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    ax: np.ndarray
+    ay: np.ndarray
+    az: np.ndarray
+    m: np.ndarray
+
+    @classmethod
+    def zeros(cls, n: int, allocator=None) -> "ParticleSystem":
+        alloc = allocator or (lambda k: np.zeros(k, dtype=np.float64))
+        return cls(*[alloc(n) for _ in _FIELDS])
+
+    @classmethod
+    def from_arrays(cls, pos: np.ndarray, vel: np.ndarray, mass: np.ndarray,
+                    acc: np.ndarray | None = None) -> "ParticleSystem":
+        n = mass.shape[0]
+        acc = np.zeros((n, 3)) if acc is None else acc
+        cols = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2],
+                          acc[:, 0], acc[:, 1], acc[:, 2], mass)]
+        return cls(*cols)
+
+    @property
+    def n(self) -> int:
+        return int(self.x.shape[0])
+
+    def view(self) -> View:
+        for f in _FIELDS:
+            a = getattr(self, f)
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(f"field {f} must be contiguous float64")
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        return View(self.n, *[p(getattr(self, f)) for f in _FIELDS])
+
+    def acc(self) -> np.ndarray:
+        return np.stack([self.ax, self.ay, self.az], axis=1)
+
+    def copy(self) -> "ParticleSystem":
+        return ParticleSystem(*[getattr(self, f).copy() for f in _FIELDS])
+
+
+# ---------------------------------------------------------------------------
+# force functions (NBodySimProForceFunction)
+# ---------------------------------------------------------------------------
+
+def _force(name: str, system: ParticleSystem, gravity: Gravity, context) -> np.ndarray:
+    L = library()
+    err = Error()
+    v = system.view()
+    ctx = context.handle if isinstance(context, CudaContext) else context
+    _check(getattr(L, name)(C.byref(v), C.byref(gravity), ctx, C.byref(err)), err)
+    return system.acc()
+
+
+def n_body_sim_pro_gravity_compute_acceleration_cuda(system: ParticleSystem, gravity: Gravity,
+                                                     context=None) -> np.ndarray:
+    """`cuda` algorithm: exact all-pairs forces written into system.ax/ay/az."""
+    return _force("n_body_sim_pro_gravity_compute_acceleration_cuda", system, gravity, context)
+
+
+def n_body_sim_pro_barnes_hut_compute_acceleration_cuda(system: ParticleSystem, gravity: Gravity,
+                                                        context=None) -> np.ndarray:
+    """`barnes_hut_cuda` algorithm: GPU Barnes-Hut forces into system.ax/ay/az."""
+    return _force("n_body_sim_pro_barnes_hut_compute_acceleration_cuda", system, gravity, context)
+
+
+class CudaContext:
+    """NBodySimProCudaContext: device-resident state, stepping and diagnostics."""
+
+    def __init__(self, theta: float | None = None, multipole_order: int | None = None,
+                 leaf_capacity: int | None = None):
+        L = library()
+        err = Error()
+        h = L.n_body_sim_pro_cuda_context_create(C.byref(err))
+        if not h:
+            raise CudaError(err.status or Status.UNSUPPORTED_PLATFORM,
+                            err.message.decode(errors="replace"))
+        self.handle = C.c_void_p(h)
+        self.n = 0
+        if theta is not None:
+            self.theta = theta
+        if multipole_order is not None:
+            self.set_multipole_order(multipole_order)
+        if leaf_capacity is not None:
+            self.set_leaf_capacity(leaf_capacity)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            library().n_body_sim_pro_cuda_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def theta(self) -> float:
+        return library().n_body_sim_pro_cuda_context_theta(self.handle)
+
+    @theta.setter
+    def theta(self, value: float) -> None:
+        library().n_body_sim_pro_cuda_context_set_theta(self.handle, float(value))
+
+    def set_multipole_order(self, order: int) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_multipole_order(self.handle, order,
+                                                                         C.byref(err)), err)
+
+    def set_leaf_capacity(self, capacity: int) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_leaf_capacity(self.handle, capacity,
+                                                                       C.byref(err)), err)
+
+    def stats(self) -> dict:
+        s = BarnesHutStats()
+        if library().n_body_sim_pro_cuda_context_stats(self.handle, C.byref(s)) != 0:
+            raise CudaError(Status.INVALID_ARGUMENT, "stats")
+        return s.as_dict()
+
+    def timings(self) -> dict:
+        t = Timings()
+        library().n_body_sim_pro_cuda_context_timings(self.handle, C.byref(t))
+        return t.as_dict()
+
+    def upload(self, system: ParticleSystem) -> None:
+        err = Error()
+        v = system.view()
+        _check(library().n_body_sim_pro_cuda_upload(self.handle, C.byref(v), C.byref(err)), err)
+        self.n = system.n
+
+    def download(self, system: ParticleSystem) -> None:
+        err = Error()
+        v = system.view()
+        _check(library().n_body_sim_pro_cuda_download(self.handle, C.byref(v), C.byref(err)), err)
+
+    def compute_acceleration(self, gravity: Gravity, algorithm: Algorithm) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_compute_acceleration(
+            self.handle, C.byref(gravity), int(algorithm), C.byref(err)), err)
+
+    def advance(self, gravity: Gravity, timestep: float, steps: int,
+                algorithm: Algorithm = Algorithm.ALL_PAIRS,
+                integrator: Integrator = Integrator.LEAPFROG) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_advance(self.handle, C.byref(gravity),
+                                                     int(integrator), float(timestep), int(steps),
+                                                     int(algorithm), C.byref(err)), err)
+
+    def diagnostics(self, gravity: Gravity | None = None, potential: bool = False):
+        err = Error()
+        q = DiagnosticsQuantities()
+        pe = C.c_double(0.0)
+        g = C.byref(gravity) if gravity is not None else None
+        _check(library().n_body_sim_pro_cuda_diagnostics(self.handle, g, C.byref(q),
+                                                         C.byref(pe) if potential else None,
+                                                         C.byref(err)), err)
+        return (q.as_array(), pe.value) if potential else q.as_array()
+
+    def reference_acceleration(self, gravity: Gravity, targets: np.ndarray) -> np.ndarray:
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        out = np.zeros((t.shape[0], 3), dtype=np.float64)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_reference_acceleration(
+            self.handle, C.byref(gravity), t.ctypes.data_as(C.POINTER(C.c_int64)), t.shape[0],
+            out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(err)), err)
+        return out
+
+    def morton_order(self):
+        keys = np.zeros(self.n, dtype=np.uint64)
+        perm = np.zeros(self.n, dtype=np.uint64)
+        root = np.zeros(4, dtype=np.float64)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_morton_order(
+            self.handle, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+            perm.ctypes.data_as(C.POINTER(C.c_uint64)),
+            root.ctypes.data_as(C.POINTER(C.c_double)), C.byref(err)), err)
+        return keys, perm, root
+
+    def synchronize(self) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_synchronize(self.handle, C.byref(err)), err)

@@ -1,0 +1,835 @@
+/*
+ * C17 host layer of libn_body_sim_pro_cuda: argument checking and error
+ * reporting with the reference engine's conventions, device memory and stream
+ * management, the integrator loops, the all-pairs tile autotuner, and the
+ * plugin entry points.  All GPU work is enqueued through the launchers of
+ * internal.h on the context's stream.
+ *
+ * Reference behaviour followed here:
+ *   error reporting       src/c/core/status.c:29-46 (n_body_sim_pro_error_set)
+ *   argument checks       src/c/physics/gravity.c:19-23, integrator.c:145-156,
+ *                         barnes_hut.c:446-451, :642-646
+ *   integrator semantics  src/c/physics/integrator.c:15-172
+ */
+#include "n_body_sim_pro_cuda.h"
+
+#include "bh.h"
+#include "internal.h"
+
+#include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------- */
+/* errors                                                                     */
+/* ------------------------------------------------------------------------- */
+
+static NBodySimProStatus fail(NBodySimProError* error, NBodySimProStatus status, const char* file,
+                              int line, const char* message) {
+    if (error != NULL) {
+        error->status = status;
+        error->source_file = file;
+        error->source_line = line;
+        size_t length = message != NULL ? strlen(message) : 0;
+        if (length >= sizeof(error->message)) length = sizeof(error->message) - 1;
+        if (length > 0) memcpy(error->message, message, length);
+        error->message[length] = '\0';
+    }
+    return status;
+}
+
+#define FAIL(status, message) fail(error, (status), __FILE__, __LINE__, (message))
+
+static NBodySimProStatus cuda_fail(NBodySimProError* error, cudaError_t code, const char* what,
+                                   const char* file, int line) {
+    char text[256];
+    snprintf(text, sizeof(text), "%s: %s", what, cudaGetErrorString(code));
+    NBodySimProStatus status = N_BODY_SIM_PRO_STATUS_INVALID_STATE;
+    if (code == cudaErrorMemoryAllocation) {
+        status = N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY;
+    } else if (code == cudaErrorNoDevice || code == cudaErrorInsufficientDriver ||
+               code == cudaErrorNoKernelImageForDevice || code == cudaErrorInvalidDevice) {
+        status = N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM;
+    }
+    return fail(error, status, file, line, text);
+}
+
+#define CUDA_TRY(call)                                                              \
+    do {                                                                            \
+        cudaError_t cuda_try_code = (call);                                         \
+        if (cuda_try_code != cudaSuccess)                                           \
+            return cuda_fail(error, cuda_try_code, #call, __FILE__, __LINE__);      \
+    } while (0)
+
+/* ------------------------------------------------------------------------- */
+/* context                                                                    */
+/* ------------------------------------------------------------------------- */
+
+enum { TUNE_SLOTS = 16, EVENT_COUNT = 10 };
+
+typedef struct TuneEntry {
+    size_t n;
+    int zero_softening;
+    NbspAllPairsShape shape;
+} TuneEntry;
+
+struct NBodySimProCudaContext {
+    int device;
+    int sm_count;
+    cudaStream_t stream;
+    cudaEvent_t events[EVENT_COUNT];
+
+    size_t capacity;  /* particles the state buffers hold */
+    size_t n;         /* resident particle count */
+    size_t n_padded;  /* n rounded up to 256 (all-pairs source tiles) */
+    int resident;     /* a state was uploaded */
+
+    double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *m;
+    void* packed;     /* float4[capacity_padded] */
+    void* partial_hi; /* float4[partial_elems] */
+    void* partial_lo;
+    size_t partial_elems;
+    double* centre;   /* device double[3] */
+    double* scratch;  /* device doubles */
+    size_t scratch_elems;
+    double* out;      /* device double[16] */
+    int* status;      /* device status bits */
+    double* host_out; /* pinned double[16] */
+    int* host_status; /* pinned int */
+
+    double theta;
+    int multipole_order;
+    int leaf_capacity;
+    NbspBarnesHut* bh;
+    int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
+
+    NBodySimProBarnesHutStats stats;
+    NBodySimProCudaTimings timings;
+
+    TuneEntry tune[TUNE_SLOTS];
+    int tune_count;
+    int autotune;
+};
+
+static void release_state(NBodySimProCudaContext* c) {
+    double** arrays[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->ax, &c->ay, &c->az, &c->m};
+    for (size_t k = 0; k < sizeof(arrays) / sizeof(arrays[0]); ++k) {
+        cudaFree(*arrays[k]);
+        *arrays[k] = NULL;
+    }
+    cudaFree(c->packed);
+    c->packed = NULL;
+    c->capacity = 0;
+}
+
+NBodySimProCudaContext* n_body_sim_pro_cuda_context_create(NBodySimProError* error) {
+    int count = 0;
+    cudaError_t code = cudaGetDeviceCount(&count);
+    if (code != cudaSuccess || count == 0) {
+        fail(error, N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM, __FILE__, __LINE__,
+             code != cudaSuccess ? cudaGetErrorString(code) : "no CUDA device");
+        return NULL;
+    }
+    NBodySimProCudaContext* c = (NBodySimProCudaContext*)calloc(1, sizeof(*c));
+    if (c == NULL) {
+        fail(error, N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY, __FILE__, __LINE__,
+             "failed to allocate CUDA context");
+        return NULL;
+    }
+    c->theta = 0.7;
+    c->multipole_order = 1;
+    c->leaf_capacity = 16;
+    const char* tune = getenv("NBSP_AUTOTUNE");
+    c->autotune = !(tune != NULL && tune[0] == '0');
+    struct cudaDeviceProp prop;
+    if ((code = cudaGetDevice(&c->device)) != cudaSuccess ||
+        (code = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) {
+        free(c);
+        cuda_fail(error, code, "cudaGetDeviceProperties", __FILE__, __LINE__);
+        return NULL;
+    }
+    if (prop.major < 10) {
+        free(c);
+        fail(error, N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM, __FILE__, __LINE__,
+             "this library is built for sm_100a (B200)");
+        return NULL;
+    }
+    c->sm_count = prop.multiProcessorCount;
+    code = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    for (int k = 0; k < EVENT_COUNT && code == cudaSuccess; ++k) code = cudaEventCreate(&c->events[k]);
+    if (code == cudaSuccess) code = cudaMalloc((void**)&c->centre, 3 * sizeof(double));
+    if (code == cudaSuccess) code = cudaMalloc((void**)&c->out, 16 * sizeof(double));
+    if (code == cudaSuccess) code = cudaMalloc((void**)&c->status, sizeof(int));
+    if (code == cudaSuccess) code = cudaMallocHost((void**)&c->host_out, 16 * sizeof(double));
+    if (code == cudaSuccess) code = cudaMallocHost((void**)&c->host_status, sizeof(int));
+    if (code == cudaSuccess) code = cudaMemset(c->status, 0, sizeof(int));
+    if (code != cudaSuccess) {
+        cuda_fail(error, code, "context allocation", __FILE__, __LINE__);
+        n_body_sim_pro_cuda_context_destroy(c);
+        return NULL;
+    }
+    return c;
+}
+
+void n_body_sim_pro_cuda_context_destroy(NBodySimProCudaContext* c) {
+    if (c == NULL) return;
+    cudaSetDevice(c->device);
+    if (c->stream != NULL) cudaStreamSynchronize(c->stream);
+    nbsp_bh_destroy(c->bh);
+    release_state(c);
+    cudaFree(c->partial_hi);
+    cudaFree(c->partial_lo);
+    cudaFree(c->scratch);
+    cudaFree(c->centre);
+    cudaFree(c->out);
+    cudaFree(c->status);
+    cudaFreeHost(c->host_out);
+    cudaFreeHost(c->host_status);
+    for (int k = 0; k < EVENT_COUNT; ++k)
+        if (c->events[k] != NULL) cudaEventDestroy(c->events[k]);
+    if (c->stream != NULL) cudaStreamDestroy(c->stream);
+    free(c);
+}
+
+void n_body_sim_pro_cuda_context_set_theta(NBodySimProCudaContext* c, double theta) {
+    if (c != NULL) c->theta = theta;
+}
+
+double n_body_sim_pro_cuda_context_theta(const NBodySimProCudaContext* c) {
+    return c != NULL ? c->theta : 0.0;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_multipole_order(NBodySimProCudaContext* c,
+                                                                  int order,
+                                                                  NBodySimProError* error) {
+    if (c == NULL || (order != 1 && order != 2))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "multipole order must be 1 or 2");
+    c->multipole_order = order;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_capacity(NBodySimProCudaContext* c,
+                                                                int capacity,
+                                                                NBodySimProError* error) {
+    if (c == NULL || capacity < 1 || capacity > NBSP_BH_MAX_LEAF)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "leaf capacity must be in 1..64");
+    c->leaf_capacity = capacity;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+int n_body_sim_pro_cuda_context_stats(const NBodySimProCudaContext* c,
+                                      NBodySimProBarnesHutStats* stats) {
+    if (c == NULL || stats == NULL) return 1;
+    *stats = c->stats;
+    return 0;
+}
+
+int n_body_sim_pro_cuda_context_timings(const NBodySimProCudaContext* c,
+                                        NBodySimProCudaTimings* timings) {
+    if (c == NULL || timings == NULL) return 1;
+    *timings = c->timings;
+    return 0;
+}
+
+const char* n_body_sim_pro_cuda_architecture(void) { return "sm_100a"; }
+
+unsigned long long nbsp_kernel_launch_count = 0;
+
+unsigned long long n_body_sim_pro_cuda_kernel_launches(void) {
+    return __atomic_load_n(&nbsp_kernel_launch_count, __ATOMIC_RELAXED);
+}
+
+static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+static NBodySimProStatus ensure_capacity(NBodySimProCudaContext* c, size_t n,
+                                         NBodySimProError* error) {
+    if (n <= c->capacity && c->packed != NULL) return N_BODY_SIM_PRO_STATUS_OK;
+    release_state(c);
+    const size_t cap = n < 256 ? 256 : n;
+    double** arrays[] = {&c->x, &c->y, &c->z, &c->vx, &c->vy, &c->vz, &c->ax, &c->ay, &c->az, &c->m};
+    for (size_t k = 0; k < sizeof(arrays) / sizeof(arrays[0]); ++k) {
+        CUDA_TRY(cudaMalloc((void**)arrays[k], cap * sizeof(double)));
+    }
+    CUDA_TRY(cudaMalloc(&c->packed, round_up(cap, 256) * 16));
+    c->capacity = cap;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus ensure_scratch(NBodySimProCudaContext* c, size_t doubles,
+                                        NBodySimProError* error) {
+    if (doubles <= c->scratch_elems) return N_BODY_SIM_PRO_STATUS_OK;
+    cudaFree(c->scratch);
+    c->scratch = NULL;
+    c->scratch_elems = 0;
+    CUDA_TRY(cudaMalloc((void**)&c->scratch, doubles * sizeof(double)));
+    c->scratch_elems = doubles;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus ensure_partials(NBodySimProCudaContext* c, size_t elems,
+                                         NBodySimProError* error) {
+    if (elems <= c->partial_elems) return N_BODY_SIM_PRO_STATUS_OK;
+    cudaFree(c->partial_hi);
+    cudaFree(c->partial_lo);
+    c->partial_hi = c->partial_lo = NULL;
+    c->partial_elems = 0;
+    CUDA_TRY(cudaMalloc(&c->partial_hi, elems * 16));
+    CUDA_TRY(cudaMalloc(&c->partial_lo, elems * 16));
+    c->partial_elems = elems;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* Read and clear the device status word; map it to a status code. */
+static NBodySimProStatus check_device_status(NBodySimProCudaContext* c, NBodySimProError* error) {
+    CUDA_TRY(cudaMemcpyAsync(c->host_status, c->status, sizeof(int), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->bh_pending) {
+        nbsp_bh_collect(c->bh, &c->stats, &c->timings);
+        c->bh_pending = 0;
+    }
+    const int bits = *c->host_status;
+    if (bits & NBSP_DEVICE_ERROR_NONFINITE_POSITION)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "non-finite particle position");
+    if (bits & NBSP_DEVICE_ERROR_DUPLICATE_POSITION) /* barnes_hut.c:149-153 */
+        return FAIL(N_BODY_SIM_PRO_STATUS_OVERFLOW,
+                    "Barnes-Hut tree exceeded maximum depth (duplicate positions?)");
+    if (bits & NBSP_DEVICE_ERROR_TREE_INCONSISTENT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_OVERFLOW, "Barnes-Hut tree build exceeded its bounds");
+    if (bits & NBSP_DEVICE_ERROR_WALK_LIMIT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "Barnes-Hut walk exceeded its step limit");
+    if (bits & NBSP_DEVICE_ERROR_ENSEMBLE_LIMIT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "ensemble kernel exceeded its limits");
+    if (bits != 0) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "unknown device status");
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus check_gravity(const NBodySimProGravity* g, NBodySimProError* error) {
+    if (!isfinite(g->gravitational_constant) || !isfinite(g->softening_squared) ||
+        g->softening_squared < 0.0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "gravity parameters must be finite with non-negative softening");
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* all-pairs tile autotuner                                                   */
+/* ------------------------------------------------------------------------- */
+
+static const NbspAllPairsShape kShapes[] = {
+    {128, 4, 1}, {128, 2, 1}, {256, 2, 1}, {64, 8, 1}, {128, 8, 1}, {64, 4, 1}, {256, 4, 1},
+};
+
+/* Source chunks so that (target blocks x chunks) fills whole waves of resident CTAs. */
+static NbspAllPairsShape fit_chunks(const NBodySimProCudaContext* c, NbspAllPairsShape s,
+                                    size_t n) {
+    const size_t per_cta = (size_t)s.block * (size_t)s.per_thread;
+    const size_t target_blocks = (n + per_cta - 1) / per_cta;
+    int resident = nbsp_allpairs_resident_ctas(s);
+    if (resident < 1) resident = 1;
+    const size_t slots = (size_t)c->sm_count * (size_t)resident;
+    const size_t tiles = round_up(n, 256) / (size_t)s.block;
+    size_t best_chunks = 1;
+    double best_eff = 0.0;
+    for (size_t chunks = 1; chunks <= 64 && chunks <= tiles; ++chunks) {
+        const size_t tiles_per_chunk = (tiles + chunks - 1) / chunks;
+        if (chunks > 1 && tiles_per_chunk < 2) break;
+        const size_t ctas = target_blocks * chunks;
+        const size_t waves = (ctas + slots - 1) / slots;
+        /* useful work / work the busiest SM slot does, minus a small cost per chunk */
+        const double work = (double)target_blocks * (double)tiles;
+        const double span = (double)waves * (double)tiles_per_chunk * (double)slots;
+        const double eff = work / span - 0.002 * (double)chunks;
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best_chunks = chunks;
+        }
+    }
+    s.chunks = (int)best_chunks;
+    return s;
+}
+
+static NbspAllPairsShape choose_shape(NBodySimProCudaContext* c, size_t n, float eps2) {
+    const int zero = eps2 == 0.f;
+    for (int k = 0; k < c->tune_count; ++k)
+        if (c->tune[k].n == n && c->tune[k].zero_softening == zero) return c->tune[k].shape;
+    NbspAllPairsShape best = fit_chunks(c, kShapes[0], n);
+    if (c->autotune && n >= 2048) {
+        float best_ms = 1e30f;
+        const int shapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+        for (int k = 0; k < shapes; ++k) {
+            if (!nbsp_allpairs_shape_supported(kShapes[k])) continue;
+            NbspAllPairsShape s = fit_chunks(c, kShapes[k], n);
+            if ((size_t)s.chunks * n > c->partial_elems) continue;
+            float total = 0.f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(c->events[8], c->stream);
+                nbsp_allpairs_force(c->packed, n, c->n_padded, eps2, s, c->partial_hi,
+                                    c->partial_lo, c->stream);
+                cudaEventRecord(c->events[9], c->stream);
+                cudaEventSynchronize(c->events[9]);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, c->events[8], c->events[9]);
+                if (rep > 0) total += ms;
+            }
+            if (total < best_ms) {
+                best_ms = total;
+                best = s;
+            }
+        }
+    }
+    const int slot = c->tune_count < TUNE_SLOTS ? c->tune_count++ : (int)(n % TUNE_SLOTS);
+    c->tune[slot].n = n;
+    c->tune[slot].zero_softening = zero;
+    c->tune[slot].shape = best;
+    return best;
+}
+
+/* Partial buffers big enough for any candidate shape at n (<= 64 chunks). */
+static NBodySimProStatus prepare_allpairs(NBodySimProCudaContext* c, size_t n,
+                                          NBodySimProError* error) {
+    const size_t want = n * 64;
+    const size_t cap_bytes = (size_t)1 << 30; /* at most 2 x 1 GiB of partials */
+    size_t elems = want * 16 > cap_bytes ? cap_bytes / 16 : want;
+    if (elems < n) elems = n;
+    return ensure_partials(c, elems, error);
+}
+
+/* forces of the resident, already packed state -> c->ax/ay/az (FP64) */
+static NBodySimProStatus allpairs_accelerations(NBodySimProCudaContext* c,
+                                                const NBodySimProGravity* g,
+                                                NBodySimProError* error) {
+    const size_t n = c->n;
+    NBodySimProStatus st = prepare_allpairs(c, n, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    const float eps2 = (float)g->softening_squared;
+    NbspAllPairsShape s = choose_shape(c, n, eps2);
+    if ((size_t)s.chunks * n > c->partial_elems) s.chunks = (int)(c->partial_elems / n);
+    nbsp_allpairs_force(c->packed, n, c->n_padded, eps2, s, c->partial_hi, c->partial_lo,
+                        c->stream);
+    nbsp_allpairs_finalize(c->partial_hi, c->partial_lo, n, s.chunks, g->gravitational_constant,
+                           c->ax, c->ay, c->az, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus pack_state(NBodySimProCudaContext* c, NBodySimProError* error) {
+    NBodySimProStatus st = ensure_scratch(c, 11 * 1024, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    nbsp_centre_of_mass(c->x, c->y, c->z, c->m, c->n, c->scratch, c->centre, c->stream);
+    nbsp_pack_relative(c->x, c->y, c->z, c->m, c->n, c->n_padded, c->centre, c->packed, c->status,
+                       c->stream);
+    CUDA_TRY(cudaGetLastError());
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* One force evaluation of the resident state with `algorithm`. */
+static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
+                                                const NBodySimProGravity* g,
+                                                NBodySimProCudaAlgorithm algorithm,
+                                                NBodySimProError* error) {
+    if (c->n == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT) {
+        NbspBarnesHutParams p;
+        p.theta = c->theta;
+        p.gravitational_constant = g->gravitational_constant;
+        p.softening_squared = g->softening_squared;
+        p.multipole_order = c->multipole_order;
+        p.leaf_capacity = c->leaf_capacity;
+        NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
+        c->bh_pending = 1;
+        return nbsp_bh_accelerations(&c->bh, &s, &p, c->status, c->stream, &c->stats,
+                                     &c->timings, error);
+    }
+    NBodySimProStatus st = pack_state(c, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    return allpairs_accelerations(c, g, error);
+}
+
+/* ------------------------------------------------------------------------- */
+/* plugin force functions                                                     */
+/* ------------------------------------------------------------------------- */
+
+static NBodySimProCudaContext* g_default_context = NULL;
+
+static NBodySimProCudaContext* context_or_default(void* context, NBodySimProError* error) {
+    if (context != NULL) return (NBodySimProCudaContext*)context;
+    if (g_default_context == NULL) g_default_context = n_body_sim_pro_cuda_context_create(error);
+    return g_default_context;
+}
+
+static NBodySimProStatus copy_in(NBodySimProCudaContext* c, const NBodySimProParticleSystemView* v,
+                                 int everything, NBodySimProError* error) {
+    const size_t n = v->particle_count;
+    const size_t bytes = n * sizeof(double);
+    struct {
+        double* dst;
+        const double* src;
+        int always;
+    } copies[] = {
+        {c->x, v->positions_x, 1},      {c->y, v->positions_y, 1},
+        {c->z, v->positions_z, 1},      {c->m, v->masses, 1},
+        {c->vx, v->velocities_x, 0},    {c->vy, v->velocities_y, 0},
+        {c->vz, v->velocities_z, 0},    {c->ax, v->accelerations_x, 0},
+        {c->ay, v->accelerations_y, 0}, {c->az, v->accelerations_z, 0},
+    };
+    for (size_t k = 0; k < sizeof(copies) / sizeof(copies[0]); ++k) {
+        if (!copies[k].always && !everything) continue;
+        if (copies[k].src == NULL) {
+            if (copies[k].always) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                                              "view position and mass arrays must not be null");
+            CUDA_TRY(cudaMemsetAsync(copies[k].dst, 0, bytes, c->stream));
+            continue;
+        }
+        CUDA_TRY(cudaMemcpyAsync(copies[k].dst, copies[k].src, bytes, cudaMemcpyHostToDevice,
+                                 c->stream));
+    }
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus copy_accelerations_out(NBodySimProCudaContext* c,
+                                                const NBodySimProParticleSystemView* v,
+                                                NBodySimProError* error) {
+    const size_t bytes = v->particle_count * sizeof(double);
+    if (v->accelerations_x == NULL || v->accelerations_y == NULL || v->accelerations_z == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "view acceleration arrays must not be null");
+    CUDA_TRY(cudaMemcpyAsync(v->accelerations_x, c->ax, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(v->accelerations_y, c->ay, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(v->accelerations_z, c->az, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus view_force(const NBodySimProParticleSystemView* view,
+                                    const NBodySimProGravity* gravity, void* context,
+                                    NBodySimProCudaAlgorithm algorithm, NBodySimProError* error) {
+    if (view == NULL || gravity == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "view and gravity parameters must not be null");
+    NBodySimProStatus st = check_gravity(gravity, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && view->particle_count == 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "cannot build a Barnes-Hut tree for an empty system");
+    NBodySimProCudaContext* c = context_or_default(context, error);
+    if (c == NULL) return error != NULL ? error->status : N_BODY_SIM_PRO_STATUS_UNSUPPORTED_PLATFORM;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = view->particle_count;
+    if (n == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    if ((st = ensure_capacity(c, n, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    c->n = n;
+    c->n_padded = round_up(n, 256);
+    c->resident = 0; /* the plugin path only stages positions and masses */
+    if ((st = copy_in(c, view, 0, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    CUDA_TRY(cudaEventRecord(c->events[0], c->stream));
+    if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
+        return st;
+    CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
+    if ((st = copy_accelerations_out(c, view, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS) {
+        memset(&c->timings, 0, sizeof(c->timings));
+        c->timings.walk_ms = ms;
+    }
+    c->timings.total_ms = ms;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_gravity_compute_acceleration_cuda(
+    const NBodySimProParticleSystemView* view, const NBodySimProGravity* gravity, void* context,
+    NBodySimProError* error) {
+    return view_force(view, gravity, context, N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS, error);
+}
+
+NBodySimProStatus n_body_sim_pro_barnes_hut_compute_acceleration_cuda(
+    const NBodySimProParticleSystemView* view, const NBodySimProGravity* gravity, void* context,
+    NBodySimProError* error) {
+    return view_force(view, gravity, context, N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT, error);
+}
+
+/* ------------------------------------------------------------------------- */
+/* device-resident API                                                        */
+/* ------------------------------------------------------------------------- */
+
+NBodySimProStatus n_body_sim_pro_cuda_upload(NBodySimProCudaContext* c,
+                                             const NBodySimProParticleSystemView* view,
+                                             NBodySimProError* error) {
+    if (c == NULL || view == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context and view must not be null");
+    CUDA_TRY(cudaSetDevice(c->device));
+    NBodySimProStatus st = ensure_capacity(c, view->particle_count, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    c->n = view->particle_count;
+    c->n_padded = round_up(c->n, 256);
+    if (c->n > 0 && (st = copy_in(c, view, 1, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->resident = 1;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_download(NBodySimProCudaContext* c,
+                                               const NBodySimProParticleSystemView* view,
+                                               NBodySimProError* error) {
+    if (c == NULL || view == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context and view must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    if (view->particle_count != c->n)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "view particle count differs from the resident state");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t bytes = c->n * sizeof(double);
+    struct {
+        double* dst;
+        const double* src;
+    } copies[] = {
+        {view->positions_x, c->x},      {view->positions_y, c->y},
+        {view->positions_z, c->z},      {view->velocities_x, c->vx},
+        {view->velocities_y, c->vy},    {view->velocities_z, c->vz},
+        {view->accelerations_x, c->ax}, {view->accelerations_y, c->ay},
+        {view->accelerations_z, c->az}, {view->masses, c->m},
+    };
+    for (size_t k = 0; k < sizeof(copies) / sizeof(copies[0]); ++k) {
+        if (copies[k].dst == NULL || bytes == 0) continue;
+        CUDA_TRY(cudaMemcpyAsync(copies[k].dst, copies[k].src, bytes, cudaMemcpyDeviceToHost,
+                                 c->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_compute_acceleration(NBodySimProCudaContext* c,
+                                                           const NBodySimProGravity* gravity,
+                                                           NBodySimProCudaAlgorithm algorithm,
+                                                           NBodySimProError* error) {
+    if (c == NULL || gravity == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context and gravity must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    NBodySimProStatus st = check_gravity(gravity, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && c->n == 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "cannot build a Barnes-Hut tree for an empty system");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaEventRecord(c->events[0], c->stream));
+    if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
+        return st;
+    CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
+    if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS) {
+        memset(&c->timings, 0, sizeof(c->timings));
+        c->timings.walk_ms = ms;
+    }
+    c->timings.total_ms = ms;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* Leapfrog / Verlet on all-pairs: opening kick+drift, then per step one force
+ * pass and one fused epilogue (closing kick of this step + opening kick and
+ * drift of the next + repack). */
+static NBodySimProStatus advance_allpairs_kdk(NBodySimProCudaContext* c,
+                                              const NBodySimProGravity* g, double dt, int steps,
+                                              NBodySimProError* error) {
+    const size_t n = c->n;
+    const double h = 0.5 * dt;
+    NBodySimProStatus st = prepare_allpairs(c, n, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if ((st = ensure_scratch(c, 11 * 1024, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    nbsp_kick_drift(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, n, h, dt,
+                    c->stream);
+    nbsp_centre_of_mass(c->x, c->y, c->z, c->m, n, c->scratch, c->centre, c->stream);
+    nbsp_pack_relative(c->x, c->y, c->z, c->m, n, c->n_padded, c->centre, c->packed, c->status,
+                       c->stream);
+    const float eps2 = (float)g->softening_squared;
+    NbspAllPairsShape s = choose_shape(c, n, eps2);
+    if ((size_t)s.chunks * n > c->partial_elems) s.chunks = (int)(c->partial_elems / n);
+    for (int step = 0; step < steps; ++step) {
+        nbsp_allpairs_force(c->packed, n, c->n_padded, eps2, s, c->partial_hi, c->partial_lo,
+                            c->stream);
+        if (step + 1 < steps) {
+            nbsp_allpairs_finalize_kick_kick_drift_pack(
+                c->partial_hi, c->partial_lo, n, c->n_padded, s.chunks, g->gravitational_constant,
+                c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, c->m, h, dt, c->centre,
+                c->packed, c->status, c->stream);
+        } else {
+            nbsp_allpairs_finalize_kick(c->partial_hi, c->partial_lo, n, s.chunks,
+                                        g->gravitational_constant, c->ax, c->ay, c->az, c->vx,
+                                        c->vy, c->vz, h, c->stream);
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_advance(NBodySimProCudaContext* c,
+                                              const NBodySimProGravity* gravity,
+                                              NBodySimProIntegratorType integrator,
+                                              double timestep, int steps,
+                                              NBodySimProCudaAlgorithm algorithm,
+                                              NBodySimProError* error) {
+    if (c == NULL || gravity == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "view, gravity, and force function must not be null");
+    if (!(timestep > 0.0)) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "timestep must be positive");
+    if (steps < 0) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "steps must be non-negative");
+    if (integrator != N_BODY_SIM_PRO_INTEGRATOR_EULER &&
+        integrator != N_BODY_SIM_PRO_INTEGRATOR_LEAPFROG &&
+        integrator != N_BODY_SIM_PRO_INTEGRATOR_VELOCITY_VERLET)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown integrator type");
+    if (algorithm != N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS &&
+        algorithm != N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown algorithm");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    NBodySimProStatus st = check_gravity(gravity, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && c->n == 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "cannot build a Barnes-Hut tree for an empty system");
+    if (c->n == 0 || steps == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaEventRecord(c->events[0], c->stream));
+    const size_t n = c->n;
+    const double dt = timestep, h = 0.5 * timestep;
+    if (integrator == N_BODY_SIM_PRO_INTEGRATOR_EULER) {
+        for (int step = 0; step < steps; ++step) {
+            if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
+                return st;
+            nbsp_euler_update(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, n, dt,
+                              c->stream);
+        }
+    } else if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS) {
+        if ((st = advance_allpairs_kdk(c, gravity, dt, steps, error)) != N_BODY_SIM_PRO_STATUS_OK)
+            return st;
+    } else {
+        for (int step = 0; step < steps; ++step) {
+            nbsp_kick_drift(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, n, h, dt,
+                            c->stream);
+            if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
+                return st;
+            nbsp_kick_drift(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, n, h, 0.0,
+                            c->stream);
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
+    if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
+    c->timings.total_ms = ms;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_diagnostics(NBodySimProCudaContext* c,
+                                                  const NBodySimProGravity* gravity,
+                                                  NBodySimProDiagnosticsQuantities* q,
+                                                  double* potential_energy,
+                                                  NBodySimProError* error) {
+    if (c == NULL || q == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "view and quantities must not be null");
+    if (potential_energy != NULL && gravity == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "view, gravity, and output must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    CUDA_TRY(cudaSetDevice(c->device));
+    memset(q, 0, sizeof(*q));
+    if (potential_energy != NULL) *potential_energy = 0.0;
+    if (c->n == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    NBodySimProStatus st = ensure_scratch(c, c->n > 11 * 1024 ? c->n : 11 * 1024, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    nbsp_global_sums(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->m, c->n, c->scratch, c->out,
+                     c->stream);
+    if (potential_energy != NULL)
+        nbsp_potential_energy(c->x, c->y, c->z, c->m, c->n, gravity->gravitational_constant,
+                              gravity->softening_squared, c->scratch, c->out + 11, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c->host_out, c->out, 12 * sizeof(double), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const double* r = c->host_out;
+    q->kinetic_energy = r[0];
+    q->total_mass = r[1];
+    q->total_momentum_x = r[2];
+    q->total_momentum_y = r[3];
+    q->total_momentum_z = r[4];
+    q->total_angular_momentum_x = r[5];
+    q->total_angular_momentum_y = r[6];
+    q->total_angular_momentum_z = r[7];
+    if (r[1] != 0.0) {
+        q->center_of_mass_x = r[8] / r[1];
+        q->center_of_mass_y = r[9] / r[1];
+        q->center_of_mass_z = r[10] / r[1];
+    }
+    if (potential_energy != NULL) *potential_energy = r[11];
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_reference_acceleration(NBodySimProCudaContext* c,
+                                                             const NBodySimProGravity* gravity,
+                                                             const int64_t* targets, size_t count,
+                                                             double* out,
+                                                             NBodySimProError* error) {
+    if (c == NULL || gravity == NULL || (count > 0 && (targets == NULL || out == NULL)))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "arguments must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    for (size_t t = 0; t < count; ++t)
+        if (targets[t] < 0 || (size_t)targets[t] >= c->n)
+            return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "target index out of range");
+    if (count == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int chunks = (int)(4 * c->sm_count * 4 / ((count + 127) / 128));
+    if (chunks < 1) chunks = 1;
+    if ((size_t)chunks > c->n / 256 + 1) chunks = (int)(c->n / 256 + 1);
+    NBodySimProStatus st = ensure_scratch(c, 3 * count * (size_t)chunks, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    int64_t* d_targets = NULL;
+    double* d_out = NULL;
+    CUDA_TRY(cudaMallocAsync((void**)&d_targets, count * sizeof(int64_t), c->stream));
+    cudaError_t code = cudaMallocAsync((void**)&d_out, 3 * count * sizeof(double), c->stream);
+    if (code == cudaSuccess)
+        code = cudaMemcpyAsync(d_targets, targets, count * sizeof(int64_t), cudaMemcpyHostToDevice,
+                               c->stream);
+    if (code == cudaSuccess) {
+        nbsp_reference_subset(c->x, c->y, c->z, c->m, c->n, d_targets, count,
+                              gravity->gravitational_constant, gravity->softening_squared,
+                              c->scratch, chunks, d_out, c->stream);
+        code = cudaGetLastError();
+    }
+    if (code == cudaSuccess)
+        code = cudaMemcpyAsync(out, d_out, 3 * count * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream);
+    cudaFreeAsync(d_targets, c->stream);
+    if (d_out != NULL) cudaFreeAsync(d_out, c->stream);
+    if (code == cudaSuccess) code = cudaStreamSynchronize(c->stream);
+    if (code != cudaSuccess) return cuda_fail(error, code, "reference acceleration", __FILE__, __LINE__);
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_morton_order(NBodySimProCudaContext* c, uint64_t* keys_sorted,
+                                                   uint64_t* permutation, double* root,
+                                                   NBodySimProError* error) {
+    if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    if (c->n == 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "cannot build a Barnes-Hut tree for an empty system");
+    CUDA_TRY(cudaSetDevice(c->device));
+    NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
+    NBodySimProStatus st =
+        nbsp_bh_morton(&c->bh, &s, c->status, c->stream, keys_sorted, permutation, root, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    return check_device_status(c, error);
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_synchronize(NBodySimProCudaContext* c,
+                                                  NBodySimProError* error) {
+    if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return N_BODY_SIM_PRO_STATUS_OK;
+}

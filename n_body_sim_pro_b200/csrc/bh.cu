@@ -1,0 +1,1033 @@
+// GPU Barnes-Hut kernels for sm_100a.
+//
+// Reference (richie-rich90454/n_body_sim_pro, src/c/barnes_hut/barnes_hut.c):
+//   root cube      :453-483   keys  :286-305   sort  :312-339
+//   reorder        :402-440   COM   :214-253   walk  :549-636   scatter :692-704
+//
+// The Morton keys and the sort permutation are bit-exact with the reference:
+// all FP64 arithmetic of the root cube and of morton_axis_code is done with
+// explicitly rounded __d*_rn intrinsics (no contraction), and the 8 x 8-bit
+// stable LSD sort yields the same permutation as the reference's stable
+// 3 x 21-bit LSD sort (a stable sort by the full key, ties by original index).
+//
+// The tree differs from the reference's pointer octree by design: it is built
+// in parallel from the sorted keys (a Karras binary radix tree, one thread per
+// internal node), collapsed to a path-compressed octree whose leaves hold up to
+// `leaf_capacity` Morton-contiguous particles, and stored in depth-first order
+// with skip links so the walk needs no stack.  Parity is judged on forces
+// against the FP64 all-pairs oracle, and the opening test is the reference's:
+// accept a cell when (2h)^2 < theta^2 d^2, d to the cell centre of mass.
+#include "bh.h"
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// bounds
+// ---------------------------------------------------------------------------
+
+constexpr int kBoundsThreads = 256;
+constexpr int kBoundsBlocks = 1024;
+constexpr int kBoundsVals = 10;  // min xyz, max xyz, m, mx, my, mz
+
+__global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
+    const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+    const double* __restrict__ m, size_t n, double* __restrict__ partial, int* status) {
+  __shared__ double sh[kBoundsVals][kBoundsThreads];
+  double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
+                           0.0,      0.0,      0.0,      0.0};
+  bool bad = false;
+  for (size_t i = blockIdx.x * (size_t)kBoundsThreads + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * kBoundsThreads) {
+    const double px = x[i], py = y[i], pz = z[i], pm = m[i];
+    bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
+    v[0] = fmin(v[0], px);
+    v[1] = fmin(v[1], py);
+    v[2] = fmin(v[2], pz);
+    v[3] = fmax(v[3], px);
+    v[4] = fmax(v[4], py);
+    v[5] = fmax(v[5], pz);
+    v[6] += pm;
+    v[7] += pm * px;
+    v[8] += pm * py;
+    v[9] += pm * pz;
+  }
+  if (bad) atomicOr(status, NBSP_DEVICE_ERROR_NONFINITE_POSITION);
+  const int t = threadIdx.x;
+  for (int q = 0; q < kBoundsVals; ++q) sh[q][t] = v[q];
+  __syncthreads();
+  for (int stride = kBoundsThreads / 2; stride > 0; stride >>= 1) {
+    if (t < stride) {
+      for (int q = 0; q < 3; ++q) sh[q][t] = fmin(sh[q][t], sh[q][t + stride]);
+      for (int q = 3; q < 6; ++q) sh[q][t] = fmax(sh[q][t], sh[q][t + stride]);
+      for (int q = 6; q < kBoundsVals; ++q) sh[q][t] += sh[q][t + stride];
+    }
+    __syncthreads();
+  }
+  if (t < kBoundsVals) partial[blockIdx.x * kBoundsVals + t] = sh[t][0];
+}
+
+// Root cube with the exact FP64 operation sequence of barnes_hut.c:471-483.
+__global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
+    const double* __restrict__ partial, int blocks, double* __restrict__ geometry) {
+  __shared__ double sh[kBoundsVals][kBoundsThreads];
+  double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
+                           0.0,      0.0,      0.0,      0.0};
+  for (int b = threadIdx.x; b < blocks; b += kBoundsThreads) {
+    for (int q = 0; q < 3; ++q) v[q] = fmin(v[q], partial[b * kBoundsVals + q]);
+    for (int q = 3; q < 6; ++q) v[q] = fmax(v[q], partial[b * kBoundsVals + q]);
+    for (int q = 6; q < kBoundsVals; ++q) v[q] += partial[b * kBoundsVals + q];
+  }
+  const int t = threadIdx.x;
+  for (int q = 0; q < kBoundsVals; ++q) sh[q][t] = v[q];
+  __syncthreads();
+  for (int stride = kBoundsThreads / 2; stride > 0; stride >>= 1) {
+    if (t < stride) {
+      for (int q = 0; q < 3; ++q) sh[q][t] = fmin(sh[q][t], sh[q][t + stride]);
+      for (int q = 3; q < 6; ++q) sh[q][t] = fmax(sh[q][t], sh[q][t + stride]);
+      for (int q = 6; q < kBoundsVals; ++q) sh[q][t] += sh[q][t + stride];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    const double lo[3] = {sh[0][0], sh[1][0], sh[2][0]};
+    const double hi[3] = {sh[3][0], sh[4][0], sh[5][0]};
+    double half = __dmul_rn(0.5, __dsub_rn(hi[0], lo[0]));
+    for (int k = 1; k < 3; ++k) {
+      const double e = __dmul_rn(0.5, __dsub_rn(hi[k], lo[k]));
+      if (e > half) half = e;
+    }
+    if (half == 0.0) half = 0.5;
+    half = __dmul_rn(half, 1.0 + 1.0e-9);
+    for (int k = 0; k < 3; ++k) geometry[k] = __dmul_rn(0.5, __dadd_rn(lo[k], hi[k]));
+    geometry[3] = half;
+    const double mt = sh[6][0];
+    for (int k = 0; k < 3; ++k) geometry[4 + k] = mt != 0.0 ? sh[7 + k][0] / mt : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Morton keys
+// ---------------------------------------------------------------------------
+
+// barnes_hut.c:286-294 with every FP64 operation explicitly rounded.
+__device__ __forceinline__ uint64_t axis_code(double value, double centre, double half) {
+  double t = __dadd_rn(__ddiv_rn(__dsub_rn(value, centre), __dmul_rn(2.0, half)), 0.5);
+  if (t < 0.0) {
+    t = 0.0;
+  } else if (t >= 1.0) {
+    t = 1.0 - 1.0e-15;
+  }
+  return (uint64_t)__double2ull_rz(__dmul_rn(t, 2097152.0));
+}
+
+// Spread the low 21 bits of v to every third bit (bit b -> bit 3b).
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+  v &= 0x1fffffull;
+  v = (v | (v << 32)) & 0x001f00000000ffffull;
+  v = (v | (v << 16)) & 0x001f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__global__ void keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, size_t n,
+                            const double* __restrict__ geometry, uint64_t* __restrict__ keys,
+                            uint32_t* __restrict__ index) {
+  const double cx = geometry[0], cy = geometry[1], cz = geometry[2], h = geometry[3];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    keys[i] = spread3(axis_code(x[i], cx, h)) | (spread3(axis_code(y[i], cy, h)) << 1) |
+              (spread3(axis_code(z[i], cz, h)) << 2);
+    index[i] = (uint32_t)i;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stable LSD radix sort, 8-bit digits
+// ---------------------------------------------------------------------------
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kRadix = 256;
+
+__global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(
+    const uint64_t* __restrict__ keys, size_t n, int shift, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[kRadix];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * kSortTile;
+  for (int k = threadIdx.x; k < kSortTile; k += kSortThreads) {
+    const size_t i = base + k;
+    if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  hist[(size_t)blockIdx.x * kRadix + threadIdx.x] = h[threadIdx.x];
+}
+
+// One block: per digit, exclusive prefix over tiles (in place); digit bases into
+// hist[tiles * 256 + d].
+__global__ void __launch_bounds__(kRadix) sort_scan_kernel(uint32_t* __restrict__ hist,
+                                                           int tiles) {
+  __shared__ uint32_t tot[kRadix];
+  const int d = threadIdx.x;
+  uint32_t run = 0;
+  for (int t = 0; t < tiles; ++t) {
+    const uint32_t c = hist[(size_t)t * kRadix + d];
+    hist[(size_t)t * kRadix + d] = run;
+    run += c;
+  }
+  tot[d] = run;
+  __syncthreads();
+  // exclusive scan of the 256 digit totals (Hillis-Steele on a copy)
+  uint32_t v = run;
+  for (int off = 1; off < kRadix; off <<= 1) {
+    __syncthreads();
+    const uint32_t add = d >= off ? tot[d - off] : 0u;
+    __syncthreads();
+    v += add;
+    tot[d] = v;
+  }
+  hist[(size_t)tiles * kRadix + d] = v - run;
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
+    const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int shift,
+    const uint32_t* __restrict__ hist, int tiles, int* status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint64_t* sk = reinterpret_cast<uint64_t*>(smem);                     // kSortTile
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);           // kSortTile
+  uint32_t* wc = sv + kSortTile;                                        // kSortWarps * 256
+  uint32_t* start = wc + kSortWarps * kRadix;                           // 256
+  uint32_t* gofs = start + kRadix;                                      // 256
+
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  for (int k = t; k < kSortWarps * kRadix; k += kSortThreads) wc[k] = 0;
+  gofs[t] = hist[(size_t)tiles * kRadix + t] + hist[(size_t)blockIdx.x * kRadix + t];
+  __syncthreads();
+
+  const size_t base = (size_t)blockIdx.x * kSortTile + (size_t)w * (kSortItems * 32);
+  const unsigned lt = (1u << lane) - 1u;
+  uint64_t key[kSortItems];
+  uint32_t val[kSortItems];
+  uint32_t rank[kSortItems];
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const size_t i = base + (size_t)it * 32 + lane;
+    const bool valid = i < n;
+    key[it] = valid ? keys_in[i] : 0ull;
+    val[it] = valid ? vals_in[i] : 0u;
+    const unsigned digit = valid ? ((unsigned)(key[it] >> shift) & 0xffu) : 0x100u;
+    const unsigned peers = __match_any_sync(kFull, digit);
+    uint32_t before = 0;
+    if (valid) before = wc[w * kRadix + digit];
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) wc[w * kRadix + digit] = before + __popc(peers);
+    __syncwarp();
+    rank[it] = before + __popc(peers & lt);
+  }
+  __syncthreads();
+  {  // per digit: exclusive over warps; tile totals
+    uint32_t run = 0;
+    for (int ww = 0; ww < kSortWarps; ++ww) {
+      const uint32_t c = wc[ww * kRadix + t];
+      wc[ww * kRadix + t] = run;
+      run += c;
+    }
+    start[t] = run;
+  }
+  __syncthreads();
+  {  // exclusive scan of tile digit totals
+    const uint32_t own = start[t];
+    uint32_t v = own;
+    for (int off = 1; off < kRadix; off <<= 1) {
+      __syncthreads();
+      const uint32_t add = t >= off ? start[t - off] : 0u;
+      __syncthreads();
+      v += add;
+      start[t] = v;
+    }
+    __syncthreads();
+    start[t] = v - own;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const size_t i = base + (size_t)it * 32 + lane;
+    if (i < n) {
+      const unsigned digit = (unsigned)(key[it] >> shift) & 0xffu;
+      const uint32_t pos = start[digit] + wc[w * kRadix + digit] + rank[it];
+      if (pos < (uint32_t)kSortTile) {
+        sk[pos] = key[it];
+        sv[pos] = val[it];
+      } else {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      }
+    }
+  }
+  __syncthreads();
+  const size_t tile_base = (size_t)blockIdx.x * kSortTile;
+  const int count = (int)(n - tile_base < (size_t)kSortTile ? n - tile_base : (size_t)kSortTile);
+  for (int p = t; p < count; p += kSortThreads) {
+    const uint64_t k = sk[p];
+    const unsigned digit = (unsigned)(k >> shift) & 0xffu;
+    const size_t dst = (size_t)gofs[digit] + (size_t)(p - (int)start[digit]);
+    if (dst < n) {
+      keys_out[dst] = k;
+      vals_out[dst] = sv[p];
+    } else {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    }
+  }
+}
+
+// The reference's insertion build fails with OVERFLOW when two particles share
+// a position (barnes_hut.c:149-153: more than 128 subdivisions).  Equal
+// positions have equal keys, so after the sort they sit in one run of equal
+// keys; each particle is compared with the next kDupWindow particles of its run
+// (runs of equal 63-bit keys are otherwise rare: cells of 2^-21 of the root).
+constexpr int kDupWindow = 32;
+__global__ void duplicates_kernel(const uint64_t* __restrict__ keys,
+                                  const uint32_t* __restrict__ perm, const double* __restrict__ x,
+                                  const double* __restrict__ y, const double* __restrict__ z,
+                                  size_t n, int* status) {
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s + 1 < n;
+       s += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[s];
+    if (keys[s + 1] != k) continue;
+    const uint32_t i = perm[s];
+    if (i >= n) continue;
+    const double px = x[i], py = y[i], pz = z[i];
+    for (size_t t = s + 1; t < n && t <= s + kDupWindow && keys[t] == k; ++t) {
+      const uint32_t j = perm[t];
+      if (j < n && x[j] == px && y[j] == py && z[j] == pz) {
+        atomicOr(status, NBSP_DEVICE_ERROR_DUPLICATE_POSITION);
+        return;
+      }
+    }
+  }
+}
+
+constexpr size_t kDownsweepSmem =
+    kSortTile * 8 + kSortTile * 4 + kSortWarps * kRadix * 4 + 2 * kRadix * 4;
+
+// ---------------------------------------------------------------------------
+// gather / scatter
+// ---------------------------------------------------------------------------
+
+__global__ void gather_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, const double* __restrict__ m,
+                              const uint32_t* __restrict__ perm, size_t n,
+                              const double* __restrict__ geometry, float4* __restrict__ pos,
+                              int* status) {
+  const double cx = geometry[4], cy = geometry[5], cz = geometry[6];
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
+       s += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = perm[s];
+    if (i >= n) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      pos[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
+    }
+    pos[s] = make_float4((float)__dsub_rn(x[i], cx), (float)__dsub_rn(y[i], cy),
+                         (float)__dsub_rn(z[i], cz), (float)m[i]);
+  }
+}
+
+__global__ void scatter_kernel(const float4* __restrict__ hi, const float4* __restrict__ lo,
+                               const uint32_t* __restrict__ perm, size_t n, double g,
+                               double* __restrict__ ax, double* __restrict__ ay,
+                               double* __restrict__ az) {
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
+       s += (size_t)gridDim.x * blockDim.x) {
+    const float4 h = hi[s], l = lo[s];
+    const uint32_t i = perm[s];
+    if (i >= n) continue;  // the gather already flagged a bad permutation
+    ax[i] = g * ((double)h.x + (double)l.x);
+    ay[i] = g * ((double)h.y + (double)l.y);
+    az[i] = g * ((double)h.z + (double)l.z);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tree
+// ---------------------------------------------------------------------------
+
+// Scratch layout of one tree; binary ids: internal node i -> i (0..n-2),
+// particle leaf k -> (n-1) + k.
+struct Tree {
+  int n;
+  int2* range;        // [n-1] first, last of internal nodes
+  int2* child;        // [n-1] binary ids
+  int* delta;         // [n-1] common prefix length in bits
+  int* parent;        // [2n-1] binary parent id (root: -1)
+  int* cell;          // [2n-1] octree level of a cell node, -1 otherwise
+  int* kept;          // [2n-1] 1 if the node is in the bucketed octree
+  uint32_t* mask;     // [n]   levels of kept nodes starting at particle k
+  uint32_t* offset;   // [n+1] exclusive scan of popcounts; offset[n] = node count
+  uint32_t* block_sums;  // scan scratch
+  // octree nodes, depth-first order, capacity 2n-1
+  int4* info;         // next, begin, leaf count (0: internal), parent
+  int* level;
+  int* nchild;
+  int* arrive;
+  int* height;
+  double4* mom;       // mass, com xyz (relative to the centre of mass)
+  double* quad64;     // 6 per node: xx xy xz yy yz zz (trace-free)
+  float4* com;        // walk format: com xyz, mass
+  float* ropen2;      // (2h / theta)^2
+  float4* quad;       // 2 per node: (xx, xy, xz, yy), (yz, 0, 0, 0)
+  unsigned long long* leaves;  // [1]
+};
+
+constexpr int kScanItems = 2048;
+
+// Sub-buffers of the tree scratch, each 256-byte aligned, carved from an
+// integer base address (tree_bytes() carves from 0 to measure the layout).
+template <typename T>
+__host__ __device__ inline T* carve(uintptr_t& p, size_t count) {
+  T* out = reinterpret_cast<T*>(p);
+  p += (count * sizeof(T) + 255) & ~(size_t)255;
+  return out;
+}
+
+__host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* end) {
+  Tree t;
+  const size_t n = n_ < 2 ? 2 : n_;
+  const size_t ni = n - 1, nb = 2 * n - 1;
+  t.n = (int)n_;
+  t.range = carve<int2>(p, ni);
+  t.child = carve<int2>(p, ni);
+  t.delta = carve<int>(p, ni);
+  t.parent = carve<int>(p, nb);
+  t.cell = carve<int>(p, nb);
+  t.kept = carve<int>(p, nb);
+  t.mask = carve<uint32_t>(p, n);
+  t.offset = carve<uint32_t>(p, n + 1);
+  t.block_sums = carve<uint32_t>(p, (n + kScanItems - 1) / kScanItems + 1);
+  t.info = carve<int4>(p, nb);
+  t.level = carve<int>(p, nb);
+  t.nchild = carve<int>(p, nb);
+  t.arrive = carve<int>(p, nb);
+  t.height = carve<int>(p, nb);
+  t.mom = carve<double4>(p, nb);
+  t.quad64 = carve<double>(p, 6 * nb);
+  t.com = carve<float4>(p, nb);
+  t.ropen2 = carve<float>(p, nb);
+  t.quad = carve<float4>(p, 2 * nb);
+  t.leaves = carve<unsigned long long>(p, 1);
+  if (end != nullptr) *end = p;
+  return t;
+}
+
+inline Tree tree_view(void* base, size_t n) {
+  return tree_layout(reinterpret_cast<uintptr_t>(base), n, nullptr);
+}
+
+size_t tree_bytes(size_t n) {
+  uintptr_t end = 0;
+  tree_layout(0, n, &end);
+  return (size_t)end;
+}
+
+// Common prefix length of sorted keys i and j in bits (Karras 2012, with the
+// index as tie breaker); -1 outside [0, n).
+__device__ __forceinline__ int prefix(const uint64_t* __restrict__ keys, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const uint64_t a = keys[i], b = keys[j];
+  if (a != b) return __clzll(a ^ b) - 1;  // keys use the low 63 bits
+  return 63 + __clz((unsigned)(i ^ j));
+}
+
+__global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, Tree t, int* status) {
+  const int n = t.n;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = prefix(keys, n, i, i + 1) - prefix(keys, n, i, i - 1) >= 0 ? 1 : -1;
+  const int dmin = prefix(keys, n, i, i - d);
+  int lmax = 2;
+  while (prefix(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int step = lmax >> 1; step >= 1; step >>= 1)
+    if (prefix(keys, n, i, i + (l + step) * d) > dmin) l += step;
+  const int j = i + l * d;
+  const int dnode = prefix(keys, n, i, j);
+  int s = 0;
+  int div = 2;
+  for (;;) {
+    const int step = (l + div - 1) / div;
+    if (prefix(keys, n, i, i + (s + step) * d) > dnode) s += step;
+    if (step <= 1) break;
+    div <<= 1;
+  }
+  const int gamma = i + s * d + (d < 0 ? -1 : 0);
+  const int first = min(i, j), last = max(i, j);
+  if (first < 0 || last >= n || gamma < first || gamma >= last) {
+    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    return;
+  }
+  const int left = first == gamma ? (n - 1) + gamma : gamma;
+  const int right = last == gamma + 1 ? (n - 1) + gamma + 1 : gamma + 1;
+  t.range[i] = make_int2(first, last);
+  t.child[i] = make_int2(left, right);
+  t.delta[i] = dnode;
+  t.parent[left] = i;
+  t.parent[right] = i;
+  if (i == 0) t.parent[0] = -1;
+}
+
+__device__ __forceinline__ int level_of_delta(int delta) { return min(delta / 3, 21); }
+
+// Octree cell nodes among the binary nodes (see file comment).
+__global__ void cells_kernel(Tree t, int* status) {
+  const int n = t.n;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= 2 * n - 1) return;
+  int cell = -1;
+  const int p = t.parent[b];
+  if (b != 0 && (p < 0 || p >= n - 1)) {  // every non-root node has an internal parent
+    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    t.cell[b] = -1;
+    return;
+  }
+  if (b < n - 1) {
+    const int lvl = level_of_delta(t.delta[b]);
+    if (b == 0 || level_of_delta(t.delta[p]) < lvl) cell = lvl;
+  } else {
+    if (level_of_delta(t.delta[p]) <= 20) cell = 22;
+  }
+  t.cell[b] = cell;
+}
+
+__device__ __forceinline__ int first_of(const Tree& t, int b) {
+  return b < t.n - 1 ? t.range[b].x : b - (t.n - 1);
+}
+__device__ __forceinline__ int last_of(const Tree& t, int b) {
+  return b < t.n - 1 ? t.range[b].y : b - (t.n - 1);
+}
+
+// Octree parent of a cell node: the nearest binary ancestor that is a cell.
+__device__ __forceinline__ int octree_parent(const Tree& t, int b, int* status) {
+  int p = t.parent[b];
+  for (int guard = 0; p >= 0 && t.cell[p] < 0; ++guard) {
+    if (guard > 96 || p >= t.n - 1) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return -1;
+    }
+    p = t.parent[p];
+  }
+  if (p >= t.n - 1) {
+    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    return -1;
+  }
+  return p;
+}
+
+__global__ void keep_kernel(Tree t, int leaf_capacity, int* status) {
+  const int n = t.n;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= 2 * n - 1) return;
+  int kept = 0;
+  const int lvl = t.cell[b];
+  if (lvl >= 0) {
+    if (b == 0) {
+      kept = 1;
+    } else {
+      const int p = octree_parent(t, b, status);
+      kept = p >= 0 && (last_of(t, p) - first_of(t, p) + 1) > leaf_capacity;
+    }
+    if (kept) atomicOr(&t.mask[first_of(t, b)], 1u << lvl);
+  }
+  t.kept[b] = kept;
+}
+
+// Exclusive scan of popc(mask[k]) into offset[0..n].
+__global__ void scan_reduce_kernel(Tree t) {
+  __shared__ uint32_t sh[256];
+  const int n = t.n;
+  const size_t base = (size_t)blockIdx.x * kScanItems;
+  uint32_t s = 0;
+  for (int k = threadIdx.x; k < kScanItems; k += 256) {
+    const size_t i = base + k;
+    if (i < (size_t)n) s += __popc(t.mask[i]);
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int stride = 128; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) sh[threadIdx.x] += sh[threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) t.block_sums[blockIdx.x] = sh[0];
+}
+
+__global__ void scan_blocks_kernel(Tree t, int blocks) {
+  if (threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (int b = 0; b < blocks; ++b) {
+    const uint32_t c = t.block_sums[b];
+    t.block_sums[b] = run;
+    run += c;
+  }
+  t.offset[t.n] = run;
+}
+
+__global__ void scan_apply_kernel(Tree t) {
+  __shared__ uint32_t sh[256];
+  const int n = t.n;
+  const size_t base = (size_t)blockIdx.x * kScanItems;
+  constexpr int per = kScanItems / 256;  // 8 contiguous items per thread
+  uint32_t v[per];
+  uint32_t s = 0;
+  for (int k = 0; k < per; ++k) {
+    const size_t i = base + (size_t)threadIdx.x * per + k;
+    v[k] = i < (size_t)n ? __popc(t.mask[i]) : 0u;
+    s += v[k];
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  uint32_t incl = s;
+  for (int off = 1; off < 256; off <<= 1) {
+    const uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+    __syncthreads();
+    incl += add;
+    sh[threadIdx.x] = incl;
+    __syncthreads();
+  }
+  uint32_t run = t.block_sums[blockIdx.x] + incl - s;
+  for (int k = 0; k < per; ++k) {
+    const size_t i = base + (size_t)threadIdx.x * per + k;
+    if (i < (size_t)n) t.offset[i] = run;
+    run += v[k];
+  }
+}
+
+__device__ __forceinline__ int dfs_index(const Tree& t, int begin, int lvl) {
+  return (int)(t.offset[begin] + __popc(t.mask[begin] & ((1u << lvl) - 1u)));
+}
+
+__global__ void place_kernel(Tree t, int leaf_capacity, int* status) {
+  const int n = t.n;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= 2 * n - 1 || !t.kept[b]) return;
+  const int lvl = t.cell[b];
+  const int begin = first_of(t, b), end = last_of(t, b) + 1;
+  const int count = end - begin;
+  const int node = dfs_index(t, begin, lvl);
+  const int total = (int)t.offset[n];
+  if (node < 0 || node >= total || total > 2 * n - 1) {
+    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    return;
+  }
+  const int next = end >= n ? total : (int)t.offset[end];
+  const bool leaf = b >= n - 1 || count <= leaf_capacity || lvl >= 21;
+  int parent_node = -1;
+  if (b != 0) {
+    const int p = octree_parent(t, b, status);
+    if (p < 0) return;
+    parent_node = dfs_index(t, first_of(t, p), t.cell[p]);
+    if (parent_node < 0 || parent_node >= node) {  // parents precede children in DFS order
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return;
+    }
+    atomicAdd(&t.nchild[parent_node], 1);
+  }
+  t.info[node] = make_int4(next, begin, leaf ? count : 0, parent_node);
+  t.level[node] = lvl;
+  t.arrive[node] = 0;
+  t.height[node] = 1;
+  if (leaf) atomicAdd(t.leaves, 1ull);
+}
+
+// Trace-free quadrupole accumulation helpers (FP64).
+struct Moments {
+  double m, cx, cy, cz;
+  double q[6];  // xx xy xz yy yz zz
+};
+
+__device__ void finish_node(const Tree& t, int node, const Moments& mo, double root_size,
+                            double inv_theta2, int lvl) {
+  t.mom[node] = make_double4(mo.m, mo.cx, mo.cy, mo.cz);
+  for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
+  t.com[node] = make_float4((float)mo.cx, (float)mo.cy, (float)mo.cz, (float)mo.m);
+  // cell side 2h = root side / 2^lvl ; accept when (2h)^2 < theta^2 d^2
+  const double side = ldexp(root_size, -min(lvl, 21));
+  const double r2 = side * side * inv_theta2;
+  t.ropen2[node] = (float)r2;
+  t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
+  t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
+}
+
+// L2-coherent load of a double4 written by another thread of this grid.
+__device__ __forceinline__ double4 ldcg_d4(const double4* p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Bottom-up moments: leaves sum their particles, the last child to finish
+// combines its parent (children read in depth-first order: deterministic).
+__global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
+                               const double* __restrict__ geometry, double inv_theta2,
+                               int* status) {
+  const int total = (int)t.offset[t.n];
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= total) return;
+  const int4 info = t.info[node];
+  if (info.z == 0) return;  // internal nodes are finished by their last child
+  if (info.z < 0 || info.y < 0 || info.y + info.z > t.n) {
+    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    return;
+  }
+  const double root_size = 2.0 * geometry[3];
+  Moments mo;
+  {
+    double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int j = info.y; j < info.y + info.z; ++j) {
+      const float4 p = pos[j];
+      m += (double)p.w;
+      sx += (double)p.w * (double)p.x;
+      sy += (double)p.w * (double)p.y;
+      sz += (double)p.w * (double)p.z;
+    }
+    mo.m = m;
+    mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
+    mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
+    mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
+    for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
+    for (int j = info.y; j < info.y + info.z; ++j) {
+      const float4 p = pos[j];
+      const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double w = (double)p.w;
+      mo.q[0] += w * (3.0 * dx * dx - r2);
+      mo.q[1] += w * (3.0 * dx * dy);
+      mo.q[2] += w * (3.0 * dx * dz);
+      mo.q[3] += w * (3.0 * dy * dy - r2);
+      mo.q[4] += w * (3.0 * dy * dz);
+      mo.q[5] += w * (3.0 * dz * dz - r2);
+    }
+  }
+  finish_node(t, node, mo, root_size, inv_theta2, t.level[node]);
+  int h = 1;
+  int parent = info.w;
+  for (int climb = 0; parent >= 0; ++climb) {
+    if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return;
+    }
+    __threadfence();
+    const int arrived = atomicAdd(&t.arrive[parent], 1);
+    if (arrived != __ldcg(&t.nchild[parent]) - 1) return;
+    __threadfence();
+    // combine children of `parent` (first child = parent + 1, then skip links)
+    const int4 pinfo = __ldcg(&t.info[parent]);
+    double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    int hmax = 0;
+    int c = parent + 1, guard = 0;
+    while (c != pinfo.x) {
+      if (++guard > 8 || c < 0 || c >= total) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        return;
+      }
+      const double4 cm = ldcg_d4(&t.mom[c]);
+      m += cm.x;
+      sx += cm.x * cm.y;
+      sy += cm.x * cm.z;
+      sz += cm.x * cm.w;
+      hmax = max(hmax, __ldcg(&t.height[c]));
+      c = __ldcg(&t.info[c]).x;
+    }
+    Moments pm;
+    pm.m = m;
+    pm.cx = m != 0.0 ? sx / m : 0.0;
+    pm.cy = m != 0.0 ? sy / m : 0.0;
+    pm.cz = m != 0.0 ? sz / m : 0.0;
+    for (int k = 0; k < 6; ++k) pm.q[k] = 0.0;
+    c = parent + 1;
+    while (c != pinfo.x) {
+      const double4 cm = ldcg_d4(&t.mom[c]);
+      const double dx = cm.y - pm.cx, dy = cm.z - pm.cy, dz = cm.w - pm.cz;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double w = cm.x;
+      pm.q[0] += __ldcg(&t.quad64[6 * c + 0]) + w * (3.0 * dx * dx - r2);
+      pm.q[1] += __ldcg(&t.quad64[6 * c + 1]) + w * (3.0 * dx * dy);
+      pm.q[2] += __ldcg(&t.quad64[6 * c + 2]) + w * (3.0 * dx * dz);
+      pm.q[3] += __ldcg(&t.quad64[6 * c + 3]) + w * (3.0 * dy * dy - r2);
+      pm.q[4] += __ldcg(&t.quad64[6 * c + 4]) + w * (3.0 * dy * dz);
+      pm.q[5] += __ldcg(&t.quad64[6 * c + 5]) + w * (3.0 * dz * dz - r2);
+      c = __ldcg(&t.info[c]).x;
+    }
+    h = hmax + 1;
+    t.height[parent] = h;
+    finish_node(t, parent, pm, root_size, inv_theta2, __ldcg(&t.level[parent]));
+    parent = pinfo.w;
+  }
+}
+
+__device__ __forceinline__ float rsqrt_mufu(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void fold(float& hi, float& lo, float a) {
+  const float s = __fadd_rn(hi, a);
+  const float bp = __fsub_rn(s, hi);
+  const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(a, bp));
+  hi = s;
+  lo = __fadd_rn(lo, err);
+}
+
+constexpr int kWalkThreads = 256;
+
+// Warp-cooperative stackless walk: the 32 lanes own 32 Morton-consecutive
+// targets and visit the same node sequence; a cell is opened when any lane's
+// opening test fails (so every lane's own test holds for every cell it
+// accepts), otherwise all lanes apply its multipole and skip its subtree.
+template <int ORDER>
+__global__ void __launch_bounds__(kWalkThreads) walk_kernel(
+    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
+    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
+  if (warp * 32 >= n) return;
+  const int s = warp * 32 + lane;
+  const bool active = s < n;
+  const float4 p = pos[active ? s : n - 1];
+  const int total = (int)t.offset[n];
+  const int limit = 2 * total + 64;
+
+  float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+  float px = 0.f, py = 0.f, pz = 0.f;
+  int pending = 0;
+  unsigned approx = 0, exact = 0;
+  int node = 0, steps = 0;
+  while ((unsigned)node < (unsigned)total) {
+    if (++steps > limit) {
+      if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
+      break;
+    }
+    const int4 info = t.info[node];
+    if (info.z < 0 || info.y < 0 || info.y + info.z > n || info.x <= node) {
+      if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      break;
+    }
+    if (info.z > 0) {
+      const int j1 = info.y + info.z;
+      for (int j = info.y; j < j1; ++j) {
+        const float4 q = pos[j];
+        const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        const float rinv = j == s ? 0.f : rsqrt_mufu(r2);  // barnes_hut.c:572
+        const float w = q.w * (rinv * rinv * rinv);
+        px = fmaf(w, dx, px);
+        py = fmaf(w, dy, py);
+        pz = fmaf(w, dz, pz);
+      }
+      exact += active ? (unsigned)(info.z - ((s >= info.y && s < j1) ? 1 : 0)) : 0u;
+      pending += info.z;
+      node = info.x;
+    } else {
+      const float4 c = t.com[node];
+      const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const bool open = active && !(d2 > t.ropen2[node]);
+      if (__any_sync(kFull, open)) {
+        node = node + 1;
+        continue;
+      }
+      const float r2 = d2 + eps2;
+      const float rinv = rsqrt_mufu(r2);
+      const float rinv2 = rinv * rinv;
+      const float rinv3 = rinv * rinv2;
+      float w = c.w * rinv3;
+      if (ORDER == 2) {
+        const float4 qa = t.quad[2 * node];
+        const float qyz = t.quad[2 * node + 1].x;
+        const float qzz = -qa.x - qa.w;
+        // Q d and d.Q.d, d = com - target
+        const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
+        const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qyz * dz));
+        const float qdz = fmaf(qa.z, dx, fmaf(qyz, dy, qzz * dz));
+        const float dqd = fmaf(dx, qdx, fmaf(dy, qdy, dz * qdz));
+        const float rinv5 = rinv3 * rinv2;
+        const float rinv7 = rinv5 * rinv2;
+        // a = G [ M d / r^3 - Q d / r^5 + 5/2 (d.Q.d) d / r^7 ]
+        w = fmaf(2.5f * dqd, rinv7, w);
+        px = fmaf(-qdx, rinv5, px);
+        py = fmaf(-qdy, rinv5, py);
+        pz = fmaf(-qdz, rinv5, pz);
+      }
+      px = fmaf(w, dx, px);
+      py = fmaf(w, dy, py);
+      pz = fmaf(w, dz, pz);
+      approx += active ? 1u : 0u;
+      pending += 1;
+      node = info.x;
+    }
+    if (pending >= 32) {
+      fold(hx, lx, px);
+      fold(hy, ly, py);
+      fold(hz, lz, pz);
+      px = py = pz = 0.f;
+      pending = 0;
+    }
+  }
+  fold(hx, lx, px);
+  fold(hy, ly, py);
+  fold(hz, lz, pz);
+  if (active) {
+    acc_hi[s] = make_float4(hx, hy, hz, 0.f);
+    acc_lo[s] = make_float4(lx, ly, lz, 0.f);
+  }
+  unsigned long long a = approx, e = exact;
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_down_sync(kFull, a, off);
+    e += __shfl_down_sync(kFull, e, off);
+  }
+  if (lane == 0) {
+    atomicAdd(&counters[0], a);
+    atomicAdd(&counters[1], e);
+  }
+}
+
+__global__ void tree_counts_kernel(Tree t, unsigned long long* counters) {
+  if (threadIdx.x != 0) return;
+  counters[2] = t.offset[t.n];
+  counters[3] = *t.leaves;
+  counters[4] = (unsigned long long)t.height[0];
+}
+
+int grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 64) b = 148 * 64;
+  return (int)b;
+}
+
+}  // namespace
+
+extern "C" {
+
+void nbsp_bh_bounds(const double* x, const double* y, const double* z, const double* m, size_t n,
+                    double* partial, double* geometry, int* status, cudaStream_t stream) {
+  size_t blocks = (n + kBoundsThreads - 1) / kBoundsThreads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > (size_t)kBoundsBlocks) blocks = kBoundsBlocks;
+  NBSP_COUNT_LAUNCH(1), bounds_kernel<<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(x, y, z, m, n, partial, status);
+  NBSP_COUNT_LAUNCH(1), bounds_final_kernel<<<1, kBoundsThreads, 0, stream>>>(partial, (int)blocks, geometry);
+}
+
+void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
+                  const double* geometry, uint64_t* keys, uint32_t* index, cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), keys_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, y, z, n, geometry, keys, index);
+}
+
+void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt, uint32_t* index_alt,
+                  size_t n, uint32_t* hist, int* status, cudaStream_t stream) {
+  cudaFuncSetAttribute(sort_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kDownsweepSmem);
+  const int tiles = (int)((n + kSortTile - 1) / kSortTile);
+  uint64_t* kin = keys;
+  uint32_t* vin = index;
+  uint64_t* kout = keys_alt;
+  uint32_t* vout = index_alt;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 8 * pass;
+    NBSP_COUNT_LAUNCH(1), sort_upsweep_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, hist);
+    NBSP_COUNT_LAUNCH(1), sort_scan_kernel<<<1, kRadix, 0, stream>>>(hist, tiles);
+    NBSP_COUNT_LAUNCH(1), sort_downsweep_kernel<<<tiles, kSortThreads, kDownsweepSmem, stream>>>(
+        kin, vin, kout, vout, n, shift, hist, tiles, status);
+    uint64_t* tk = kin;
+    kin = kout;
+    kout = tk;
+    uint32_t* tv = vin;
+    vin = vout;
+    vout = tv;
+  }
+  // 8 passes (even): the result is back in (keys, index)
+}
+
+void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double* x,
+                        const double* y, const double* z, size_t n, int* status,
+                        cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), duplicates_kernel<<<grid_for(n, 256), 256, 0, stream>>>(keys, perm, x, y, z, n, status);
+}
+
+void nbsp_bh_gather(const double* x, const double* y, const double* z, const double* m,
+                    const uint32_t* perm, size_t n, const double* geometry, void* pos4,
+                    int* status, cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, y, z, m, perm, n, geometry,
+                                                      (float4*)pos4, status);
+}
+
+size_t nbsp_bh_tree_bytes(size_t n) { return tree_bytes(n); }
+
+void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree, int* status,
+                   cudaStream_t stream) {
+  Tree t = tree_view(tree, n);
+  const size_t nb = 2 * n - 1;
+  cudaMemsetAsync(t.mask, 0, n * sizeof(uint32_t), stream);
+  cudaMemsetAsync(t.nchild, 0, nb * sizeof(int), stream);
+  cudaMemsetAsync(t.leaves, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(t.parent, 0xff, nb * sizeof(int), stream);  // -1: not yet linked
+  if (n >= 2)
+    NBSP_COUNT_LAUNCH(1), radix_tree_kernel<<<(unsigned)((n - 1 + 255) / 256), 256, 0, stream>>>(keys, t, status);
+  NBSP_COUNT_LAUNCH(1), cells_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, status);
+  NBSP_COUNT_LAUNCH(1), keep_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
+  const int blocks = (int)((n + kScanItems - 1) / kScanItems);
+  NBSP_COUNT_LAUNCH(1), scan_reduce_kernel<<<blocks, 256, 0, stream>>>(t);
+  NBSP_COUNT_LAUNCH(1), scan_blocks_kernel<<<1, 32, 0, stream>>>(t, blocks);
+  NBSP_COUNT_LAUNCH(1), scan_apply_kernel<<<blocks, 256, 0, stream>>>(t);
+  NBSP_COUNT_LAUNCH(1), place_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
+}
+
+void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry, double theta, int order,
+                     void* tree, int* status, cudaStream_t stream) {
+  (void)order;
+  Tree t = tree_view(tree, n);
+  const size_t nb = 2 * n - 1;
+  const double inv_theta2 = theta > 0.0 ? 1.0 / (theta * theta) : INFINITY;
+  NBSP_COUNT_LAUNCH(1), moments_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>((const float4*)pos4, t,
+                                                                   geometry, inv_theta2, status);
+}
+
+void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, float eps2,
+                  void* acc_hi, void* acc_lo, unsigned long long* counters, int* status,
+                  cudaStream_t stream) {
+  Tree t = tree_view(const_cast<void*>(tree), n);
+  const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
+  if (order == 2) {
+    NBSP_COUNT_LAUNCH(1), walk_kernel<2><<<blocks, kWalkThreads, 0, stream>>>((const float4*)pos4, (int)n, t, eps2,
+                                                        (float4*)acc_hi, (float4*)acc_lo, counters,
+                                                        status);
+  } else {
+    NBSP_COUNT_LAUNCH(1), walk_kernel<1><<<blocks, kWalkThreads, 0, stream>>>((const float4*)pos4, (int)n, t, eps2,
+                                                        (float4*)acc_hi, (float4*)acc_lo, counters,
+                                                        status);
+  }
+}
+
+void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* perm, size_t n,
+                     double g, double* ax, double* ay, double* az, cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), scatter_kernel<<<grid_for(n, 256), 256, 0, stream>>>((const float4*)acc_hi,
+                                                       (const float4*)acc_lo, perm, n, g, ax, ay,
+                                                       az);
+}
+
+void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,
+                         cudaStream_t stream) {
+  Tree t = tree_view(const_cast<void*>(tree), n);
+  NBSP_COUNT_LAUNCH(1), tree_counts_kernel<<<1, 32, 0, stream>>>(t, counters);
+}
+
+}  // extern "C"

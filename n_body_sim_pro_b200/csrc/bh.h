@@ -1,0 +1,129 @@
+/*
+ * GPU Barnes-Hut: host orchestration (bh_host.c, C17) and kernel launchers
+ * (bh.cu).  Internal; hidden visibility.
+ *
+ * Pipeline per force evaluation (all on one stream, no host synchronisation):
+ *   bounds      FP64 bbox -> root cube (barnes_hut.c:453-483) + centre of mass
+ *   keys        63-bit Morton keys, bit-exact with barnes_hut.c:286-305
+ *   sort        stable LSD radix sort, 8 x 8-bit digits (same permutation as
+ *               the reference's 3 x 21-bit LSD sort, barnes_hut.c:312-339)
+ *   gather      float4 (x - com, m) in Morton order
+ *   build       binary radix tree over the sorted keys (one thread per
+ *               internal node), collapsed to a path-compressed octree with
+ *               leaf buckets, laid out in depth-first order with skip links
+ *   moments     bottom-up monopole + trace-free quadrupole in FP64
+ *   walk        warp-cooperative stackless walk, opening test
+ *               (2h)^2 < theta^2 d^2 to the cell centre of mass
+ *   scatter     a[perm[s]] = G * a_sorted[s] in FP64
+ */
+#ifndef NBSP_BH_H
+#define NBSP_BH_H
+
+#include "n_body_sim_pro_cuda.h"
+#include "internal.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBSP_BH_MAX_LEAF 64
+
+typedef struct NbspBarnesHut NbspBarnesHut;
+
+typedef struct NbspBarnesHutParams {
+    double theta;
+    double gravitational_constant;
+    double softening_squared;
+    int multipole_order;
+    int leaf_capacity;
+} NbspBarnesHutParams;
+
+typedef struct NbspBarnesHutState {
+    const double *x, *y, *z, *m;
+    double *ax, *ay, *az;
+    size_t n;
+} NbspBarnesHutState;
+
+/* Enqueue one full Barnes-Hut force evaluation; accelerations into s->ax/ay/az.
+ * Statistics and phase timings of the evaluation are copied into *stats and
+ * *timings by nbsp_bh_collect after the stream has been synchronised. */
+NBSP_HIDDEN NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** bh,
+                                                    const NbspBarnesHutState* s,
+                                                    const NbspBarnesHutParams* p, int* status,
+                                                    cudaStream_t stream,
+                                                    NBodySimProBarnesHutStats* stats,
+                                                    NBodySimProCudaTimings* timings,
+                                                    NBodySimProError* error);
+
+/* After a stream synchronisation: fill stats / timings of the last evaluation. */
+NBSP_HIDDEN void nbsp_bh_collect(NbspBarnesHut* bh, NBodySimProBarnesHutStats* stats,
+                                 NBodySimProCudaTimings* timings);
+
+/* Keys + sort only; copies the sorted keys / permutation / root to the host (synchronises). */
+NBSP_HIDDEN NBodySimProStatus nbsp_bh_morton(NbspBarnesHut** bh, const NbspBarnesHutState* s,
+                                             int* status, cudaStream_t stream,
+                                             uint64_t* keys_sorted, uint64_t* permutation,
+                                             double* root, NBodySimProError* error);
+
+NBSP_HIDDEN void nbsp_bh_destroy(NbspBarnesHut* bh);
+
+/* ---- kernel launchers (bh.cu) -------------------------------------------- */
+
+/* bbox + centre of mass: geometry[0..3] = root centre xyz + half size (bit-exact
+ * with the reference), geometry[4..6] = centre of mass.  partial >= 1024*10 doubles. */
+NBSP_HIDDEN void nbsp_bh_bounds(const double* x, const double* y, const double* z,
+                                const double* m, size_t n, double* partial, double* geometry,
+                                int* status, cudaStream_t stream);
+
+NBSP_HIDDEN void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
+                              const double* geometry, uint64_t* keys, uint32_t* index,
+                              cudaStream_t stream);
+
+/* Stable LSD radix sort of (keys, index) by all 64 key bits.  `keys`/`index`
+ * are ping-ponged with `keys_alt`/`index_alt`; the sorted result ends in the
+ * first pair.  `hist` >= 256 * ceil(n / 4096) + 256 words. */
+NBSP_HIDDEN void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt,
+                              uint32_t* index_alt, size_t n, uint32_t* hist, int* status,
+                              cudaStream_t stream);
+
+/* Flag NBSP_DEVICE_ERROR_DUPLICATE_POSITION when two particles share a position. */
+NBSP_HIDDEN void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double* x,
+                                    const double* y, const double* z, size_t n, int* status,
+                                    cudaStream_t stream);
+
+NBSP_HIDDEN void nbsp_bh_gather(const double* x, const double* y, const double* z,
+                                const double* m, const uint32_t* perm, size_t n,
+                                const double* geometry, void* pos4, int* status,
+                                cudaStream_t stream);
+
+/* Device-side layout of the tree build scratch; sized by nbsp_bh_tree_bytes. */
+NBSP_HIDDEN size_t nbsp_bh_tree_bytes(size_t n);
+
+/* Build the octree from the sorted keys. `tree` is nbsp_bh_tree_bytes(n) bytes. */
+NBSP_HIDDEN void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree,
+                               int* status, cudaStream_t stream);
+
+/* Moments + walk-format node records.  order 1 or 2. */
+NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry,
+                                 double theta, int order, void* tree, int* status,
+                                 cudaStream_t stream);
+
+/* Walk: a_sorted (float4 hi, lo per target) and interaction counters. */
+NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order,
+                              float softening_squared, void* acc_hi, void* acc_lo,
+                              unsigned long long* counters, int* status, cudaStream_t stream);
+
+/* a[perm[s]] = G * (hi + lo)[s] */
+NBSP_HIDDEN void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* perm,
+                                 size_t n, double gravitational_constant, double* ax, double* ay,
+                                 double* az, cudaStream_t stream);
+
+/* Copy node_count, leaf_count and depth of the tree to counters[2..4]. */
+NBSP_HIDDEN void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,
+                                     cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,234 @@
+/*
+ * Host orchestration of the GPU Barnes-Hut force evaluation (C17).
+ * Buffer management and the order of the kernel launches of bh.cu; replaces
+ * n_body_sim_pro_barnes_hut_compute_acceleration (src/c/barnes_hut/barnes_hut.c:638-690)
+ * and its timing/statistics bookkeeping (:648-688, :255-283).
+ */
+#include "bh.h"
+
+#include <cuda_runtime_api.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { BH_EVENTS = 8, BH_COUNTERS = 8 };
+
+struct NbspBarnesHut {
+    size_t capacity;
+    double* partial;    /* 1024 * 10 */
+    double* geometry;   /* 8 */
+    uint64_t* keys;
+    uint64_t* keys_alt;
+    uint32_t* index;
+    uint32_t* index_alt;
+    uint32_t* hist;
+    void* pos4;
+    void* tree;
+    void* acc_hi;
+    void* acc_lo;
+    unsigned long long* counters;       /* device */
+    unsigned long long* host_counters;  /* pinned */
+    cudaEvent_t events[BH_EVENTS];
+    int timed;                          /* events hold a full evaluation */
+};
+
+static NBodySimProStatus bh_fail(NBodySimProError* error, NBodySimProStatus status,
+                                 const char* file, int line, const char* message) {
+    if (error != NULL) {
+        error->status = status;
+        error->source_file = file;
+        error->source_line = line;
+        snprintf(error->message, sizeof(error->message), "%s", message);
+    }
+    return status;
+}
+
+static NBodySimProStatus bh_cuda(NBodySimProError* error, cudaError_t code, const char* what,
+                                 int line) {
+    char text[256];
+    snprintf(text, sizeof(text), "%s: %s", what, cudaGetErrorString(code));
+    return bh_fail(error,
+                   code == cudaErrorMemoryAllocation ? N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY
+                                                     : N_BODY_SIM_PRO_STATUS_INVALID_STATE,
+                   __FILE__, line, text);
+}
+
+#define BH_TRY(call)                                                     \
+    do {                                                                 \
+        cudaError_t bh_try_code = (call);                                \
+        if (bh_try_code != cudaSuccess)                                  \
+            return bh_cuda(error, bh_try_code, #call, __LINE__);         \
+    } while (0)
+
+static void release_buffers(NbspBarnesHut* b) {
+    void* buffers[] = {b->partial, b->geometry, b->keys, b->keys_alt, b->index, b->index_alt,
+                       b->hist, b->pos4, b->tree, b->acc_hi, b->acc_lo};
+    for (size_t k = 0; k < sizeof(buffers) / sizeof(buffers[0]); ++k) cudaFree(buffers[k]);
+    b->partial = b->geometry = NULL;
+    b->keys = b->keys_alt = NULL;
+    b->index = b->index_alt = NULL;
+    b->hist = NULL;
+    b->pos4 = b->tree = b->acc_hi = b->acc_lo = NULL;
+    b->capacity = 0;
+}
+
+void nbsp_bh_destroy(NbspBarnesHut* b) {
+    if (b == NULL) return;
+    release_buffers(b);
+    cudaFree(b->counters);
+    cudaFreeHost(b->host_counters);
+    for (int k = 0; k < BH_EVENTS; ++k)
+        if (b->events[k] != NULL) cudaEventDestroy(b->events[k]);
+    free(b);
+}
+
+static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProError* error) {
+    NbspBarnesHut* b = *handle;
+    if (b == NULL) {
+        b = (NbspBarnesHut*)calloc(1, sizeof(*b));
+        if (b == NULL)
+            return bh_fail(error, N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY, __FILE__, __LINE__,
+                           "failed to allocate Barnes-Hut context");
+        *handle = b;
+        for (int k = 0; k < BH_EVENTS; ++k) BH_TRY(cudaEventCreate(&b->events[k]));
+        BH_TRY(cudaMalloc((void**)&b->counters, BH_COUNTERS * sizeof(unsigned long long)));
+        BH_TRY(cudaMallocHost((void**)&b->host_counters, BH_COUNTERS * sizeof(unsigned long long)));
+        memset(b->host_counters, 0, BH_COUNTERS * sizeof(unsigned long long));
+    }
+    if (n <= b->capacity) return N_BODY_SIM_PRO_STATUS_OK;
+    release_buffers(b);
+    const size_t cap = n < 1024 ? 1024 : n;
+    const size_t tiles = (cap + 4095) / 4096;
+    BH_TRY(cudaMalloc((void**)&b->partial, 1024 * 10 * sizeof(double)));
+    BH_TRY(cudaMalloc((void**)&b->geometry, 8 * sizeof(double)));
+    BH_TRY(cudaMalloc((void**)&b->keys, cap * sizeof(uint64_t)));
+    BH_TRY(cudaMalloc((void**)&b->keys_alt, cap * sizeof(uint64_t)));
+    BH_TRY(cudaMalloc((void**)&b->index, cap * sizeof(uint32_t)));
+    BH_TRY(cudaMalloc((void**)&b->index_alt, cap * sizeof(uint32_t)));
+    BH_TRY(cudaMalloc((void**)&b->hist, (256 * tiles + 256) * sizeof(uint32_t)));
+    BH_TRY(cudaMalloc(&b->pos4, cap * 16));
+    BH_TRY(cudaMalloc(&b->tree, nbsp_bh_tree_bytes(cap)));
+    BH_TRY(cudaMalloc(&b->acc_hi, cap * 16));
+    BH_TRY(cudaMalloc(&b->acc_lo, cap * 16));
+    b->capacity = cap;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, int* status,
+                                cudaStream_t stream) {
+    nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status, stream);
+    cudaEventRecord(b->events[1], stream);
+    nbsp_bh_keys(s->x, s->y, s->z, s->n, b->geometry, b->keys, b->index, stream);
+    cudaEventRecord(b->events[2], stream);
+    nbsp_bh_sort(b->keys, b->index, b->keys_alt, b->index_alt, s->n, b->hist, status, stream);
+    cudaEventRecord(b->events[3], stream);
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnesHutState* s,
+                                        const NbspBarnesHutParams* p, int* status,
+                                        cudaStream_t stream, NBodySimProBarnesHutStats* stats,
+                                        NBodySimProCudaTimings* timings,
+                                        NBodySimProError* error) {
+    NBodySimProStatus st = ensure(handle, s->n, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    NbspBarnesHut* b = *handle;
+    const size_t n = s->n;
+    if (n == 1) { /* a lone particle feels nothing; no tree to walk */
+        BH_TRY(cudaMemsetAsync(s->ax, 0, sizeof(double), stream));
+        BH_TRY(cudaMemsetAsync(s->ay, 0, sizeof(double), stream));
+        BH_TRY(cudaMemsetAsync(s->az, 0, sizeof(double), stream));
+        memset(stats, 0, sizeof(*stats));
+        stats->node_count = stats->leaf_count = stats->maximum_depth = 1;
+        b->timed = 0;
+        return N_BODY_SIM_PRO_STATUS_OK;
+    }
+    BH_TRY(cudaMemsetAsync(b->counters, 0, BH_COUNTERS * sizeof(unsigned long long), stream));
+    cudaEventRecord(b->events[0], stream);
+    morton(b, s, status, stream);
+    nbsp_bh_duplicates(b->keys, b->index, s->x, s->y, s->z, n, status, stream);
+    nbsp_bh_gather(s->x, s->y, s->z, s->m, b->index, n, b->geometry, b->pos4, status, stream);
+    nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
+    cudaEventRecord(b->events[4], stream);
+    nbsp_bh_moments(b->pos4, n, b->geometry, p->theta, p->multipole_order, b->tree, status, stream);
+    cudaEventRecord(b->events[5], stream);
+    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, (float)p->softening_squared, b->acc_hi,
+                 b->acc_lo, b->counters, status, stream);
+    cudaEventRecord(b->events[6], stream);
+    nbsp_bh_scatter(b->acc_hi, b->acc_lo, b->index, n, p->gravitational_constant, s->ax, s->ay,
+                    s->az, stream);
+    nbsp_bh_tree_counts(b->tree, n, b->counters, stream);
+    cudaEventRecord(b->events[7], stream);
+    BH_TRY(cudaGetLastError());
+    BH_TRY(cudaMemcpyAsync(b->host_counters, b->counters, BH_COUNTERS * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, stream));
+    b->timed = 1;
+    /* stats/timings are read after the caller synchronises */
+    (void)stats;
+    (void)timings;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+static double elapsed(const NbspBarnesHut* b, int from, int to) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, b->events[from], b->events[to]) != cudaSuccess) return 0.0;
+    return (double)ms;
+}
+
+void nbsp_bh_collect(NbspBarnesHut* b, NBodySimProBarnesHutStats* stats,
+                     NBodySimProCudaTimings* timings) {
+    if (b == NULL || !b->timed) return;
+    const unsigned long long* c = b->host_counters;
+    stats->accepted_approximations = (size_t)c[0];
+    stats->exact_interactions = (size_t)c[1];
+    stats->node_count = (size_t)c[2];
+    stats->leaf_count = (size_t)c[3];
+    stats->internal_node_count = (size_t)(c[2] - c[3]);
+    stats->maximum_depth = (size_t)c[4];
+    timings->bounds_ms = elapsed(b, 0, 1);
+    timings->keys_ms = elapsed(b, 1, 2);
+    timings->sort_ms = elapsed(b, 2, 3);
+    timings->build_ms = elapsed(b, 3, 4);
+    timings->moments_ms = elapsed(b, 4, 5);
+    timings->walk_ms = elapsed(b, 5, 6);
+    timings->integrate_ms = elapsed(b, 6, 7);
+    timings->total_ms = elapsed(b, 0, 7);
+    stats->build_time_seconds = (timings->total_ms - timings->walk_ms - timings->integrate_ms) * 1e-3;
+    stats->evaluation_time_seconds = timings->walk_ms * 1e-3;
+}
+
+NBodySimProStatus nbsp_bh_morton(NbspBarnesHut** handle, const NbspBarnesHutState* s,
+                                 int* status, cudaStream_t stream, uint64_t* keys_sorted,
+                                 uint64_t* permutation, double* root, NBodySimProError* error) {
+    NBodySimProStatus st = ensure(handle, s->n, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    NbspBarnesHut* b = *handle;
+    const size_t n = s->n;
+    cudaEventRecord(b->events[0], stream);
+    morton(b, s, status, stream);
+    BH_TRY(cudaGetLastError());
+    uint32_t* perm32 = NULL;
+    if (permutation != NULL) {
+        perm32 = (uint32_t*)malloc(n * sizeof(uint32_t));
+        if (perm32 == NULL)
+            return bh_fail(error, N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY, __FILE__, __LINE__,
+                           "failed to allocate permutation copy");
+    }
+    cudaError_t code = cudaSuccess;
+    if (keys_sorted != NULL)
+        code = cudaMemcpyAsync(keys_sorted, b->keys, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                               stream);
+    if (code == cudaSuccess && perm32 != NULL)
+        code = cudaMemcpyAsync(perm32, b->index, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               stream);
+    if (code == cudaSuccess && root != NULL)
+        code = cudaMemcpyAsync(root, b->geometry, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                               stream);
+    if (code == cudaSuccess) code = cudaStreamSynchronize(stream);
+    if (code == cudaSuccess && perm32 != NULL)
+        for (size_t i = 0; i < n; ++i) permutation[i] = perm32[i];
+    free(perm32);
+    if (code != cudaSuccess) return bh_cuda(error, code, "morton order copy", __LINE__);
+    b->timed = 0;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}

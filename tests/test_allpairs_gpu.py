@@ -1,0 +1,148 @@
+"""`cuda` all-pairs algorithm vs the FP64 oracle (parity), through the C ABI.
+
+Mirrors the reference's tests/numerical/gravity_test.c (known answers) and
+openmp_equivalence_test.c / simd_equivalence_test.c (cross-kernel
+equivalence), with FP32-force tolerances written here:
+
+    rms relative error   sqrt(sum|a - a_ref|^2 / sum|a_ref|^2)  <= 2e-6
+    max relative error   max_i |a_i - a_ref,i| / |a_ref,i|       <= 5e-5
+
+(FP32 tile sums with TwoSum-compensated accumulation on positions relative
+to the FP64 centre of mass; the reference's FP64 SIMD kernels are held to
+1e-10, a bound no FP32 kernel can meet.)
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RMS_TOL = 2e-6
+MAX_TOL = 5e-5
+
+
+def to_system(nb, p):
+    return nb.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS])
+
+
+def vec_max_rel(a, ref):
+    num = np.linalg.norm(a - ref, axis=1)
+    den = np.linalg.norm(ref, axis=1)
+    den = np.where(den > 1e-300, den, 1.0)
+    return float(np.max(num / den))
+
+
+def gpu_forces(nb, p, G, eps, ctx=None):
+    s = to_system(nb, p)
+    return nb.n_body_sim_pro_gravity_compute_acceleration_cuda(s, nb.gravity_init(G, eps), ctx)
+
+
+def test_two_body_analytic(cuda):
+    """gravity_test.c:30-60: a0 = (1,0,0), a1 = (-1,0,0) (eps = 0)."""
+    p = O.preset("two_body", 2, 1)
+    a = gpu_forces(cuda, p, 1.0, 0.0)
+    np.testing.assert_allclose(a, [[1, 0, 0], [-1, 0, 0]], atol=1e-6)
+
+
+def test_self_force_excluded(cuda):
+    """gravity_test.c:62-89: a lone particle feels nothing, eps = 0, no NaN."""
+    p = O.Particles.zeros(1)
+    p.x[:] = p.y[:] = p.z[:] = 1.0
+    p.m[:] = 1000.0
+    a = gpu_forces(cuda, p, 1.0, 0.0)
+    assert np.all(a == 0.0)
+
+
+def test_softening_bounds_force(cuda):
+    """gravity_test.c:91-124."""
+    p = O.Particles.zeros(2)
+    p.x[1] = 1e-8
+    p.m[:] = 1.0
+    a = gpu_forces(cuda, p, 1.0, 1e-2)
+    assert abs(a[1, 0]) < 1e6 and a[1, 0] < 0
+
+
+def test_mutual_force_antisymmetry(cuda):
+    """gravity_test.c:126-152: equal masses -> exactly opposite accelerations."""
+    p = O.preset("two_body", 2, 1)
+    a = gpu_forces(cuda, p, 1.0, 0.3)
+    assert np.array_equal(a[0], -a[1])
+
+
+@pytest.mark.parametrize("eps", [0.02, 0.0])
+def test_random_cloud_matches_reference(cuda, eps):
+    """openmp_equivalence_test.c:30-68 (N=512 seed 42) and
+    simd_equivalence_test.c:160-196 (eps = 0: finite, no NaN)."""
+    p = O.preset("random_cloud", 512, 42)
+    ref = O.gravity_reference(p.copy(), 1.0, eps)
+    a = gpu_forces(cuda, p, 1.0, eps)
+    assert np.all(np.isfinite(a))
+    assert O.rms_relative_error(a, ref) < RMS_TOL
+    assert vec_max_rel(a, ref) < MAX_TOL
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 255, 257, 1000, 4097])
+def test_ragged_sizes(cuda, n):
+    p = O.preset("globular_cluster", n, 5)
+    ref = O.gravity_reference(p.copy(), 1.0, 0.01)
+    a = gpu_forces(cuda, p, 1.0, 0.01)
+    if n == 1:
+        assert np.all(a == 0.0)
+    else:
+        assert O.rms_relative_error(a, ref) < RMS_TOL
+        assert vec_max_rel(a, ref) < MAX_TOL
+
+
+def test_empty_system_is_a_no_op(cuda):
+    s = cuda.ParticleSystem.zeros(0)
+    cuda.n_body_sim_pro_gravity_compute_acceleration_cuda(s, cuda.gravity_init(1.0, 0.01))
+
+
+def test_plummer_16384_matches_reference(cuda, ctx):
+    """Plummer a = 1, M = 1, N = 16384, seed 42, eps = 0.01 vs the scalar FP64
+    reference kernel (openmp restatement: same per-target loop)."""
+    p = O.preset("globular_cluster", 16384, 42)
+    ref = O.gravity_reference(p.copy(), 1.0, 0.01, openmp=True)
+    a = gpu_forces(cuda, p, 1.0, 0.01, ctx)
+    rms, mx = O.rms_relative_error(a, ref), vec_max_rel(a, ref)
+    print(f"plummer16384 rms={rms:.3e} max={mx:.3e}")
+    assert rms < RMS_TOL and mx < MAX_TOL
+
+
+def test_gravitational_constant_scales(cuda):
+    p = O.preset("random_cloud", 300, 7)
+    a1 = gpu_forces(cuda, p, 1.0, 0.02)
+    a3 = gpu_forces(cuda, p, 3.0, 0.02)
+    np.testing.assert_allclose(a3, 3.0 * a1, rtol=1e-12)
+
+
+def test_repeatable(cuda, ctx):
+    p = O.preset("globular_cluster", 5000, 9)
+    a = gpu_forces(cuda, p, 1.0, 0.01, ctx)
+    b = gpu_forces(cuda, p, 1.0, 0.01, ctx)
+    assert np.array_equal(a, b)
+
+
+def test_device_fp64_reference_matches_oracle(cuda, ctx):
+    """The device FP64 precision oracle restates gravity.c:46-61 exactly: only
+    the summation grouping differs from the CPU."""
+    p = O.preset("uniform_log_mass", 20000, 3)
+    s = to_system(cuda, p)
+    ctx.upload(s)
+    targets = np.random.default_rng(0).choice(p.n, 512, replace=False)
+    g = cuda.gravity_init(1.0, 1e-3)
+    dev = ctx.reference_acceleration(g, targets)
+    cpu = O.gravity_subset(p, 1.0, 1e-3, targets)
+    np.testing.assert_allclose(dev, cpu, rtol=1e-12, atol=0)
+
+
+def test_precision_study_small(cuda, ctx):
+    """Config-3 shape at N = 32768: uniform cube, log-uniform masses, eps = 1e-3."""
+    p = O.preset("uniform_log_mass", 32768, 11)
+    targets = np.random.default_rng(1).choice(p.n, 1024, replace=False)
+    ref = O.gravity_subset(p, 1.0, 1e-3, targets)
+    a = gpu_forces(cuda, p, 1.0, 1e-3, ctx)[targets]
+    rms, mx = O.rms_relative_error(a, ref), vec_max_rel(a, ref)
+    print(f"precision rms={rms:.3e} max={mx:.3e}")
+    assert rms < 1e-5 and mx < 5e-4
