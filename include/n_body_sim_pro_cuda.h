@@ -295,6 +295,63 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_synchronize(
 /* Name of the library's GPU architecture target ("sm_100a"). */
 N_BODY_SIM_PRO_CUDA_API const char* n_body_sim_pro_cuda_architecture(void);
 
+/* ---- ensembles of many small systems ------------------------------------------- */
+
+/*
+ * Many independent systems (each 1..4096 particles, its own softened all-pairs
+ * gravity, leapfrog KDK: src/c/physics/gravity.c:37-67 and
+ * src/c/physics/integrator.c:47-85 per system) advanced together.  The
+ * reference has no ensemble driver: a user would loop
+ * n_body_sim_pro_integrator_advance over the systems.
+ */
+typedef struct NBodySimProCudaEnsemble NBodySimProCudaEnsemble;
+
+typedef struct NBodySimProCudaEnsembleInfo {
+    size_t systems;
+    size_t particles;
+    int threads_per_block;      /* autotuned tile shape */
+    int targets_per_thread;
+    int grid;                   /* persistent CTAs (one resident wave) */
+    int work_items;             /* system bundles, longest first */
+    double last_advance_ms;     /* device time of the last advance */
+    double autotune_ms[3];      /* measured candidates (2 steps each) */
+} NBodySimProCudaEnsembleInfo;
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProCudaEnsemble* n_body_sim_pro_cuda_ensemble_create(
+    NBodySimProError* error);
+N_BODY_SIM_PRO_CUDA_API void n_body_sim_pro_cuda_ensemble_destroy(NBodySimProCudaEnsemble* e);
+
+/* `view` holds the systems back to back: system k is [offsets[k], offsets[k+1]);
+ * offsets has system_count + 1 entries, offsets[0] = 0, offsets[system_count] =
+ * view->particle_count. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_upload(
+    NBodySimProCudaEnsemble* e, const NBodySimProParticleSystemView* view,
+    const uint64_t* offsets, size_t system_count, NBodySimProError* error);
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_download(
+    NBodySimProCudaEnsemble* e, const NBodySimProParticleSystemView* view,
+    NBodySimProError* error);
+
+/* Measure the candidate tile shapes on the uploaded ensemble (state restored
+ * afterwards) and keep the fastest; advance calls it on first use. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_autotune(
+    NBodySimProCudaEnsemble* e, const NBodySimProGravity* gravity, double timestep,
+    NBodySimProError* error);
+
+/*
+ * `steps` leapfrog steps of every system.  Each call first computes the forces
+ * of the current positions (the integrators' precondition), then runs the
+ * steps.  one_launch_per_system = 0: one persistent kernel captured in a CUDA
+ * graph for the whole ensemble and all steps; 1: the per-system path (one
+ * all-pairs launch sequence per system and step), the baseline.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_advance(
+    NBodySimProCudaEnsemble* e, const NBodySimProGravity* gravity, double timestep, int steps,
+    int one_launch_per_system, NBodySimProError* error);
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_info(
+    const NBodySimProCudaEnsemble* e, NBodySimProCudaEnsembleInfo* info, NBodySimProError* error);
+
 /* Number of CUDA kernels this process has launched through the library. */
 N_BODY_SIM_PRO_CUDA_API unsigned long long n_body_sim_pro_cuda_kernel_launches(void);
 

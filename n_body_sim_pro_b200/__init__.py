@@ -119,6 +119,20 @@ class Timings(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class EnsembleInfo(C.Structure):
+    """NBodySimProCudaEnsembleInfo: the autotuned shape and the last device time."""
+
+    _fields_ = [("systems", C.c_size_t), ("particles", C.c_size_t),
+                ("threads_per_block", C.c_int), ("targets_per_thread", C.c_int),
+                ("grid", C.c_int), ("work_items", C.c_int), ("last_advance_ms", C.c_double),
+                ("autotune_ms", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "autotune_ms"}
+        d["autotune_ms"] = list(self.autotune_ms)
+        return d
+
+
 class CudaError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{Status(status).name}: {message}")
@@ -182,6 +196,14 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_synchronize": (st, [vp, pe]),
         "n_body_sim_pro_cuda_architecture": (C.c_char_p, []),
         "n_body_sim_pro_cuda_kernel_launches": (C.c_ulonglong, []),
+        "n_body_sim_pro_cuda_ensemble_create": (vp, [pe]),
+        "n_body_sim_pro_cuda_ensemble_destroy": (None, [vp]),
+        "n_body_sim_pro_cuda_ensemble_upload": (st, [vp, pv, C.POINTER(C.c_uint64), C.c_size_t,
+                                                     pe]),
+        "n_body_sim_pro_cuda_ensemble_download": (st, [vp, pv, pe]),
+        "n_body_sim_pro_cuda_ensemble_autotune": (st, [vp, pg, C.c_double, pe]),
+        "n_body_sim_pro_cuda_ensemble_advance": (st, [vp, pg, C.c_double, C.c_int, C.c_int, pe]),
+        "n_body_sim_pro_cuda_ensemble_info": (st, [vp, C.POINTER(EnsembleInfo), pe]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -401,3 +423,70 @@ class CudaContext:
     def synchronize(self) -> None:
         err = Error()
         _check(library().n_body_sim_pro_cuda_synchronize(self.handle, C.byref(err)), err)
+
+
+class CudaEnsemble:
+    """NBodySimProCudaEnsemble: many independent systems advanced together."""
+
+    def __init__(self):
+        L = library()
+        err = Error()
+        h = L.n_body_sim_pro_cuda_ensemble_create(C.byref(err))
+        if not h:
+            raise CudaError(err.status or Status.UNSUPPORTED_PLATFORM,
+                            err.message.decode(errors="replace"))
+        self.handle = C.c_void_p(h)
+        self.offsets = None
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            library().n_body_sim_pro_cuda_ensemble_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, system: ParticleSystem, offsets) -> None:
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        err = Error()
+        v = system.view()
+        _check(library().n_body_sim_pro_cuda_ensemble_upload(
+            self.handle, C.byref(v), off.ctypes.data_as(C.POINTER(C.c_uint64)), off.shape[0] - 1,
+            C.byref(err)), err)
+        self.offsets = off
+
+    def download(self, system: ParticleSystem) -> None:
+        err = Error()
+        v = system.view()
+        _check(library().n_body_sim_pro_cuda_ensemble_download(self.handle, C.byref(v),
+                                                               C.byref(err)), err)
+
+    def autotune(self, gravity: Gravity, timestep: float) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_ensemble_autotune(self.handle, C.byref(gravity),
+                                                               float(timestep), C.byref(err)), err)
+
+    def advance(self, gravity: Gravity, timestep: float, steps: int,
+                one_launch_per_system: bool = False) -> float:
+        """Advance every system; returns the device milliseconds of the call."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_ensemble_advance(
+            self.handle, C.byref(gravity), float(timestep), int(steps),
+            1 if one_launch_per_system else 0, C.byref(err)), err)
+        return self.info()["last_advance_ms"]
+
+    def info(self) -> dict:
+        i = EnsembleInfo()
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_ensemble_info(self.handle, C.byref(i), C.byref(err)),
+               err)
+        return i.as_dict()
