@@ -352,6 +352,35 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_advance(
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_ensemble_info(
     const NBodySimProCudaEnsemble* e, NBodySimProCudaEnsembleInfo* info, NBodySimProError* error);
 
+/* ---- all-pairs without device allocation ---------------------------------------- */
+
+/*
+ * No counterpart in the reference engine.
+ *
+ * All-pairs accelerations (the `cuda` algorithm's arithmetic) for callers that
+ * cannot allocate device memory: code running while a CUDA graph is being
+ * captured, plugins whose host framework owns every device allocation, loops
+ * that must not touch the allocator after start-up.  The caller passes DEVICE
+ * pointers for the inputs (positions, masses) and outputs (accelerations, FP64
+ * SoA) and, optionally, a cudaStream_t (NULL: the legacy default stream); the
+ * work is only enqueued, nothing synchronises and nothing is allocated or freed.
+ *
+ * The working memory is one static device array of about 4.3 MiB that every
+ * GPU loading this library holds until the process exits, so:
+ *   - particle_count must be <= 16384 (else INVALID_ARGUMENT, no GPU work);
+ *   - every call shares the array: calls whose GPU work overlaps (e.g. on two
+ *     unordered streams) race and give wrong results;
+ *   - the first call on each device looks up the array's address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Host pointers are rejected with INVALID_ARGUMENT.  Non-finite positions are
+ * not reported (no device status is read back): they give non-finite output.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_allpairs_acceleration_noalloc(
+    const double* positions_x, const double* positions_y, const double* positions_z,
+    const double* masses, double* accelerations_x, double* accelerations_y,
+    double* accelerations_z, size_t particle_count, double gravitational_constant,
+    double softening_length, void* stream, NBodySimProError* error);
+
 /* Number of CUDA kernels this process has launched through the library. */
 N_BODY_SIM_PRO_CUDA_API unsigned long long n_body_sim_pro_cuda_kernel_launches(void);
 
