@@ -328,7 +328,12 @@ def run_ours(args, wl, world, rank, local):
         kernel = "allpairs_force_kernel"
         interactions = float(n) * n
     achieved = flops / (kernel_ms * 1e-3) / 1e12
+    try:
+        probe = nb.measure_fp32_peak()
+    except nb.CudaError:
+        probe = None
     roofline = {"bound": "fp32", "kernel": kernel, "achieved": round(achieved, 3),
+                "probe": probe,
                 "peak": round(peak_max, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_max, 4),
                 "frac_at_load_clock": round(achieved / fp32_peak_tflops(sm_count, mhz_load), 4),

@@ -381,6 +381,13 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_allpairs_accelerat
     double* accelerations_z, size_t particle_count, double gravitational_constant,
     double softening_length, void* stream, NBodySimProError* error);
 
+/* Measured throughput of the current GPU: scalar FFMA and paired FFMA
+ * (fma.f32x2) in TFLOP/s, MUFU reciprocal square roots per second, and the
+ * nominal SM clock; the denominators of the FP32 roofline.  Any pointer may be NULL. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_measure_fp32_peak(
+    double* ffma_tflops, double* ffma2_tflops, double* rsqrt_per_second, double* sm_clock_mhz,
+    NBodySimProError* error);
+
 /* Number of CUDA kernels this process has launched through the library. */
 N_BODY_SIM_PRO_CUDA_API unsigned long long n_body_sim_pro_cuda_kernel_launches(void);
 

@@ -158,6 +158,16 @@ def kernel_launches() -> int:
     """CUDA kernels this process has launched through the library."""
     return int(library().n_body_sim_pro_cuda_kernel_launches())
 
+
+def measure_fp32_peak() -> dict:
+    """Measured FFMA / FFMA2 TFLOP/s and MUFU rsqrt/s of the current GPU."""
+    vals = [C.c_double(0.0) for _ in range(4)]
+    err = Error()
+    _check(library().n_body_sim_pro_cuda_measure_fp32_peak(*[C.byref(v) for v in vals],
+                                                          C.byref(err)), err)
+    return {"ffma_tflops": vals[0].value, "ffma2_tflops": vals[1].value,
+            "rsqrt_per_s": vals[2].value, "sm_clock_mhz": vals[3].value}
+
 _lib = None
 
 
@@ -204,6 +214,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_ensemble_autotune": (st, [vp, pg, C.c_double, pe]),
         "n_body_sim_pro_cuda_ensemble_advance": (st, [vp, pg, C.c_double, C.c_int, C.c_int, pe]),
         "n_body_sim_pro_cuda_ensemble_info": (st, [vp, C.POINTER(EnsembleInfo), pe]),
+        "n_body_sim_pro_cuda_measure_fp32_peak": (st, [C.POINTER(C.c_double)] * 4 + [pe]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

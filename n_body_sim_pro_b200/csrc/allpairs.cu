@@ -110,6 +110,121 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_kernel(
   }
 }
 
+// Paired variant: sm_100 executes two FP32 lanes' worth of add/mul/fma per
+// instruction with the .f32x2 forms, so two targets share every arithmetic
+// instruction of the interaction; only the MUFU rsqrt stays scalar.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+template <int BLOCK, int K, bool ZERO_SOFTENING>
+__global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
+    const float4* __restrict__ packed, int n, int n_padded, int chunk_len, float eps2,
+    float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
+  static_assert(K % 2 == 0, "targets are processed in pairs");
+  constexpr int P = K / 2;
+  __shared__ float4 tile[BLOCK];
+  const int tid = threadIdx.x;
+  const int first_target = blockIdx.x * (BLOCK * K) + tid;
+
+  unsigned long long X[P], Y[P], Z[P];
+  float hx[K], hy[K], hz[K], lx[K], ly[K], lz[K];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const int i0 = first_target + (2 * p) * BLOCK, i1 = first_target + (2 * p + 1) * BLOCK;
+    const float4 a = i0 < n ? packed[i0] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 b = i1 < n ? packed[i1] : make_float4(0.f, 0.f, 0.f, 0.f);
+    X[p] = pack2(a.x, b.x);
+    Y[p] = pack2(a.y, b.y);
+    Z[p] = pack2(a.z, b.z);
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+  const unsigned long long E2 = pack2(eps2, eps2);
+
+  const int j0 = blockIdx.y * chunk_len;
+  const int j1 = min(j0 + chunk_len, n_padded);
+  float4 next = j0 < j1 ? packed[j0 + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int jt = j0; jt < j1; jt += BLOCK) {
+    __syncthreads();
+    tile[tid] = next;
+    __syncthreads();
+    if (jt + BLOCK < j1) next = packed[jt + BLOCK + tid];
+    unsigned long long AX[P], AY[P], AZ[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) AX[p] = AY[p] = AZ[p] = 0ull;
+#pragma unroll 8
+    for (int j = 0; j < BLOCK; ++j) {
+      const float4 s = tile[j];
+      const unsigned long long SX = pack2(s.x, s.x), SY = pack2(s.y, s.y), SZ = pack2(s.z, s.z);
+      const unsigned long long SW = pack2(s.w, s.w);
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const unsigned long long dx = sub2(SX, X[p]);
+        const unsigned long long dy = sub2(SY, Y[p]);
+        const unsigned long long dz = sub2(SZ, Z[p]);
+        const unsigned long long r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+        float r2a, r2b;
+        unpack2(r2, r2a, r2b);
+        float ra = rsqrt_mufu(r2a), rb = rsqrt_mufu(r2b);
+        if (ZERO_SOFTENING) {
+          ra = r2a > 0.f ? ra : 0.f;
+          rb = r2b > 0.f ? rb : 0.f;
+        }
+        const unsigned long long R = pack2(ra, rb);
+        const unsigned long long W = mul2(SW, mul2(mul2(R, R), R));
+        AX[p] = fma2(W, dx, AX[p]);
+        AY[p] = fma2(W, dy, AY[p]);
+        AZ[p] = fma2(W, dz, AZ[p]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      float a, b;
+      unpack2(AX[p], a, b);
+      fold(hx[2 * p], lx[2 * p], a);
+      fold(hx[2 * p + 1], lx[2 * p + 1], b);
+      unpack2(AY[p], a, b);
+      fold(hy[2 * p], ly[2 * p], a);
+      fold(hy[2 * p + 1], ly[2 * p + 1], b);
+      unpack2(AZ[p], a, b);
+      fold(hz[2 * p], lz[2 * p], a);
+      fold(hz[2 * p + 1], lz[2 * p + 1], b);
+    }
+  }
+
+  const size_t base = (size_t)blockIdx.y * (size_t)n;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i = first_target + k * BLOCK;
+    if (i < n) {
+      hi_out[base + i] = make_float4(hx[k], hy[k], hz[k], 0.f);
+      lo_out[base + i] = make_float4(lx[k], ly[k], lz[k], 0.f);
+    }
+  }
+}
+
 typedef void (*ForceKernel)(const float4*, int, int, int, float, float4*, float4*);
 
 template <int BLOCK, int K>
@@ -118,7 +233,20 @@ ForceKernel pick(bool zero_softening) {
                         : allpairs_force_kernel<BLOCK, K, false>;
 }
 
+template <int BLOCK, int K>
+ForceKernel pick_paired(bool zero_softening) {
+  return zero_softening ? allpairs_force_paired_kernel<BLOCK, K, true>
+                        : allpairs_force_paired_kernel<BLOCK, K, false>;
+}
+
 ForceKernel select_kernel(NbspAllPairsShape s, bool zero_softening) {
+  if (s.paired) {
+    if (s.block == 64 && s.per_thread == 8) return pick_paired<64, 8>(zero_softening);
+    if (s.block == 128 && s.per_thread == 4) return pick_paired<128, 4>(zero_softening);
+    if (s.block == 128 && s.per_thread == 8) return pick_paired<128, 8>(zero_softening);
+    if (s.block == 256 && s.per_thread == 4) return pick_paired<256, 4>(zero_softening);
+    return nullptr;
+  }
 #define NBSP_CASE(B, K) \
   if (s.block == B && s.per_thread == K) return pick<B, K>(zero_softening);
   NBSP_CASE(64, 4)

@@ -320,7 +320,9 @@ static NBodySimProStatus check_gravity(const NBodySimProGravity* g, NBodySimProE
 /* ------------------------------------------------------------------------- */
 
 static const NbspAllPairsShape kShapes[] = {
-    {128, 4, 1}, {128, 2, 1}, {256, 2, 1}, {64, 8, 1}, {128, 8, 1}, {64, 4, 1}, {256, 4, 1},
+    {128, 4, 1, 0}, {128, 2, 1, 0}, {256, 2, 1, 0}, {64, 8, 1, 0}, {128, 8, 1, 0},
+    {64, 4, 1, 0},  {256, 4, 1, 0}, {64, 8, 1, 1},  {128, 4, 1, 1}, {128, 8, 1, 1},
+    {256, 4, 1, 1},
 };
 
 /* Source chunks so that (target blocks x chunks) fills whole waves of resident CTAs. */
@@ -650,8 +652,11 @@ static NBodySimProStatus advance_allpairs_kdk(NBodySimProCudaContext* c,
     NbspAllPairsShape s = choose_shape(c, n, eps2);
     if ((size_t)s.chunks * n > c->partial_elems) s.chunks = (int)(c->partial_elems / n);
     for (int step = 0; step < steps; ++step) {
+        const int last = step + 1 == steps;
+        if (last) cudaEventRecord(c->events[2], c->stream);
         nbsp_allpairs_force(c->packed, n, c->n_padded, eps2, s, c->partial_hi, c->partial_lo,
                             c->stream);
+        if (last) cudaEventRecord(c->events[3], c->stream);
         if (step + 1 < steps) {
             nbsp_allpairs_finalize_kick_kick_drift_pack(
                 c->partial_hi, c->partial_lo, n, c->n_padded, s.chunks, g->gravitational_constant,
@@ -721,6 +726,14 @@ NBodySimProStatus n_body_sim_pro_cuda_advance(NBodySimProCudaContext* c,
     if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS &&
+        integrator != N_BODY_SIM_PRO_INTEGRATOR_EULER) {
+        float force_ms = 0.f; /* the last step's force kernel alone */
+        cudaEventElapsedTime(&force_ms, c->events[2], c->events[3]);
+        memset(&c->timings, 0, sizeof(c->timings));
+        c->timings.walk_ms = force_ms;
+        c->timings.integrate_ms = ms - force_ms * steps;
+    }
     c->timings.total_ms = ms;
     return N_BODY_SIM_PRO_STATUS_OK;
 }

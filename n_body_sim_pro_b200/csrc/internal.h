@@ -39,6 +39,7 @@ typedef struct NbspAllPairsShape {
     int block;        /* threads per CTA (64, 128 or 256) */
     int per_thread;   /* targets per thread (1, 2, 4 or 8) */
     int chunks;       /* source chunks S (grid.y); partials reduced in FP64 */
+    int paired;       /* 1: targets processed in pairs with fma/add/mul.f32x2 */
 } NbspAllPairsShape;
 
 /* Number of CTAs per SM the force kernel of this shape can keep resident. */
