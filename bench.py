@@ -50,6 +50,8 @@ WORKLOADS = {
                                  ic="plummer", steps=3),
     "allpairs_precision_262k": dict(n=262144, algorithm="all_pairs", eps=1e-3, dt=1e-4,
                                     ic="uniform_log_mass", steps=3),
+    "ensemble_4096": dict(n=None, algorithm="ensemble", systems=4096, lo=32, hi=4096, eps=0.01,
+                          dt=1e-3, ic="ensemble", steps=1000),
 }
 
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
@@ -270,7 +272,9 @@ def run_ours(args, wl, world, rank, local):
     pos, vel, mass = initial_conditions(wl["ic"], n, seed=42 + rank)
     g = nb.gravity_init(1.0, wl["eps"])
     algo = nb.Algorithm.BARNES_HUT if wl["algorithm"] == "barnes_hut" else nb.Algorithm.ALL_PAIRS
-    ctx = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1))
+    ctx = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1),
+                         leaf_capacity=wl.get("leaf"))
+    ctx.set_walk(0 if wl.get("walk") == "stackless" else 1)
     system = nb.ParticleSystem.from_arrays(pos, vel, mass)
     ctx.upload(system)
     ctx.compute_acceleration(g, algo)
@@ -355,6 +359,76 @@ def run_ours(args, wl, world, rank, local):
                 stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms))
 
 
+def ensemble_ic(wl, seed=42):
+    """Systems of round(exp(U(ln lo, ln hi))) Plummer particles (a = 1, M = 1), each
+    from its own seeded stream, concatenated."""
+    sizes, blocks = [], []
+    for k in range(wl["systems"]):
+        rng = np.random.default_rng([seed, k])
+        n = int(np.clip(np.rint(np.exp(rng.uniform(np.log(wl["lo"]), np.log(wl["hi"])))),
+                        wl["lo"], wl["hi"]))
+        blocks.append(plummer_block(rng, n, 1.0, 1.0, (0.0, 0.0, 0.0)))
+        sizes.append(n)
+    pos = np.vstack([b[0] for b in blocks])
+    vel = np.vstack([b[1] for b in blocks])
+    mass = np.concatenate([b[2] for b in blocks])
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    return pos, vel, mass, offsets
+
+
+def run_ensemble(args, wl, world, rank, local):
+    import torch
+
+    import n_body_sim_pro_b200 as nb
+
+    pos, vel, mass, offsets = ensemble_ic(wl, seed=42 + rank)
+    n = mass.shape[0]
+    sizes = np.diff(offsets.astype(np.int64))
+    g = nb.gravity_init(1.0, wl["eps"])
+    system = nb.ParticleSystem.from_arrays(pos, vel, mass)
+    ens = nb.CudaEnsemble()
+    ens.upload(system, offsets)
+    ens.autotune(g, wl["dt"])
+    launches0 = None
+    for _ in range(args.warmup):
+        ens.advance(g, wl["dt"], 1)
+    barrier_sync(world)
+    launches0 = nb.kernel_launches()
+    with ClockSampler(local) as clocks:
+        ms = ens.advance(g, wl["dt"], args.steps)
+    launches = nb.kernel_launches() - launches0
+    barrier_sync(world)
+    total_ms = max_over_ranks(ms, world)
+    info = ens.info()
+    # baseline: one launch sequence per system and step, on a 2-step sample
+    base_steps = 2
+    ens.upload(system, offsets)
+    base_ms = ens.advance(g, wl["dt"], base_steps, one_launch_per_system=True)
+    baseline = {"value": n * base_steps / (base_ms * 1e-3), "unit": "particle-steps/s",
+                "sample": f"{base_steps} steps, per-system all-pairs launches "
+                          f"({int(nb.kernel_launches())} launches so far)"}
+    interactions = float(np.sum(sizes.astype(np.float64) ** 2))
+    peaks, peak_kind = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
+    flops = FLOPS_PAIR * interactions * (args.steps + 1)  # + the initial force pass
+    achieved = flops / (total_ms * 1e-3) / 1e12
+    clk = clocks.summary()
+    roofline = {"bound": "fp32", "kernel": "ensemble_kernel", "achieved": round(achieved, 3),
+                "peak": round(peak_max, 2), "unit": "TFLOP/s", "frac": round(achieved / peak_max, 4),
+                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x {peaks.get('sm_max_mhz')} MHz "
+                             f"({peak_kind})", "flops_per_launch": flops,
+                "launch_ms": round(total_ms, 3), "traffic": None}
+    ens.close()
+    value = world * n * args.steps / (total_ms * 1e-3)
+    return dict(value=value, total_ms=total_ms, rms=None, max_rel=None, drift=None,
+                roofline=roofline, clocks=clk, launches=launches, e2e=None,
+                interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
+                stats={"systems": int(len(sizes)), "particles": int(n),
+                       "ensemble": info, "one_launch_per_system": baseline},
+                timings={"advance_ms": round(ms, 3)})
+
+
 def ctx_timings_summary(step_ms, walk_ms):
     return {"step_ms_mean": round(float(np.mean(step_ms)), 4),
             "walk_ms_mean": round(float(np.mean(walk_ms)), 4)}
@@ -406,8 +480,15 @@ def main(argv=None):
     ap.add_argument("--workload", default="bh_collision_1m", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--order", type=int, default=None, choices=[1, 2])
+    ap.add_argument("--walk", default=None, choices=["lists", "stackless"])
+    ap.add_argument("--leaf", type=int, default=None)
     args = ap.parse_args(argv)
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    for key in ("theta", "order", "walk", "leaf"):
+        if getattr(args, key) is not None:
+            wl[key] = getattr(args, key)
     if args.steps is None:
         args.steps = wl["steps"]
     args.warmup = max(args.warmup, 3)
@@ -415,6 +496,8 @@ def main(argv=None):
     config = {"workload": args.workload, "particles": wl["n"], "algorithm": wl["algorithm"],
               "theta": wl.get("theta"), "softening": wl["eps"], "timestep": wl["dt"],
               "integrator": "leapfrog_kdk", "multipole_order": wl.get("order"),
+              "walk": wl.get("walk", "lists") if wl["algorithm"] == "barnes_hut" else None,
+              "leaf_capacity": wl.get("leaf", 16) if wl["algorithm"] == "barnes_hut" else None,
               "initial_conditions": wl["ic"], "l2": "256 MiB write between timed steps",
               "parallelism": f"replicas x{args.gpus}"}
 
@@ -444,9 +527,13 @@ def main(argv=None):
         return 0
 
     world, rank, local = dist_setup(args.gpus)
-    r = run_ours(args, wl, world, rank, local)
+    if wl["algorithm"] == "ensemble":
+        r = run_ensemble(args, wl, world, rank, local)
+        config["particles"] = r["stats"]["particles"]
+    else:
+        r = run_ours(args, wl, world, rank, local)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and wl["algorithm"] != "ensemble":
         try:
             pos, vel, mass = initial_conditions(wl["ic"], wl["n"], seed=42)
             threads = os.cpu_count() or 1

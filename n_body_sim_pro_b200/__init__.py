@@ -188,6 +188,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_theta": (C.c_double, [vp]),
         "n_body_sim_pro_cuda_context_set_multipole_order": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_leaf_capacity": (st, [vp, C.c_int, pe]),
+        "n_body_sim_pro_cuda_context_set_walk": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_gravity_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
@@ -360,6 +361,12 @@ class CudaContext:
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_multipole_order(self.handle, order,
                                                                          C.byref(err)), err)
+
+    def set_walk(self, walk: int) -> None:
+        """0: stackless skip-link walk; 1: interaction-list walk (default)."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_walk(self.handle, int(walk),
+                                                              C.byref(err)), err)
 
     def set_leaf_capacity(self, capacity: int) -> None:
         err = Error()

@@ -102,6 +102,7 @@ struct NBodySimProCudaContext {
     double theta;
     int multipole_order;
     int leaf_capacity;
+    int walk_mode;
     NbspBarnesHut* bh;
     int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
 
@@ -141,6 +142,7 @@ NBodySimProCudaContext* n_body_sim_pro_cuda_context_create(NBodySimProError* err
     c->theta = 0.7;
     c->multipole_order = 1;
     c->leaf_capacity = 16;
+    c->walk_mode = NBSP_BH_WALK_LISTS;
     const char* tune = getenv("NBSP_AUTOTUNE");
     c->autotune = !(tune != NULL && tune[0] == '0');
     struct cudaDeviceProp prop;
@@ -216,6 +218,16 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_capacity(NBodySimProCudaC
     if (c == NULL || capacity < 1 || capacity > NBSP_BH_MAX_LEAF)
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "leaf capacity must be in 1..64");
     c->leaf_capacity = capacity;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(NBodySimProCudaContext* c, int walk,
+                                                       NBodySimProError* error) {
+    if (c == NULL || (walk != N_BODY_SIM_PRO_CUDA_WALK_STACKLESS &&
+                      walk != N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown Barnes-Hut walk");
+    c->walk_mode = walk == N_BODY_SIM_PRO_CUDA_WALK_STACKLESS ? NBSP_BH_WALK_STACKLESS
+                                                              : NBSP_BH_WALK_LISTS;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
@@ -441,6 +453,7 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.softening_squared = g->softening_squared;
         p.multipole_order = c->multipole_order;
         p.leaf_capacity = c->leaf_capacity;
+        p.walk_mode = c->walk_mode;
         NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
         c->bh_pending = 1;
         return nbsp_bh_accelerations(&c->bh, &s, &p, c->status, c->stream, &c->stats,

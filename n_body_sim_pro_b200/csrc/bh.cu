@@ -386,6 +386,7 @@ struct Tree {
   float4* com;        // walk format: com xyz, mass
   float* ropen2;      // (2h / theta)^2
   float4* quad;       // 2 per node: (xx, xy, xz, yy), (yz, 0, 0, 0)
+  int* children;      // 8 per internal node, depth-first order (interaction-list walk)
   unsigned long long* leaves;  // [1]
 };
 
@@ -424,6 +425,7 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.com = carve<float4>(p, nb);
   t.ropen2 = carve<float>(p, nb);
   t.quad = carve<float4>(p, 2 * nb);
+  t.children = carve<int>(p, 8 * nb);
   t.leaves = carve<unsigned long long>(p, 1);
   if (end != nullptr) *end = p;
   return t;
@@ -738,6 +740,7 @@ __global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         return;
       }
+      t.children[8 * parent + guard - 1] = c;
       const double4 cm = ldcg_d4(&t.mom[c]);
       m += cm.x;
       sx += cm.x * cm.y;
@@ -746,6 +749,7 @@ __global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
       hmax = max(hmax, __ldcg(&t.height[c]));
       c = __ldcg(&t.info[c]).x;
     }
+    for (int k = guard; k < 8; ++k) t.children[8 * parent + k] = -1;
     Moments pm;
     pm.m = m;
     pm.cx = m != 0.0 ? sx / m : 0.0;
@@ -793,16 +797,15 @@ constexpr int kWalkThreads = 256;
 // targets and visit the same node sequence; a cell is opened when any lane's
 // opening test fails (so every lane's own test holds for every cell it
 // accepts), otherwise all lanes apply its multipole and skip its subtree.
+struct WalkAcc {
+  float hx, hy, hz, lx, ly, lz;  // compensated acceleration / G
+  unsigned approx, exact;        // accepted cells, particle-particle terms
+};
+
 template <int ORDER>
-__global__ void __launch_bounds__(kWalkThreads) walk_kernel(
-    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
-    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
-  if (warp * 32 >= n) return;
-  const int s = warp * 32 + lane;
-  const bool active = s < n;
-  const float4 p = pos[active ? s : n - 1];
+__device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, int n,
+                                               const Tree& t, float eps2, int s, bool active,
+                                               float4 p, int lane, int* status, WalkAcc& out) {
   const int total = (int)t.offset[n];
   const int limit = 2 * total + 64;
 
@@ -885,19 +888,251 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
   fold(hx, lx, px);
   fold(hy, ly, py);
   fold(hz, lz, pz);
+  out.hx = hx;
+  out.hy = hy;
+  out.hz = hz;
+  out.lx = lx;
+  out.ly = ly;
+  out.lz = lz;
+  out.approx = approx;
+  out.exact = exact;
+}
+
+__device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active, int lane,
+                                           float4* __restrict__ acc_hi,
+                                           float4* __restrict__ acc_lo,
+                                           unsigned long long* __restrict__ counters) {
   if (active) {
-    acc_hi[s] = make_float4(hx, hy, hz, 0.f);
-    acc_lo[s] = make_float4(lx, ly, lz, 0.f);
+    acc_hi[s] = make_float4(a.hx, a.hy, a.hz, 0.f);
+    acc_lo[s] = make_float4(a.lx, a.ly, a.lz, 0.f);
   }
-  unsigned long long a = approx, e = exact;
+  unsigned long long ap = a.approx, ex = a.exact;
   for (int off = 16; off > 0; off >>= 1) {
-    a += __shfl_down_sync(kFull, a, off);
-    e += __shfl_down_sync(kFull, e, off);
+    ap += __shfl_down_sync(kFull, ap, off);
+    ex += __shfl_down_sync(kFull, ex, off);
   }
   if (lane == 0) {
-    atomicAdd(&counters[0], a);
-    atomicAdd(&counters[1], e);
+    atomicAdd(&counters[0], ap);
+    atomicAdd(&counters[1], ex);
   }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(kWalkThreads) walk_kernel(
+    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
+    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
+  if (warp * 32 >= n) return;
+  const int s = warp * 32 + lane;
+  const bool active = s < n;
+  const float4 p = pos[active ? s : n - 1];
+  WalkAcc a;
+  stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
+  store_walk(a, s, active, lane, acc_hi, acc_lo, counters);
+}
+
+// Accepted-cell term (monopole, optionally + trace-free quadrupole), d = com - target:
+// a = G [ M d / r^3 - Q d / r^5 + 5/2 (d.Q.d) d / r^7 ],  r^2 = d^2 + eps^2.
+template <int ORDER>
+__device__ __forceinline__ void cell_term(const Tree& t, int node, float4 c, float4 p, float eps2,
+                                          float& px, float& py, float& pz) {
+  const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+  const float rinv = rsqrt_mufu(r2);
+  const float rinv2 = rinv * rinv;
+  const float rinv3 = rinv * rinv2;
+  float w = c.w * rinv3;
+  if (ORDER == 2) {
+    const float4 qa = t.quad[2 * node];
+    const float qyz = t.quad[2 * node + 1].x;
+    const float qzz = -qa.x - qa.w;
+    const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
+    const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qyz * dz));
+    const float qdz = fmaf(qa.z, dx, fmaf(qyz, dy, qzz * dz));
+    const float dqd = fmaf(dx, qdx, fmaf(dy, qdy, dz * qdz));
+    const float rinv5 = rinv3 * rinv2;
+    const float rinv7 = rinv5 * rinv2;
+    w = fmaf(2.5f * dqd, rinv7, w);
+    px = fmaf(-qdx, rinv5, px);
+    py = fmaf(-qdy, rinv5, py);
+    pz = fmaf(-qdz, rinv5, pz);
+  }
+  px = fmaf(w, dx, px);
+  py = fmaf(w, dy, py);
+  pz = fmaf(w, dz, pz);
+}
+
+constexpr int kListThreads = 128;  // 4 warps, one traversal group each
+constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
+constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> stackless walk
+
+// Interaction-list walk.  The 32 Morton-consecutive targets of a warp form a
+// group with an axis-aligned bounding box.  Each step the lanes pop up to 32
+// nodes from the warp's shared-memory stack and test them IN PARALLEL with the
+// group form of the reference criterion: accept when (2h)^2 < theta^2 dmin^2,
+// dmin the distance from the cell's centre of mass to the group box (so every
+// target's own test (2h)^2 < theta^2 d^2 holds as well); leaves and accepted
+// cells are appended to two lists that are evaluated, whenever 32 have
+// gathered, in dense loops where every lane computes its own target's terms.
+// A warp whose stack would overflow restarts with the stackless walk.
+template <int ORDER, int STACK>
+__global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
+    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
+    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
+  __shared__ int s_stack[kListThreads / 32][STACK];
+  __shared__ int s_cells[kListThreads / 32][kListCap];
+  __shared__ int s_leaves[kListThreads / 32][kListCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
+  if (warp * 32 >= n) return;
+  int* stack = s_stack[wib];
+  int* cells = s_cells[wib];
+  int* leaves = s_leaves[wib];
+  const int s = warp * 32 + lane;
+  const bool active = s < n;
+  const float4 p = pos[active ? s : n - 1];
+  const unsigned lt = (1u << lane) - 1u;
+
+  // group bounding box
+  float bx0 = p.x, bx1 = p.x, by0 = p.y, by1 = p.y, bz0 = p.z, bz1 = p.z;
+  for (int off = 16; off > 0; off >>= 1) {
+    bx0 = fminf(bx0, __shfl_xor_sync(kFull, bx0, off));
+    bx1 = fmaxf(bx1, __shfl_xor_sync(kFull, bx1, off));
+    by0 = fminf(by0, __shfl_xor_sync(kFull, by0, off));
+    by1 = fmaxf(by1, __shfl_xor_sync(kFull, by1, off));
+    bz0 = fminf(bz0, __shfl_xor_sync(kFull, bz0, off));
+    bz1 = fmaxf(bz1, __shfl_xor_sync(kFull, bz1, off));
+  }
+  const float gx = 0.5f * (bx0 + bx1), gy = 0.5f * (by0 + by1), gz = 0.5f * (bz0 + bz1);
+  const float ex = 0.5f * (bx1 - bx0), ey = 0.5f * (by1 - by0), ez = 0.5f * (bz1 - bz0);
+
+  const int total = (int)t.offset[n];
+  float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+  unsigned approx = 0, exact = 0;
+  int top = 1, ncell = 0, nleaf = 0, iters = 0;
+  bool overflow = false;
+  if (lane == 0) stack[0] = 0;
+  __syncwarp();
+  while (top > 0 || ncell > 0 || nleaf > 0) {
+    if (top > 0) {
+      if (++iters > total + 64) {  // every node is popped at most once
+        if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
+        break;
+      }
+      const int take = min(32, top);
+      int node = lane < take ? stack[top - 1 - lane] : -1;
+      top -= take;
+      __syncwarp();
+      bool is_leaf = false, accept = false;
+      int kids = 0;
+      int4 ca = make_int4(-1, -1, -1, -1), cb = make_int4(-1, -1, -1, -1);
+      if (node >= total) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        node = -1;
+      }
+      if (node >= 0) {
+        const int4 info = t.info[node];
+        if (info.z > 0) {
+          is_leaf = true;
+        } else {
+          const float4 c = t.com[node];
+          const float qx = fmaxf(fabsf(c.x - gx) - ex, 0.f);
+          const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
+          const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
+          const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+          accept = dmin2 > t.ropen2[node];
+          if (!accept) {
+            ca = reinterpret_cast<const int4*>(t.children)[2 * node];
+            cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
+            kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) +
+                   (cb.y >= 0) + (cb.z >= 0) + (cb.w >= 0);
+          }
+        }
+      }
+      unsigned m = __ballot_sync(kFull, is_leaf);
+      if (is_leaf) leaves[nleaf + __popc(m & lt)] = node;
+      nleaf += __popc(m);
+      m = __ballot_sync(kFull, accept);
+      if (accept) cells[ncell + __popc(m & lt)] = node;
+      ncell += __popc(m);
+      int incl = kids;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const int pushed = __shfl_sync(kFull, incl, 31);
+      if (top + pushed > STACK) {
+        overflow = true;
+        break;
+      }
+      const int base = top + incl - kids;
+      const int kid[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < kids) stack[base + k] = kid[k];
+      top += pushed;
+      __syncwarp();
+    }
+    const bool drain = top == 0;
+    if (ncell >= 32 || (drain && ncell > 0)) {
+      float px = 0.f, py = 0.f, pz = 0.f;
+      for (int e = 0; e < ncell; ++e) {
+        const int node = cells[e];
+        cell_term<ORDER>(t, node, t.com[node], p, eps2, px, py, pz);
+      }
+      fold(hx, lx, px);
+      fold(hy, ly, py);
+      fold(hz, lz, pz);
+      approx += active ? (unsigned)ncell : 0u;
+      ncell = 0;
+    }
+    if (nleaf >= 32 || (drain && nleaf > 0)) {
+      int e = 0;
+      while (e < nleaf) {  // consecutive leaves often abut: merge their particle ranges
+        const int4 first = t.info[leaves[e++]];
+        const int b = first.y;
+        int end = first.y + first.z;
+        while (e < nleaf) {
+          const int4 nx = t.info[leaves[e]];
+          if (nx.y != end) break;
+          end = nx.y + nx.z;
+          ++e;
+        }
+        float px = 0.f, py = 0.f, pz = 0.f;
+        for (int j = b; j < end; ++j) {
+          const float4 q = pos[j];
+          const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+          const float rinv = j == s ? 0.f : rsqrt_mufu(r2);  // barnes_hut.c:572
+          const float w = q.w * (rinv * rinv * rinv);
+          px = fmaf(w, dx, px);
+          py = fmaf(w, dy, py);
+          pz = fmaf(w, dz, pz);
+        }
+        fold(hx, lx, px);
+        fold(hy, ly, py);
+        fold(hz, lz, pz);
+        exact += active ? (unsigned)(end - b - ((s >= b && s < end) ? 1 : 0)) : 0u;
+      }
+      nleaf = 0;
+    }
+    __syncwarp();
+  }
+  WalkAcc a;
+  if (overflow) {
+    stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
+  } else {
+    a.hx = hx;
+    a.hy = hy;
+    a.hz = hz;
+    a.lx = lx;
+    a.ly = ly;
+    a.lz = lz;
+    a.approx = approx;
+    a.exact = exact;
+  }
+  store_walk(a, s, active, lane, acc_hi, acc_lo, counters);
 }
 
 __global__ void tree_counts_kernel(Tree t, unsigned long long* counters) {
@@ -1001,10 +1236,22 @@ void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry, double 
                                                                    geometry, inv_theta2, status);
 }
 
-void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, float eps2,
+void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode, float eps2,
                   void* acc_hi, void* acc_lo, unsigned long long* counters, int* status,
                   cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
+  if (mode == NBSP_BH_WALK_LISTS) {
+    const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
+    const float4* p = (const float4*)pos4;
+    if (order == 2) {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack><<<blocks, kListThreads, 0, stream>>>(
+          p, (int)n, t, eps2, (float4*)acc_hi, (float4*)acc_lo, counters, status);
+    } else {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack><<<blocks, kListThreads, 0, stream>>>(
+          p, (int)n, t, eps2, (float4*)acc_hi, (float4*)acc_lo, counters, status);
+    }
+    return;
+  }
   const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
   if (order == 2) {
     NBSP_COUNT_LAUNCH(1), walk_kernel<2><<<blocks, kWalkThreads, 0, stream>>>((const float4*)pos4, (int)n, t, eps2,

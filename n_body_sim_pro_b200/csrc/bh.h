@@ -36,6 +36,7 @@ typedef struct NbspBarnesHutParams {
     double softening_squared;
     int multipole_order;
     int leaf_capacity;
+    int walk_mode;
 } NbspBarnesHutParams;
 
 typedef struct NbspBarnesHutState {
@@ -108,8 +109,13 @@ NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, size_t n, const double* geome
                                  double theta, int order, void* tree, int* status,
                                  cudaStream_t stream);
 
-/* Walk: a_sorted (float4 hi, lo per target) and interaction counters. */
-NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order,
+enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
+
+/* Walk: a_sorted (float4 hi, lo per target) and interaction counters.
+ * mode NBSP_BH_WALK_STACKLESS: warp-coherent skip-link walk, per-target test;
+ * mode NBSP_BH_WALK_LISTS: lane-parallel node tests against the warp's group
+ * box, dense evaluation of gathered interaction lists. */
+NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
                               float softening_squared, void* acc_hi, void* acc_lo,
                               unsigned long long* counters, int* status, cudaStream_t stream);
 

@@ -152,7 +152,8 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     cudaEventRecord(b->events[4], stream);
     nbsp_bh_moments(b->pos4, n, b->geometry, p->theta, p->multipole_order, b->tree, status, stream);
     cudaEventRecord(b->events[5], stream);
-    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, (float)p->softening_squared, b->acc_hi,
+    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode,
+                 (float)p->softening_squared, b->acc_hi,
                  b->acc_lo, b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
     nbsp_bh_scatter(b->acc_hi, b->acc_lo, b->index, n, p->gravitational_constant, s->ax, s->ay,

@@ -21,10 +21,19 @@ def to_system(nb, p):
     return nb.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS])
 
 
-def bh(nb, p, eps, theta, ctx, order=1, leaf=16):
+WALKS = [0, 1]  # stackless skip-link walk, interaction-list walk
+
+
+@pytest.fixture(params=WALKS, ids=["stackless", "lists"])
+def walk(request):
+    return request.param
+
+
+def bh(nb, p, eps, theta, ctx, order=1, leaf=16, walk=1):
     ctx.theta = theta
     ctx.set_multipole_order(order)
     ctx.set_leaf_capacity(leaf)
+    ctx.set_walk(walk)
     s = to_system(nb, p)
     a = nb.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, nb.gravity_init(1.0, eps), ctx)
     return a, ctx.stats()
@@ -66,11 +75,11 @@ def test_morton_ties_keep_index_order(cuda, ctx):
     assert np.array_equal(k, k_ref) and np.array_equal(perm, perm_ref)
 
 
-def test_two_body_is_exact(cuda, ctx):
+def test_two_body_is_exact(cuda, ctx, walk):
     """barnes_hut_test.c:59-103: leaves only, 0 approximations, 2 exact."""
     p = O.preset("two_body", 2, 1)
     ref = O.gravity_reference(p.copy(), 1.0, 0.02)
-    a, st = bh(cuda, p, 0.02, 0.7, ctx, leaf=1)
+    a, st = bh(cuda, p, 0.02, 0.7, ctx, leaf=1, walk=walk)
     assert O.rms_relative_error(a, ref) < 1e-6
     assert st["leaf_count"] == 2
     assert st["accepted_approximations"] == 0
@@ -78,12 +87,12 @@ def test_two_body_is_exact(cuda, ctx):
 
 
 @pytest.mark.parametrize("leaf", [1, 16])
-def test_theta_tradeoff_and_accuracy(cuda, ctx, leaf):
+def test_theta_tradeoff_and_accuracy(cuda, ctx, leaf, walk):
     """barnes_hut_test.c:105-160: random cloud N=400 seed 7, eps 0.02."""
     p = O.preset("random_cloud", 400, 7)
     ref = O.gravity_reference(p.copy(), 1.0, 0.02)
-    a3, s3 = bh(cuda, p, 0.02, 0.3, ctx, leaf=leaf)
-    a12, s12 = bh(cuda, p, 0.02, 1.2, ctx, leaf=leaf)
+    a3, s3 = bh(cuda, p, 0.02, 0.3, ctx, leaf=leaf, walk=walk)
+    a12, s12 = bh(cuda, p, 0.02, 1.2, ctx, leaf=leaf, walk=walk)
     e3, e12 = O.rms_relative_error(a3, ref), O.rms_relative_error(a12, ref)
     assert e3 < 0.01
     assert e3 < e12
@@ -91,58 +100,58 @@ def test_theta_tradeoff_and_accuracy(cuda, ctx, leaf):
     assert w(s3) > w(s12)
 
 
-def test_tree_structure_and_determinism(cuda, ctx):
+def test_tree_structure_and_determinism(cuda, ctx, walk):
     """barnes_hut_test.c:162-214: spiral galaxy N=400 seed 99, one particle per leaf."""
     p = O.preset("spiral_galaxy", 400, 99)
-    a, st = bh(cuda, p, 0.05, 0.7, ctx, leaf=1)
+    a, st = bh(cuda, p, 0.05, 0.7, ctx, leaf=1, walk=walk)
     assert st["leaf_count"] == 400
     assert st["node_count"] <= 800
     assert st["internal_node_count"] > 0
     assert st["maximum_depth"] >= 2
-    b, _ = bh(cuda, p, 0.05, 0.7, ctx, leaf=1)
+    b, _ = bh(cuda, p, 0.05, 0.7, ctx, leaf=1, walk=walk)
     assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("theta", [0.3, 0.5, 0.7, 1.0])
-def test_no_less_accurate_than_reference_barnes_hut(cuda, ctx, theta):
+def test_no_less_accurate_than_reference_barnes_hut(cuda, ctx, theta, walk):
     p = O.preset("globular_cluster", 20000, 4)
     ref = O.gravity_reference(p.copy(), 1.0, 0.01, openmp=True)
     cpu, _ = O.barnes_hut(p.copy(), 1.0, 0.01, theta)
-    gpu, _ = bh(cuda, p, 0.01, theta, ctx)
+    gpu, _ = bh(cuda, p, 0.01, theta, ctx, walk=walk)
     e_cpu, e_gpu = O.rms_relative_error(cpu, ref), O.rms_relative_error(gpu, ref)
     print(f"theta={theta} cpu={e_cpu:.3e} gpu={e_gpu:.3e}")
     assert e_gpu <= e_cpu + 1e-6
 
 
-def test_quadrupole_is_more_accurate(cuda, ctx):
+def test_quadrupole_is_more_accurate(cuda, ctx, walk):
     p = O.preset("globular_cluster", 20000, 4)
     ref = O.gravity_reference(p.copy(), 1.0, 0.01, openmp=True)
-    mono, _ = bh(cuda, p, 0.01, 0.7, ctx, order=1)
-    quad, _ = bh(cuda, p, 0.01, 0.7, ctx, order=2)
+    mono, _ = bh(cuda, p, 0.01, 0.7, ctx, order=1, walk=walk)
+    quad, _ = bh(cuda, p, 0.01, 0.7, ctx, order=2, walk=walk)
     e1, e2 = O.rms_relative_error(mono, ref), O.rms_relative_error(quad, ref)
     print(f"monopole={e1:.3e} quadrupole={e2:.3e}")
     assert e2 < 0.5 * e1
 
 
-def test_collision_config_accuracy(cuda, ctx):
+def test_collision_config_accuracy(cuda, ctx, walk):
     """Config-2 shape at N=200k: two Plummer spheres 10 apart, eps 0.01, theta 0.7,
     vs the FP64 oracle on 1024 seeded targets."""
     p = O.preset("plummer_collision", 200000, 42)
     targets = np.random.default_rng(2).choice(p.n, 1024, replace=False)
     ref = O.gravity_subset(p, 1.0, 0.01, targets)
-    a, st = bh(cuda, p, 0.01, 0.7, ctx)
+    a, st = bh(cuda, p, 0.01, 0.7, ctx, walk=walk)
     e1 = O.rms_relative_error(a[targets], ref)
-    a2, _ = bh(cuda, p, 0.01, 0.7, ctx, order=2)
+    a2, _ = bh(cuda, p, 0.01, 0.7, ctx, order=2, walk=walk)
     e2 = O.rms_relative_error(a2[targets], ref)
     print(f"collision200k mono={e1:.3e} quad={e2:.3e} stats={st}")
     assert e1 < 1e-2 and e2 < e1
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 33, 4097, 10000])
-def test_ragged_sizes(cuda, ctx, n):
+def test_ragged_sizes(cuda, ctx, n, walk):
     p = O.preset("globular_cluster", n, 6)
     ref = O.gravity_reference(p.copy(), 1.0, 0.01)
-    a, st = bh(cuda, p, 0.01, 0.5, ctx)
+    a, st = bh(cuda, p, 0.01, 0.5, ctx, walk=walk)
     if n == 1:
         assert np.all(a == 0.0)
     else:
@@ -150,7 +159,7 @@ def test_ragged_sizes(cuda, ctx, n):
     assert st["node_count"] >= 1
 
 
-def test_duplicate_positions_overflow_like_reference(cuda, ctx):
+def test_duplicate_positions_overflow_like_reference(cuda, ctx, walk):
     """barnes_hut.c:149-153: duplicate positions -> OVERFLOW."""
     p = O.preset("random_cloud", 500, 3)
     p.x[10], p.y[10], p.z[10] = p.x[20], p.y[20], p.z[20]
@@ -162,7 +171,7 @@ def test_duplicate_positions_overflow_like_reference(cuda, ctx):
     bh(cuda, p, 0.01, 0.7, ctx)  # the context stays usable
 
 
-def test_barnes_hut_kdk_steps(cuda, ctx):
+def test_barnes_hut_kdk_steps(cuda, ctx, walk):
     """Leapfrog with barnes_hut_cuda forces tracks the all-pairs oracle run."""
     p = O.preset("globular_cluster", 20000, 12)
     g = cuda.gravity_init(1.0, 0.01)
@@ -171,6 +180,7 @@ def test_barnes_hut_kdk_steps(cuda, ctx):
     O.advance(q, 1.0, 0.01, 1e-3, 3, integrator=1, force=1)
     ctx.theta = 0.5
     ctx.set_multipole_order(2)
+    ctx.set_walk(walk)
     s = to_system(cuda, p)
     ctx.upload(s)
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)

@@ -4,7 +4,9 @@ gravity.c:37-67), in both the persistent graph-captured launch and the
 one-launch-per-system baseline.
 
 Tolerances (FP32 forces, FP64 state, 10 steps at dt = 1e-3): positions
-within 1e-10 absolute, velocities within 1e-8 of the FP64 oracle run.
+within 1e-10 absolute, velocities within 1e-7 of the FP64 oracle run (FP32
+force error ~1e-6 |a|, |a| up to ~10 in the smallest, tightest systems, times
+10 steps of 1e-3).
 """
 import numpy as np
 import pytest
@@ -44,7 +46,7 @@ def check(nb, s, offsets, expected):
         for f in ("x", "y", "z"):
             assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < 1e-10, (k, f)
         for f in ("vx", "vy", "vz"):
-            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < 1e-8, (k, f)
+            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < 1e-7, (k, f)
 
 
 @pytest.mark.parametrize("per_system", [False, True])
