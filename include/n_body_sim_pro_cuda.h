@@ -312,6 +312,70 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_synchronize(
 /* Name of the library's GPU architecture target ("sm_100a"). */
 N_BODY_SIM_PRO_CUDA_API const char* n_body_sim_pro_cuda_architecture(void);
 
+/* ---- learned far-field correction ------------------------------------------------ */
+
+/*
+ * A small MLP (10 -> 64 -> 64 -> 3, GELU; BF16 tensor-core products with FP32
+ * accumulation) predicting, for a cell accepted by the opening test, the
+ * residual between the exact cell sum and the cell's monopole term, in units
+ * of G M / |d|^2.  Inputs: the target offset from the cell's centre of mass
+ * over the cell side (3), the opening ratio side / |d| (1), the trace-free
+ * quadrupole over M side^2 (5) and sum m |x - com|^2 over M side^2 (1).  It is
+ * trained on the GPU from (cell, target) pairs of a resident system with exact
+ * cell sums.  In the walk it is evaluated once per accepted cell and group of
+ * 32 targets, at the group's centre; cells whose inputs fall outside the range
+ * seen in training keep the plain monopole.  The reference engine has no such
+ * component (its Barnes-Hut is monopole-only, barnes_hut.c:600-612).
+ */
+typedef struct NBodySimProCudaCorrection NBodySimProCudaCorrection;
+
+enum {
+    N_BODY_SIM_PRO_CUDA_CORRECTION_PARAMETERS = 5059, /* W1[64][10] b1 W2[64][64] b2 W3[3][64] b3 */
+    N_BODY_SIM_PRO_CUDA_CORRECTION_SCALING = 46       /* x mean, 1/std, min, max [10]; y mean, std [3] */
+};
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProCudaCorrection* n_body_sim_pro_cuda_correction_create(
+    uint64_t seed, NBodySimProError* error);
+N_BODY_SIM_PRO_CUDA_API void n_body_sim_pro_cuda_correction_destroy(
+    NBodySimProCudaCorrection* correction);
+
+/* Sample `samples` (cell, target) pairs from the resident system of `context`
+ * (cells accepted at `theta` by the reference criterion), label them with exact
+ * cell sums, and standardise: the training set (last sixteenth: validation). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_generate(
+    NBodySimProCudaCorrection* correction, NBodySimProCudaContext* context,
+    const NBodySimProGravity* gravity, double theta, size_t samples, uint64_t seed,
+    NBodySimProError* error);
+
+/* Minibatch Adam on the GPU; per-epoch mean squared errors (standardised units). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_train(
+    NBodySimProCudaCorrection* correction, int epochs, int batch, double learning_rate,
+    double* train_loss, double* validation_loss, NBodySimProError* error);
+
+/* FP32 parameters (N_BODY_SIM_PRO_CUDA_CORRECTION_PARAMETERS) and scaling table. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_get_parameters(
+    NBodySimProCudaCorrection* correction, float* parameters, float* scaling,
+    NBodySimProError* error);
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_set_parameters(
+    NBodySimProCudaCorrection* correction, const float* parameters, const float* scaling,
+    NBodySimProError* error);
+
+/* Gradient of the mean squared error over `rows` (a multiple of 128)
+ * standardised rows, from the tensor-core forward/backward kernels. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_gradient(
+    NBodySimProCudaCorrection* correction, const float* features, const float* labels,
+    size_t rows, float* gradient, double* loss, NBodySimProError* error);
+
+/* Copy up to max_rows raw (feature, label) training rows; *rows = rows held. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_samples(
+    NBodySimProCudaCorrection* correction, size_t* rows, float* features, float* labels,
+    size_t max_rows, NBodySimProError* error);
+
+/* Correct the Barnes-Hut walk of `context` with `correction` (NULL: plain). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_correction(
+    NBodySimProCudaContext* context, const NBodySimProCudaCorrection* correction,
+    NBodySimProError* error);
+
 /* ---- ensembles of many small systems ------------------------------------------- */
 
 /*

@@ -216,6 +216,25 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_ensemble_advance": (st, [vp, pg, C.c_double, C.c_int, C.c_int, pe]),
         "n_body_sim_pro_cuda_ensemble_info": (st, [vp, C.POINTER(EnsembleInfo), pe]),
         "n_body_sim_pro_cuda_measure_fp32_peak": (st, [C.POINTER(C.c_double)] * 4 + [pe]),
+        "n_body_sim_pro_cuda_correction_create": (vp, [C.c_uint64, pe]),
+        "n_body_sim_pro_cuda_correction_destroy": (None, [vp]),
+        "n_body_sim_pro_cuda_correction_generate": (st, [vp, vp, pg, C.c_double, C.c_size_t,
+                                                         C.c_uint64, pe]),
+        "n_body_sim_pro_cuda_correction_train": (st, [vp, C.c_int, C.c_int, C.c_double,
+                                                      C.POINTER(C.c_double),
+                                                      C.POINTER(C.c_double), pe]),
+        "n_body_sim_pro_cuda_correction_get_parameters": (st, [vp, C.POINTER(C.c_float),
+                                                               C.POINTER(C.c_float), pe]),
+        "n_body_sim_pro_cuda_correction_set_parameters": (st, [vp, C.POINTER(C.c_float),
+                                                               C.POINTER(C.c_float), pe]),
+        "n_body_sim_pro_cuda_correction_gradient": (st, [vp, C.POINTER(C.c_float),
+                                                         C.POINTER(C.c_float), C.c_size_t,
+                                                         C.POINTER(C.c_float),
+                                                         C.POINTER(C.c_double), pe]),
+        "n_body_sim_pro_cuda_correction_samples": (st, [vp, C.POINTER(C.c_size_t),
+                                                        C.POINTER(C.c_float),
+                                                        C.POINTER(C.c_float), C.c_size_t, pe]),
+        "n_body_sim_pro_cuda_context_set_correction": (st, [vp, vp, pe]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -368,6 +387,12 @@ class CudaContext:
         _check(library().n_body_sim_pro_cuda_context_set_walk(self.handle, int(walk),
                                                               C.byref(err)), err)
 
+    def set_correction(self, correction: "CudaCorrection | None") -> None:
+        err = Error()
+        h = correction.handle if correction is not None else None
+        _check(library().n_body_sim_pro_cuda_context_set_correction(self.handle, h,
+                                                                    C.byref(err)), err)
+
     def set_leaf_capacity(self, capacity: int) -> None:
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_leaf_capacity(self.handle, capacity,
@@ -508,3 +533,94 @@ class CudaEnsemble:
         _check(library().n_body_sim_pro_cuda_ensemble_info(self.handle, C.byref(i), C.byref(err)),
                err)
         return i.as_dict()
+
+
+CORRECTION_PARAMETERS = 5059
+CORRECTION_SCALING = 46
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class CudaCorrection:
+    """NBodySimProCudaCorrection: the learned far-field correction MLP."""
+
+    def __init__(self, seed: int = 1):
+        err = Error()
+        h = library().n_body_sim_pro_cuda_correction_create(seed, C.byref(err))
+        if not h:
+            raise CudaError(err.status or Status.UNSUPPORTED_PLATFORM,
+                            err.message.decode(errors="replace"))
+        self.handle = C.c_void_p(h)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            library().n_body_sim_pro_cuda_correction_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def generate(self, context: CudaContext, gravity: Gravity, theta: float, samples: int,
+                 seed: int = 7) -> None:
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_generate(
+            self.handle, context.handle, C.byref(gravity), float(theta), int(samples), seed,
+            C.byref(err)), err)
+
+    def train(self, epochs: int, batch: int = 4096, learning_rate: float = 1e-3):
+        tl = np.zeros(max(epochs, 1))
+        vl = np.zeros(max(epochs, 1))
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_train(
+            self.handle, int(epochs), int(batch), float(learning_rate),
+            tl.ctypes.data_as(C.POINTER(C.c_double)), vl.ctypes.data_as(C.POINTER(C.c_double)),
+            C.byref(err)), err)
+        return tl[:epochs], vl[:epochs]
+
+    def parameters(self):
+        p = np.zeros(CORRECTION_PARAMETERS, dtype=np.float32)
+        s = np.zeros(CORRECTION_SCALING, dtype=np.float32)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_get_parameters(
+            self.handle, _fptr(p), _fptr(s), C.byref(err)), err)
+        return p, s
+
+    def set_parameters(self, params=None, scaling=None) -> None:
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        s = None if scaling is None else np.ascontiguousarray(scaling, dtype=np.float32)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_set_parameters(
+            self.handle, None if p is None else _fptr(p), None if s is None else _fptr(s),
+            C.byref(err)), err)
+
+    def gradient(self, features: np.ndarray, labels: np.ndarray):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(labels, dtype=np.float32)
+        g = np.zeros(CORRECTION_PARAMETERS, dtype=np.float32)
+        loss = C.c_double(0.0)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_gradient(
+            self.handle, _fptr(x), _fptr(y), x.shape[0], _fptr(g), C.byref(loss), C.byref(err)),
+            err)
+        return g, loss.value
+
+    def samples(self, max_rows: int = 1 << 20):
+        rows = C.c_size_t(0)
+        f = np.zeros((max_rows, 10), dtype=np.float32)
+        lab = np.zeros((max_rows, 3), dtype=np.float32)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_samples(
+            self.handle, C.byref(rows), _fptr(f), _fptr(lab), max_rows, C.byref(err)), err)
+        k = min(rows.value, max_rows)
+        return f[:k], lab[:k], rows.value

@@ -103,6 +103,7 @@ struct NBodySimProCudaContext {
     int multipole_order;
     int leaf_capacity;
     int walk_mode;
+    const void* correction; /* device network of the learned correction, or NULL */
     NbspBarnesHut* bh;
     int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
 
@@ -228,6 +229,14 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(NBodySimProCudaContext* c
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown Barnes-Hut walk");
     c->walk_mode = walk == N_BODY_SIM_PRO_CUDA_WALK_STACKLESS ? NBSP_BH_WALK_STACKLESS
                                                               : NBSP_BH_WALK_LISTS;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_correction(
+    NBodySimProCudaContext* c, const NBodySimProCudaCorrection* correction,
+    NBodySimProError* error) {
+    if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
+    c->correction = nbsp_correction_net(correction);
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
@@ -454,6 +463,7 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.multipole_order = c->multipole_order;
         p.leaf_capacity = c->leaf_capacity;
         p.walk_mode = c->walk_mode;
+        p.correction = c->correction;
         NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
         c->bh_pending = 1;
         return nbsp_bh_accelerations(&c->bh, &s, &p, c->status, c->stream, &c->stats,
@@ -850,6 +860,29 @@ NBodySimProStatus n_body_sim_pro_cuda_morton_order(NBodySimProCudaContext* c, ui
         nbsp_bh_morton(&c->bh, &s, c->status, c->stream, keys_sorted, permutation, root, error);
     if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
     return check_device_status(c, error);
+}
+
+NBodySimProStatus nbsp_context_tree(NBodySimProCudaContext* c, const NBodySimProGravity* gravity,
+                                    NbspTreeRef* out, NBodySimProError* error) {
+    if (c == NULL || gravity == NULL || out == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context and gravity must not be null");
+    if (!c->resident || c->n < 2)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "need a resident system of >= 2 particles");
+    NBodySimProStatus st = check_gravity(gravity, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const void* saved = c->correction;
+    c->correction = NULL; /* the plain tree and walk */
+    st = resident_accelerations(c, gravity, N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT, error);
+    c->correction = saved;
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    out->pos4 = nbsp_bh_positions(c->bh);
+    out->tree = nbsp_bh_tree(c->bh);
+    out->n = c->n;
+    out->stream = c->stream;
+    out->status = c->status;
+    return N_BODY_SIM_PRO_STATUS_OK;
 }
 
 NBodySimProStatus n_body_sim_pro_cuda_synchronize(NBodySimProCudaContext* c,

@@ -18,6 +18,7 @@
 // against the FP64 all-pairs oracle, and the opening test is the reference's:
 // accept a cell when (2h)^2 < theta^2 d^2, d to the cell centre of mass.
 #include "bh.h"
+#include "mlp.cuh"
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -387,6 +388,9 @@ struct Tree {
   float* ropen2;      // (2h / theta)^2
   float4* quad;       // 2 per node: (xx, xy, xz, yy), (yz, 0, 0, 0)
   int* children;      // 8 per internal node, depth-first order (interaction-list walk)
+  double* trace64;    // sum m |x - com|^2 per node (FP64)
+  float* side;        // cell side 2h = root side / 2^level
+  float* spread;      // sum m |x - com|^2 / (M side^2): the correction MLP's 10th feature
   unsigned long long* leaves;  // [1]
 };
 
@@ -426,6 +430,9 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.ropen2 = carve<float>(p, nb);
   t.quad = carve<float4>(p, 2 * nb);
   t.children = carve<int>(p, 8 * nb);
+  t.trace64 = carve<double>(p, nb);
+  t.side = carve<float>(p, nb);
+  t.spread = carve<float>(p, nb);
   t.leaves = carve<unsigned long long>(p, 1);
   if (end != nullptr) *end = p;
   return t;
@@ -653,17 +660,21 @@ __global__ void place_kernel(Tree t, int leaf_capacity, int* status) {
 struct Moments {
   double m, cx, cy, cz;
   double q[6];  // xx xy xz yy yz zz
+  double t2;    // sum m |x - com|^2
 };
 
 __device__ void finish_node(const Tree& t, int node, const Moments& mo, double root_size,
                             double inv_theta2, int lvl) {
   t.mom[node] = make_double4(mo.m, mo.cx, mo.cy, mo.cz);
   for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
+  t.trace64[node] = mo.t2;
   t.com[node] = make_float4((float)mo.cx, (float)mo.cy, (float)mo.cz, (float)mo.m);
   // cell side 2h = root side / 2^lvl ; accept when (2h)^2 < theta^2 d^2
   const double side = ldexp(root_size, -min(lvl, 21));
   const double r2 = side * side * inv_theta2;
   t.ropen2[node] = (float)r2;
+  t.side[node] = (float)side;
+  t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
   t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
   t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
 }
@@ -705,11 +716,13 @@ __global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
     mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
     mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
     for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
+    mo.t2 = 0.0;
     for (int j = info.y; j < info.y + info.z; ++j) {
       const float4 p = pos[j];
       const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
       const double r2 = dx * dx + dy * dy + dz * dz;
       const double w = (double)p.w;
+      mo.t2 += w * r2;
       mo.q[0] += w * (3.0 * dx * dx - r2);
       mo.q[1] += w * (3.0 * dx * dy);
       mo.q[2] += w * (3.0 * dx * dz);
@@ -756,12 +769,14 @@ __global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
     pm.cy = m != 0.0 ? sy / m : 0.0;
     pm.cz = m != 0.0 ? sz / m : 0.0;
     for (int k = 0; k < 6; ++k) pm.q[k] = 0.0;
+    pm.t2 = 0.0;
     c = parent + 1;
     while (c != pinfo.x) {
       const double4 cm = ldcg_d4(&t.mom[c]);
       const double dx = cm.y - pm.cx, dy = cm.z - pm.cy, dz = cm.w - pm.cz;
       const double r2 = dx * dx + dy * dy + dz * dz;
       const double w = cm.x;
+      pm.t2 += __ldcg(&t.trace64[c]) + w * r2;
       pm.q[0] += __ldcg(&t.quad64[6 * c + 0]) + w * (3.0 * dx * dx - r2);
       pm.q[1] += __ldcg(&t.quad64[6 * c + 1]) + w * (3.0 * dx * dy);
       pm.q[2] += __ldcg(&t.quad64[6 * c + 2]) + w * (3.0 * dx * dz);
@@ -963,6 +978,220 @@ __device__ __forceinline__ void cell_term(const Tree& t, int node, float4 c, flo
   pz = fmaf(w, dz, pz);
 }
 
+// ---------------------------------------------------------------------------
+// learned far-field correction: features, training pairs, labels
+// ---------------------------------------------------------------------------
+
+// The 10 MLP inputs of cell `node` seen from point (tx, ty, tz) (coordinates
+// relative to the system's centre of mass, like the node data):
+//   f0..2 = (t - com) / side          f3 = side / |t - com|   (opening ratio)
+//   f4..8 = trace-free Q / (M side^2): xx, xy, xz, yy, yz
+//   f9    = sum m |x - com|^2 / (M side^2)
+// false for a massless cell.
+__device__ __forceinline__ bool cell_features(const Tree& t, int node, float4 c, float tx,
+                                              float ty, float tz, float* f) {
+  const float s = t.side[node];
+  if (!(c.w > 0.f) || !(s > 0.f)) return false;
+  const float rx = tx - c.x, ry = ty - c.y, rz = tz - c.z;
+  const float inv_s = 1.f / s;
+  const float d = sqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+  if (!(d > 0.f)) return false;
+  f[0] = rx * inv_s;
+  f[1] = ry * inv_s;
+  f[2] = rz * inv_s;
+  f[3] = s / d;
+  const float4 qa = t.quad[2 * node];
+  const float qyz = t.quad[2 * node + 1].x;
+  const float qs = 1.f / (c.w * s * s);
+  f[4] = qa.x * qs;
+  f[5] = qa.y * qs;
+  f[6] = qa.z * qs;
+  f[7] = qa.w * qs;
+  f[8] = qyz * qs;
+  f[9] = t.spread[node];
+  return true;
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Training pairs: sample k picks a random target and, walking the tree with the
+// reference criterion at theta_train, one of the cells that target accepts,
+// uniformly (reservoir sampling).  Up to 8 targets are tried per sample.
+__global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, float theta,
+                                 unsigned long long seed, int samples, int* __restrict__ target,
+                                 int* __restrict__ cell, int* status) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= samples) return;
+  const int total = (int)t.offset[n];
+  const float th2 = theta * theta;
+  unsigned long long state = mix64(seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(k + 1)));
+  int chosen = -1, tgt = 0;
+  for (int attempt = 0; attempt < 8 && chosen < 0; ++attempt) {
+    state = mix64(state + 0x9E3779B97F4A7C15ull);
+    tgt = (int)(state % (unsigned long long)n);
+    const float4 p = pos[tgt];
+    unsigned count = 0;
+    int node = 0, steps = 0;
+    while ((unsigned)node < (unsigned)total) {
+      if (++steps > total + 64) {
+        atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
+        break;
+      }
+      const int4 info = t.info[node];
+      if (info.z > 0 || info.x <= node) {
+        node = info.x > node ? info.x : total;
+        continue;
+      }
+      const float4 c = t.com[node];
+      const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float s = t.side[node];
+      if (d2 > 0.f && s * s < th2 * d2 && c.w > 0.f) {
+        ++count;
+        state = mix64(state + 0x9E3779B97F4A7C15ull);
+        if (state % count == 0) chosen = node;
+        node = info.x;
+      } else {
+        node = node + 1;
+      }
+    }
+  }
+  target[k] = tgt;
+  cell[k] = chosen;
+}
+
+// Labels from exact cell sums (all-pairs arithmetic, gravity.c:46-61, FP32
+// with compensated per-lane sums; target excluded): one warp per pair.
+//   label = (a_exact - a_monopole) |d|^2 / M   (units of G; d = com - target)
+__global__ void mlp_labels_kernel(const float4* __restrict__ pos, int n, Tree t,
+                                  const int* __restrict__ target, const int* __restrict__ cell,
+                                  int samples, float eps2, float* __restrict__ feat,
+                                  float* __restrict__ lab, int* __restrict__ ok) {
+  const int lane = threadIdx.x & 31;
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= samples) return;
+  const int node = cell[k], i = target[k];
+  const int total = (int)t.offset[n];
+  if (node < 0 || node >= total || i < 0 || i >= n) {
+    if (lane == 0) ok[k] = 0;
+    return;
+  }
+  const int4 info = t.info[node];
+  const float4 p = pos[i];
+  float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+  // A node's particles: [its first particle, the first particle of the node
+  // that follows its subtree) — or its own count for a leaf.
+  const int first = info.y;
+  const int end = info.z > 0 ? first + info.z : (info.x < total ? t.info[info.x].y : n);
+  float px = 0.f, py = 0.f, pz = 0.f;
+  int pending = 0;
+  for (int j = first + lane; j < end; j += 32) {
+    if (j == i) continue;
+    const float4 q = pos[j];
+    const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    const float rinv = rsqrt_mufu(r2);
+    const float w = q.w * (rinv * rinv * rinv);
+    px = fmaf(w, dx, px);
+    py = fmaf(w, dy, py);
+    pz = fmaf(w, dz, pz);
+    if (++pending == 32) {
+      fold(hx, lx, px);
+      fold(hy, ly, py);
+      fold(hz, lz, pz);
+      px = py = pz = 0.f;
+      pending = 0;
+    }
+  }
+  fold(hx, lx, px);
+  fold(hy, ly, py);
+  fold(hz, lz, pz);
+  double ax = (double)hx + (double)lx, ay = (double)hy + (double)ly, az = (double)hz + (double)lz;
+  for (int off = 16; off > 0; off >>= 1) {
+    ax += __shfl_xor_sync(kFull, ax, off);
+    ay += __shfl_xor_sync(kFull, ay, off);
+    az += __shfl_xor_sync(kFull, az, off);
+  }
+  if (lane != 0) return;
+  const float4 c = t.com[node];
+  float f[nbsp_mlp::kIn];
+  if (!cell_features(t, node, c, p.x, p.y, p.z, f)) {
+    ok[k] = 0;
+    return;
+  }
+  const double dx = (double)c.x - p.x, dy = (double)c.y - p.y, dz = (double)c.z - p.z;
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  const double r2 = d2 + (double)eps2;
+  const double mono = (double)c.w / (r2 * sqrt(r2));
+  const double scale = d2 / (double)c.w;
+  for (int q = 0; q < nbsp_mlp::kIn; ++q) feat[(size_t)k * nbsp_mlp::kIn + q] = f[q];
+  lab[(size_t)k * 3 + 0] = (float)((ax - mono * dx) * scale);
+  lab[(size_t)k * 3 + 1] = (float)((ay - mono * dy) * scale);
+  lab[(size_t)k * 3 + 2] = (float)((az - mono * dz) * scale);
+  ok[k] = 1;
+}
+
+// Column statistics of the kept rows: mean, 1/std, min, max of the 10 features
+// and mean, std of the 3 labels, into the network's scaling tables.
+__global__ void mlp_stats_kernel(const float* __restrict__ feat, const float* __restrict__ lab,
+                                 const int* __restrict__ ok, int rows, nbsp_mlp::Net* net) {
+  __shared__ double sh[4][256];
+  const int col = blockIdx.x;  // 0..9 features, 10..12 labels
+  const float* src = col < nbsp_mlp::kIn ? feat : lab;
+  const int stride = col < nbsp_mlp::kIn ? nbsp_mlp::kIn : 3;
+  const int c = col < nbsp_mlp::kIn ? col : col - nbsp_mlp::kIn;
+  double s = 0.0, s2 = 0.0, mn = 1e300, mx = -1e300, cnt = 0.0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    if (ok != nullptr && !ok[r]) continue;
+    const double v = src[(size_t)r * stride + c];
+    s += v;
+    s2 += v * v;
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+    cnt += 1.0;
+  }
+  sh[0][threadIdx.x] = s;
+  sh[1][threadIdx.x] = s2;
+  sh[2][threadIdx.x] = cnt;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  const double tot = sh[0][0], tot2 = sh[1][0], n = sh[2][0];
+  __syncthreads();
+  sh[0][threadIdx.x] = mn;
+  sh[1][threadIdx.x] = mx;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      sh[0][threadIdx.x] = fmin(sh[0][threadIdx.x], sh[0][threadIdx.x + st]);
+      sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][threadIdx.x + st]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double mean = n > 0 ? tot / n : 0.0;
+  const double var = n > 1 ? fmax(tot2 / n - mean * mean, 0.0) : 1.0;
+  const double sd = var > 1e-30 ? sqrt(var) : 1.0;
+  if (col < nbsp_mlp::kIn) {
+    net->x_mean[c] = (float)mean;
+    net->x_inv_std[c] = (float)(1.0 / sd);
+    net->x_min[c] = (float)sh[0][0];
+    net->x_max[c] = (float)sh[1][0];
+  } else {
+    net->y_mean[c] = (float)mean;
+    net->y_std[c] = (float)sd;
+  }
+}
+
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> stackless walk
@@ -976,13 +1205,24 @@ constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> sta
 // cells are appended to two lists that are evaluated, whenever 32 have
 // gathered, in dense loops where every lane computes its own target's terms.
 // A warp whose stack would overflow restarts with the stackless walk.
-template <int ORDER, int STACK>
+//
+// CORR: the learned far-field correction.  At every cell flush the gathered
+// cells' features are taken at the group centre, standardised, and pushed
+// through the MLP 16 cells at a time (one m16 tile per mma.sync); each target
+// then adds (M / |d|^2) * y to its monopole term, y the de-standardised network
+// output and d its own distance to the cell's centre of mass.  Cells whose
+// features fall outside the range seen in training keep the plain monopole.
+template <int ORDER, int STACK, bool CORR>
 __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
     const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
-    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
+    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status,
+    const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ int s_cells[kListThreads / 32][kListCap];
   __shared__ int s_leaves[kListThreads / 32][kListCap];
+  __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
+  __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
+  __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
@@ -1077,10 +1317,62 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
     const bool drain = top == 0;
     if (ncell >= 32 || (drain && ncell > 0)) {
       float px = 0.f, py = 0.f, pz = 0.f;
+      if (CORR) {
+        uint32_t* xs = s_x[wib];
+        float* ys = s_y[wib];
+        int* oks = s_ok[wib];
+        const int padded = (ncell + 15) & ~15;
+        for (int r = lane; r < padded; r += 32) {
+          float f[nbsp_mlp::kIn];
+          bool ok = false;
+          if (r < ncell) {
+            const int node = cells[r];
+            ok = cell_features(t, node, t.com[node], gx, gy, gz, f);
+#pragma unroll
+            for (int q = 0; q < nbsp_mlp::kIn; ++q)
+              ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
+          }
+#pragma unroll
+          for (int w = 0; w < 8; ++w) {
+            const int q0 = 2 * w, q1 = 2 * w + 1;
+            const float v0 = ok && q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
+            const float v1 = ok && q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
+            xs[r * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
+          }
+          oks[r] = ok ? 1 : 0;
+        }
+        __syncwarp();
+        const int gq = lane >> 2, tq = lane & 3;
+        for (int mt = 0; mt < padded / 16; ++mt) {
+          const int ra = mt * 16 + gq, rb = ra + 8;
+          const uint32_t xa[4] = {xs[ra * 8 + tq], xs[rb * 8 + tq], xs[ra * 8 + tq + 4],
+                                  xs[rb * 8 + tq + 4]};
+          float out[4];
+          nbsp_mlp::forward_tile(xa, net->w1, net->b1, net->w2, net->b2, net->w3, net->b3, lane,
+                                 out);
+          if (tq < 2) {
+            ys[ra * 4 + 2 * tq] = out[0];
+            ys[ra * 4 + 2 * tq + 1] = out[1];
+            ys[rb * 4 + 2 * tq] = out[2];
+            ys[rb * 4 + 2 * tq + 1] = out[3];
+          }
+        }
+        __syncwarp();
+      }
       for (int e = 0; e < ncell; ++e) {
         const int node = cells[e];
-        cell_term<ORDER>(t, node, t.com[node], p, eps2, px, py, pz);
+        const float4 c = t.com[node];
+        cell_term<ORDER>(t, node, c, p, eps2, px, py, pz);
+        if (CORR && s_ok[wib][e]) {
+          const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+          const float scale = c.w / fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          const float* ye = &s_y[wib][e * 4];
+          px = fmaf(scale, fmaf(ye[0], net->y_std[0], net->y_mean[0]), px);
+          py = fmaf(scale, fmaf(ye[1], net->y_std[1], net->y_mean[1]), py);
+          pz = fmaf(scale, fmaf(ye[2], net->y_std[2], net->y_mean[2]), pz);
+        }
       }
+      if (CORR) __syncwarp();
       fold(hx, lx, px);
       fold(hy, ly, py);
       fold(hz, lz, pz);
@@ -1236,19 +1528,25 @@ void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry, double 
                                                                    geometry, inv_theta2, status);
 }
 
-void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode, float eps2,
-                  void* acc_hi, void* acc_lo, unsigned long long* counters, int* status,
-                  cudaStream_t stream) {
+void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
+                  const void* correction, float eps2, void* acc_hi, void* acc_lo,
+                  unsigned long long* counters, int* status, cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
-  if (mode == NBSP_BH_WALK_LISTS) {
+  const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
+  if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
     const float4* p = (const float4*)pos4;
-    if (order == 2) {
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, (float4*)acc_hi, (float4*)acc_lo, counters, status);
+    float4* hi = (float4*)acc_hi;
+    float4* lo = (float4*)acc_lo;
+    if (net != nullptr) {  // the network corrects the monopole term
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true><<<blocks, kListThreads, 0, stream>>>(
+          p, (int)n, t, eps2, hi, lo, counters, status, net);
+    } else if (order == 2) {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
+          p, (int)n, t, eps2, hi, lo, counters, status, nullptr);
     } else {
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, (float4*)acc_hi, (float4*)acc_lo, counters, status);
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
+          p, (int)n, t, eps2, hi, lo, counters, status, nullptr);
     }
     return;
   }
@@ -1269,6 +1567,29 @@ void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* per
   NBSP_COUNT_LAUNCH(1), scatter_kernel<<<grid_for(n, 256), 256, 0, stream>>>((const float4*)acc_hi,
                                                        (const float4*)acc_lo, perm, n, g, ax, ay,
                                                        az);
+}
+
+void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta,
+                       unsigned long long seed, int samples, int* target, int* cell, int* status,
+                       cudaStream_t stream) {
+  Tree t = tree_view(const_cast<void*>(tree), n);
+  NBSP_COUNT_LAUNCH(1), mlp_pairs_kernel<<<(samples + 127) / 128, 128, 0, stream>>>(
+      (const float4*)pos4, (int)n, t, theta, seed, samples, target, cell, status);
+}
+
+void nbsp_bh_mlp_labels(const void* pos4, size_t n, const void* tree, const int* target,
+                        const int* cell, int samples, float eps2, float* feat, float* lab, int* ok,
+                        cudaStream_t stream) {
+  Tree t = tree_view(const_cast<void*>(tree), n);
+  const long long threads = (long long)samples * 32;
+  NBSP_COUNT_LAUNCH(1), mlp_labels_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(
+      (const float4*)pos4, (int)n, t, target, cell, samples, eps2, feat, lab, ok);
+}
+
+void nbsp_bh_mlp_stats(const float* feat, const float* lab, const int* ok, int rows, void* net,
+                       cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), mlp_stats_kernel<<<nbsp_mlp::kIn + nbsp_mlp::kOut, 256, 0, stream>>>(
+      feat, lab, ok, rows, (nbsp_mlp::Net*)net);
 }
 
 void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,

@@ -37,6 +37,7 @@ typedef struct NbspBarnesHutParams {
     int multipole_order;
     int leaf_capacity;
     int walk_mode;
+    const void* correction; /* device network (mlp.cuh Net) or NULL */
 } NbspBarnesHutParams;
 
 typedef struct NbspBarnesHutState {
@@ -116,8 +117,44 @@ enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
  * mode NBSP_BH_WALK_LISTS: lane-parallel node tests against the warp's group
  * box, dense evaluation of gathered interaction lists. */
 NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
-                              float softening_squared, void* acc_hi, void* acc_lo,
-                              unsigned long long* counters, int* status, cudaStream_t stream);
+                              const void* correction, float softening_squared, void* acc_hi,
+                              void* acc_lo, unsigned long long* counters, int* status,
+                              cudaStream_t stream);
+
+/* Learned correction: training pairs (target, accepted cell) sampled with the
+ * reference criterion at theta, their features and exact-sum labels, and the
+ * column statistics written into the network's scaling tables (`net`). */
+NBSP_HIDDEN void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta,
+                                   unsigned long long seed, int samples, int* target, int* cell,
+                                   int* status, cudaStream_t stream);
+NBSP_HIDDEN void nbsp_bh_mlp_labels(const void* pos4, size_t n, const void* tree,
+                                    const int* target, const int* cell, int samples,
+                                    float softening_squared, float* feat, float* lab, int* ok,
+                                    cudaStream_t stream);
+NBSP_HIDDEN void nbsp_bh_mlp_stats(const float* feat, const float* lab, const int* ok, int rows,
+                                   void* net, cudaStream_t stream);
+
+/* A context's freshly built Barnes-Hut tree, for training-pair generation. */
+typedef struct NbspTreeRef {
+    const void* pos4;
+    const void* tree;
+    size_t n;
+    cudaStream_t stream;
+    int* status;
+} NbspTreeRef;
+
+/* Build the tree of the context's resident state (one Barnes-Hut evaluation,
+ * synchronised and checked) and describe it. */
+NBSP_HIDDEN NBodySimProStatus nbsp_context_tree(NBodySimProCudaContext* ctx,
+                                                const NBodySimProGravity* gravity,
+                                                NbspTreeRef* out, NBodySimProError* error);
+
+/* The device network of a correction object (NULL-safe). */
+NBSP_HIDDEN const void* nbsp_correction_net(const NBodySimProCudaCorrection* correction);
+
+/* The last evaluation's Morton-ordered float4 positions and tree scratch. */
+NBSP_HIDDEN const void* nbsp_bh_positions(const NbspBarnesHut* bh);
+NBSP_HIDDEN const void* nbsp_bh_tree(const NbspBarnesHut* bh);
 
 /* a[perm[s]] = G * (hi + lo)[s] */
 NBSP_HIDDEN void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* perm,

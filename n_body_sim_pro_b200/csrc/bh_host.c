@@ -152,7 +152,7 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     cudaEventRecord(b->events[4], stream);
     nbsp_bh_moments(b->pos4, n, b->geometry, p->theta, p->multipole_order, b->tree, status, stream);
     cudaEventRecord(b->events[5], stream);
-    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode,
+    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode, p->correction,
                  (float)p->softening_squared, b->acc_hi,
                  b->acc_lo, b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
@@ -169,6 +169,9 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     (void)timings;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
+
+const void* nbsp_bh_positions(const NbspBarnesHut* b) { return b != NULL ? b->pos4 : NULL; }
+const void* nbsp_bh_tree(const NbspBarnesHut* b) { return b != NULL ? b->tree : NULL; }
 
 static double elapsed(const NbspBarnesHut* b, int from, int to) {
     float ms = 0.f;

@@ -1,0 +1,118 @@
+"""Learned far-field correction: the tensor-core backward pass against the FP64
+CPU MLP (oracle/mlp_oracle.py), training on GPU-generated (cell, target)
+pairs, and what the trained network gains over plain Barnes-Hut.
+
+Gradient tolerance: the GPU rounds inputs, weights and the hidden activations
+to BF16 (8-bit mantissa) between products; against the FP64 chain rule on the
+same BF16-rounded inputs and weights the gradient agrees to ~1e-2 relative,
+bounded here at 5e-2 (L2) with cosine similarity > 0.998, the loss to 2e-2.
+"""
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def to_system(nb, p):
+    return nb.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS])
+
+
+def test_gradient_matches_fp64_cpu(cuda):
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((512, 10)).astype(np.float32)
+    y = (0.3 * rng.standard_normal((512, 3))).astype(np.float32)
+    with cuda.CudaCorrection(seed=3) as corr:
+        p, _ = corr.parameters()
+        g, loss = corr.gradient(x, y)
+    ref_loss, ref_g = M.loss_and_gradient(p, x, y)
+    rel = np.linalg.norm(g - ref_g) / np.linalg.norm(ref_g)
+    cos = float(np.dot(g, ref_g) / (np.linalg.norm(g) * np.linalg.norm(ref_g)))
+    print(f"gradient rel={rel:.3e} cos={cos:.6f} loss={loss:.6f} ref={ref_loss:.6f}")
+    assert abs(loss - ref_loss) <= 2e-2 * ref_loss
+    assert rel < 5e-2 and cos > 0.998
+    # every parameter block receives gradient
+    k = 0
+    for name, shape in M.SIZES:
+        n = int(np.prod(shape))
+        assert np.linalg.norm(g[k:k + n]) > 0, name
+        k += n
+
+
+def test_parameters_round_trip(cuda):
+    with cuda.CudaCorrection(seed=5) as corr:
+        p, s = corr.parameters()
+        q = p * 0.5
+        corr.set_parameters(q, s)
+        p2, s2 = corr.parameters()
+    assert np.array_equal(p2, q) and np.array_equal(s2, s)
+
+
+@pytest.fixture(scope="module")
+def trained(cuda):
+    """A correction trained on the collision config at N = 200k (theta 1.0)."""
+    p = O.preset("plummer_collision", 200000, 42)
+    g = cuda.gravity_init(1.0, 0.01)
+    ctx = cuda.CudaContext(theta=1.0)
+    ctx.upload(to_system(cuda, p))
+    corr = cuda.CudaCorrection(seed=11)
+    corr.generate(ctx, g, theta=1.0, samples=1 << 18, seed=3)
+    tl, vl = corr.train(epochs=6, batch=4096, learning_rate=2e-3)
+    yield p, ctx, corr, tl, vl
+    corr.close()
+    ctx.close()
+
+
+def test_training_data_is_sane(cuda, trained):
+    _, _, corr, _, _ = trained
+    f, lab, rows = corr.samples(max_rows=4096)
+    assert rows >= (1 << 18) * 0.9
+    assert np.all(np.isfinite(f)) and np.all(np.isfinite(lab))
+    assert np.all(f[:, 3] > 0) and np.all(f[:, 3] < 1.0 + 1e-6)  # accepted at theta = 1
+    # the residual of the monopole is a fraction of the monopole itself
+    assert np.median(np.linalg.norm(lab, axis=1)) < 1.0
+
+
+def test_training_lowers_the_loss(cuda, trained):
+    _, _, _, tl, vl = trained
+    print("train loss", tl, "validation loss", vl)
+    assert vl[-1] < 0.5 * vl[0] or vl[-1] < 0.2
+    assert vl[-1] < 1.0  # below the variance of the standardised labels
+
+
+def test_correction_beats_plain_barnes_hut(cuda, trained):
+    p, ctx, corr, _, _ = trained
+    g = cuda.gravity_init(1.0, 0.01)
+    targets = np.random.default_rng(9).choice(p.n, 1024, replace=False)
+    ref = O.gravity_subset(p, 1.0, 0.01, targets)
+    s = to_system(cuda, p)
+    ctx.set_multipole_order(1)
+    ctx.set_correction(None)
+    plain = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)[targets].copy()
+    ctx.set_correction(corr)
+    fixed = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)[targets].copy()
+    ctx.set_correction(None)
+    e_plain = O.rms_relative_error(plain, ref)
+    e_fixed = O.rms_relative_error(fixed, ref)
+    print(f"theta=1.0 plain monopole rms={e_plain:.3e} corrected rms={e_fixed:.3e}")
+    assert e_fixed < 0.8 * e_plain
+
+
+def test_out_of_range_features_fall_back_to_plain(cuda, trained):
+    p, ctx, corr, _, _ = trained
+    g = cuda.gravity_init(1.0, 0.01)
+    s = to_system(cuda, p)
+    params, scaling = corr.parameters()
+    ctx.set_correction(None)
+    plain = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx).copy()
+    with cuda.CudaCorrection(seed=1) as empty:
+        bad = scaling.copy()
+        bad[20:30] = 1e30   # minimum above everything: no cell is in range
+        bad[30:40] = -1e30
+        empty.set_parameters(params, bad)
+        ctx.set_correction(empty)
+        guarded = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx).copy()
+        ctx.set_correction(None)
+    assert np.array_equal(guarded, plain)

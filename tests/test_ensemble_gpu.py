@@ -3,10 +3,10 @@ per-system leapfrog with all-pairs forces (src/c/physics/integrator.c:47-85,
 gravity.c:37-67), in both the persistent graph-captured launch and the
 one-launch-per-system baseline.
 
-Tolerances (FP32 forces, FP64 state, 10 steps at dt = 1e-3): positions
-within 1e-10 absolute, velocities within 1e-7 of the FP64 oracle run (FP32
-force error ~1e-6 |a|, |a| up to ~10 in the smallest, tightest systems, times
-10 steps of 1e-3).
+Tolerances (FP32 forces, FP64 state, T = steps x dt): an FP32 force carries a
+relative error of ~1e-6, so per system with largest acceleration A the bounds
+are |dx| <= 1e-6 A T^2 + 1e-12 and |dv| <= 2e-6 A T + 1e-12 against the FP64
+oracle run (a tight binary of a small system has A ~ 1e3).
 """
 import numpy as np
 import pytest
@@ -40,13 +40,15 @@ def oracle_run(members, eps, dt, steps):
     return out
 
 
-def check(nb, s, offsets, expected):
+def check(nb, s, offsets, expected, span=1e-2):
     for k, q in enumerate(expected):
         a, b = int(offsets[k]), int(offsets[k + 1])
+        amax = float(np.max(np.linalg.norm(q.acc(), axis=1)))
+        tx, tv = 1e-6 * amax * span * span + 1e-12, 2e-6 * amax * span + 1e-12
         for f in ("x", "y", "z"):
-            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < 1e-10, (k, f)
+            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < tx, (k, f)
         for f in ("vx", "vy", "vz"):
-            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < 1e-7, (k, f)
+            assert np.max(np.abs(getattr(s, f)[a:b] - getattr(q, f))) < tv, (k, f)
 
 
 @pytest.mark.parametrize("per_system", [False, True])
@@ -82,7 +84,7 @@ def test_ensemble_repeated_advance_and_graph_reuse(cuda):
         out = cuda.ParticleSystem.zeros(s.n)
         e.download(out)
     # each advance recomputes the initial forces of its first step: same physics
-    check(cuda, out, offsets, expected)
+    check(cuda, out, offsets, expected, span=6e-3)
 
 
 def test_ensemble_rejects_oversized_systems(cuda):
