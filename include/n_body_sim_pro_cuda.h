@@ -192,14 +192,14 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_c
     NBodySimProCudaContext* context, int capacity, NBodySimProError* error);
 
 /* Barnes-Hut walk.  Both accept a cell only when the reference's test
- * (2h)^2 < theta^2 d^2 holds for every target it is applied to
- * (src/c/barnes_hut/barnes_hut.c:596-599); they differ in how 32 targets share
- * the traversal:
+ * (2h)^2 < theta^2 d^2 holds for every one of the 32 Morton-consecutive
+ * targets it is applied to (src/c/barnes_hut/barnes_hut.c:596-599), so both
+ * accept the same cells; they differ in how the traversal is scheduled:
  *   STACKLESS          one node at a time per warp along depth-first skip
- *                      links, opened when any target's own test fails;
- *   INTERACTION_LISTS  (default) 32 nodes per step tested in parallel against
- *                      the warp's bounding box (d measured to the box), accepted
- *                      cells and leaves gathered and evaluated in dense loops. */
+ *                      links;
+ *   INTERACTION_LISTS  (default) 32 nodes per step tested in parallel from a
+ *                      per-warp stack, accepted cells and leaves gathered and
+ *                      evaluated in dense loops. */
 typedef enum NBodySimProCudaWalk {
     N_BODY_SIM_PRO_CUDA_WALK_STACKLESS = 0,
     N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS = 1

@@ -1196,15 +1196,17 @@ constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> stackless walk
 
-// Interaction-list walk.  The 32 Morton-consecutive targets of a warp form a
-// group with an axis-aligned bounding box.  Each step the lanes pop up to 32
-// nodes from the warp's shared-memory stack and test them IN PARALLEL with the
-// group form of the reference criterion: accept when (2h)^2 < theta^2 dmin^2,
-// dmin the distance from the cell's centre of mass to the group box (so every
-// target's own test (2h)^2 < theta^2 d^2 holds as well); leaves and accepted
-// cells are appended to two lists that are evaluated, whenever 32 have
-// gathered, in dense loops where every lane computes its own target's terms.
-// A warp whose stack would overflow restarts with the stackless walk.
+// Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
+// traversal.  Each step the lanes pop up to 32 nodes from the warp's
+// shared-memory stack and test them IN PARALLEL: a node is accepted when every
+// target's own reference test (2h)^2 < theta^2 d^2 holds (d to the cell's
+// centre of mass) — first tried in one shot against the group's bounding box
+// (if the box's nearest point passes, every target does), else target by
+// target from shared memory — so the accepted cells are exactly those of the
+// stackless walk.  Leaves and accepted cells are appended to two lists that
+// are evaluated, whenever 32 have gathered, in dense loops where every lane
+// computes its own target's terms.  A warp whose stack would overflow restarts
+// with the stackless walk.
 //
 // CORR: the learned far-field correction.  At every cell flush the gathered
 // cells' features are taken at the group centre, standardised, and pushed
@@ -1223,6 +1225,7 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
   __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
   __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
   __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
+  __shared__ float4 s_tgt[kListThreads / 32][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
@@ -1233,6 +1236,8 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
   const bool active = s < n;
   const float4 p = pos[active ? s : n - 1];
   const unsigned lt = (1u << lane) - 1u;
+  const int nact = min(32, n - warp * 32);  // targets of this warp
+  s_tgt[wib][lane] = p;
 
   // group bounding box
   float bx0 = p.x, bx1 = p.x, by0 = p.y, by1 = p.y, bz0 = p.z, bz1 = p.z;
@@ -1281,7 +1286,19 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
           const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
           const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
           const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
-          accept = dmin2 > t.ropen2[node];
+          const float ro = t.ropen2[node];
+          accept = dmin2 > ro;  // the whole box passes: every target passes
+          if (!accept) {        // otherwise each target's own test decides
+            accept = true;
+            for (int k = 0; k < nact; ++k) {
+              const float4 q = s_tgt[wib][k];
+              const float ex2 = c.x - q.x, ey2 = c.y - q.y, ez2 = c.z - q.z;
+              if (!(fmaf(ex2, ex2, fmaf(ey2, ey2, ez2 * ez2)) > ro)) {
+                accept = false;
+                break;
+              }
+            }
+          }
           if (!accept) {
             ca = reinterpret_cast<const int4*>(t.children)[2 * node];
             cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];

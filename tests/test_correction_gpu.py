@@ -58,8 +58,8 @@ def trained(cuda):
     ctx = cuda.CudaContext(theta=1.0)
     ctx.upload(to_system(cuda, p))
     corr = cuda.CudaCorrection(seed=11)
-    corr.generate(ctx, g, theta=1.0, samples=1 << 18, seed=3)
-    tl, vl = corr.train(epochs=6, batch=4096, learning_rate=2e-3)
+    corr.generate(ctx, g, theta=1.0, samples=1 << 20, seed=3)
+    tl, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
     yield p, ctx, corr, tl, vl
     corr.close()
     ctx.close()
@@ -68,7 +68,7 @@ def trained(cuda):
 def test_training_data_is_sane(cuda, trained):
     _, _, corr, _, _ = trained
     f, lab, rows = corr.samples(max_rows=4096)
-    assert rows >= (1 << 18) * 0.9
+    assert rows >= (1 << 20) * 0.9
     assert np.all(np.isfinite(f)) and np.all(np.isfinite(lab))
     assert np.all(f[:, 3] > 0) and np.all(f[:, 3] < 1.0 + 1e-6)  # accepted at theta = 1
     # the residual of the monopole is a fraction of the monopole itself
