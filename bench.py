@@ -294,7 +294,9 @@ def run_ours(args, wl, world, rank, local):
             t = ctx.timings()
             step_ms.append(t["total_ms"])
             walk_ms.append(t["walk_ms"])
-            stats_acc.append(ctx.stats())
+            st = ctx.stats()
+            st["walk_restarts"] = ctx.walk_restarts()
+            stats_acc.append(st)
     launches = nb.kernel_launches() - launches0
     barrier_sync(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)

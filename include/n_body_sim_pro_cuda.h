@@ -217,6 +217,12 @@ N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_stats(
 N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_timings(
     const NBodySimProCudaContext* context, NBodySimProCudaTimings* timings);
 
+/* No reference counterpart: in the last Barnes-Hut evaluation, the number of
+ * 32-target groups whose interaction-list stack would have overflowed and that
+ * were walked again by the stackless walk (same forces, more time). 0 for NULL. */
+N_BODY_SIM_PRO_CUDA_API size_t n_body_sim_pro_cuda_context_walk_restarts(
+    const NBodySimProCudaContext* context);
+
 /* ---- force functions (NBodySimProForceFunction) -------------------------------- */
 
 /*

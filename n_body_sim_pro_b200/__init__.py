@@ -150,7 +150,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_advance", "n_body_sim_pro_cuda_diagnostics",
     "n_body_sim_pro_cuda_reference_acceleration", "n_body_sim_pro_cuda_morton_order",
     "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
-    "n_body_sim_pro_cuda_kernel_launches",
+    "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
 )
 
 
@@ -191,6 +191,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_set_walk": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
+        "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
         "n_body_sim_pro_gravity_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
         "n_body_sim_pro_barnes_hut_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
         "n_body_sim_pro_cuda_upload": (st, [vp, pv, pe]),
@@ -408,6 +409,11 @@ class CudaContext:
         t = Timings()
         library().n_body_sim_pro_cuda_context_timings(self.handle, C.byref(t))
         return t.as_dict()
+
+    def walk_restarts(self) -> int:
+        """Groups of the last Barnes-Hut evaluation that the interaction-list
+        walk handed to the stackless walk (stack overflow)."""
+        return int(library().n_body_sim_pro_cuda_context_walk_restarts(self.handle))
 
     def upload(self, system: ParticleSystem) -> None:
         err = Error()

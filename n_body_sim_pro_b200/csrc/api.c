@@ -109,6 +109,7 @@ struct NBodySimProCudaContext {
 
     NBodySimProBarnesHutStats stats;
     NBodySimProCudaTimings timings;
+    size_t walk_restarts; /* groups the interaction-list walk handed to the stackless walk */
 
     TuneEntry tune[TUNE_SLOTS];
     int tune_count;
@@ -254,6 +255,10 @@ int n_body_sim_pro_cuda_context_timings(const NBodySimProCudaContext* c,
     return 0;
 }
 
+size_t n_body_sim_pro_cuda_context_walk_restarts(const NBodySimProCudaContext* c) {
+    return c == NULL ? 0 : c->walk_restarts;
+}
+
 const char* n_body_sim_pro_cuda_architecture(void) { return "sm_100a"; }
 
 unsigned long long nbsp_kernel_launch_count = 0;
@@ -309,7 +314,7 @@ static NBodySimProStatus check_device_status(NBodySimProCudaContext* c, NBodySim
     CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (c->bh_pending) {
-        nbsp_bh_collect(c->bh, &c->stats, &c->timings);
+        nbsp_bh_collect(c->bh, &c->stats, &c->timings, &c->walk_restarts);
         c->bh_pending = 0;
     }
     const int bits = *c->host_status;

@@ -16,7 +16,10 @@
 // `leaf_capacity` Morton-contiguous particles, and stored in depth-first order
 // with skip links so the walk needs no stack.  Parity is judged on forces
 // against the FP64 all-pairs oracle, and the opening test is the reference's:
-// accept a cell when (2h)^2 < theta^2 d^2, d to the cell centre of mass.
+// accept a cell when (2h)^2 < theta^2 d^2, d to the cell centre of mass.  A
+// bucket of >= 2 particles is the reference's cell of the same side and
+// particles, so it takes the same test; where the reference would open it, its
+// particles are summed exactly (a single particle is always exact).
 #include "bh.h"
 #include "mlp.cuh"
 
@@ -812,6 +815,8 @@ constexpr int kWalkThreads = 256;
 // targets and visit the same node sequence; a cell is opened when any lane's
 // opening test fails (so every lane's own test holds for every cell it
 // accepts), otherwise all lanes apply its multipole and skip its subtree.
+// Buckets (leaves of up to leaf_capacity particles) take the same test and are
+// summed particle by particle when it fails; single particles are always exact.
 struct WalkAcc {
   float hx, hy, hz, lx, ly, lz;  // compensated acceleration / G
   unsigned approx, exact;        // accepted cells, particle-particle terms
@@ -839,7 +844,16 @@ __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, i
       if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
       break;
     }
-    if (info.z > 0) {
+    // A bucket of >= 2 particles is a cell like any other: its multipole is
+    // used when every lane's opening test passes (barnes_hut.c:596-599).
+    bool direct = info.z == 1;
+    if (info.z >= 2) {
+      const float4 c = t.com[node];
+      const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      direct = __any_sync(kFull, active && !(d2 > t.ropen2[node]));
+    }
+    if (direct) {
       const int j1 = info.y + info.z;
       for (int j = info.y; j < j1; ++j) {
         const float4 q = pos[j];
@@ -949,9 +963,10 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
 
 // Accepted-cell term (monopole, optionally + trace-free quadrupole), d = com - target:
 // a = G [ M d / r^3 - Q d / r^5 + 5/2 (d.Q.d) d / r^7 ],  r^2 = d^2 + eps^2.
+// c = (com, mass); qa = (Qxx, Qxy, Qxz, Qyy), qyz = Qyz (Qzz = -Qxx - Qyy).
 template <int ORDER>
-__device__ __forceinline__ void cell_term(const Tree& t, int node, float4 c, float4 p, float eps2,
-                                          float& px, float& py, float& pz) {
+__device__ __forceinline__ void cell_term_q(float4 c, float4 qa, float qyz, float4 p, float eps2,
+                                            float& px, float& py, float& pz) {
   const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
   const float rinv = rsqrt_mufu(r2);
@@ -959,8 +974,6 @@ __device__ __forceinline__ void cell_term(const Tree& t, int node, float4 c, flo
   const float rinv3 = rinv * rinv2;
   float w = c.w * rinv3;
   if (ORDER == 2) {
-    const float4 qa = t.quad[2 * node];
-    const float qyz = t.quad[2 * node + 1].x;
     const float qzz = -qa.x - qa.w;
     const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
     const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qyz * dz));
@@ -976,6 +989,113 @@ __device__ __forceinline__ void cell_term(const Tree& t, int node, float4 c, flo
   px = fmaf(w, dx, px);
   py = fmaf(w, dy, py);
   pz = fmaf(w, dz, pz);
+}
+
+// Point sources (bucket particles and monopole cells) gathered per warp in
+// shared memory, interleaved by pairs so that one 16-byte load yields the
+// 64-bit operands {x_2i, x_2i+1} and {y_2i, y_2i+1} (resp. z and m) of the
+// paired .f32x2 instructions.
+constexpr int kStage = 64;              // sources per tile
+constexpr float kFarAway = 1e30f;       // padding: r^2 overflows to inf, rsqrt(inf) = 0
+struct SourceTile {
+  ulonglong2 xy[kStage / 2];  // {x_2i, x_2i+1}, {y_2i, y_2i+1}
+  ulonglong2 zm[kStage / 2];  // {z_2i, z_2i+1}, {m_2i, m_2i+1}
+};
+
+__device__ __forceinline__ void stage_source(SourceTile& s, int k, float4 q) {
+  float* a = reinterpret_cast<float*>(&s.xy[k >> 1]) + (k & 1);
+  float* b = reinterpret_cast<float*>(&s.zm[k >> 1]) + (k & 1);
+  a[0] = q.x;
+  a[2] = q.y;
+  b[0] = q.z;
+  b[2] = q.w;
+}
+
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// The kStage terms of a full tile on this lane's target, two sources per
+// instruction (every lane reads the same words: shared-memory broadcasts),
+// summed in FP32 and folded once.  The target's own entry, when staged, has
+// d = 0 and r^2 = eps^2 exactly: it adds W * 0 = 0 while its weight W = m /
+// eps^3 is finite (checked once per warp by self_term_is_finite); otherwise
+// GUARD drops every term with r^2 <= eps^2 (barnes_hut.c:572 skips it).
+template <bool GUARD>
+__device__ __forceinline__ void source_terms(const SourceTile& s, float4 p, float eps2,
+                                             unsigned long long& ax, unsigned long long& ay,
+                                             unsigned long long& az) {
+  const unsigned long long PX = pack2(p.x, p.x), PY = pack2(p.y, p.y), PZ = pack2(p.z, p.z);
+  const unsigned long long E2 = pack2(eps2, eps2);
+#pragma unroll
+  for (int j = 0; j < kStage / 2; ++j) {
+    const ulonglong2 a = s.xy[j], b = s.zm[j];
+    const unsigned long long dx = sub2(a.x, PX), dy = sub2(a.y, PY), dz = sub2(b.x, PZ);
+    const unsigned long long r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+    float r2a, r2b;
+    unpack2(r2, r2a, r2b);
+    float ra = rsqrt_mufu(r2a), rb = rsqrt_mufu(r2b);
+    if (GUARD) {
+      ra = r2a > eps2 ? ra : 0.f;
+      rb = r2b > eps2 ? rb : 0.f;
+    }
+    const unsigned long long R = pack2(ra, rb);
+    const unsigned long long W = mul2(b.y, mul2(mul2(R, R), R));
+    ax = fma2(W, dx, ax);
+    ay = fma2(W, dy, ay);
+    az = fma2(W, dz, az);
+  }
+}
+
+// True when the target's own term in source_terms is W * 0 with W finite:
+// eps^2 a normal number and m * rsqrt(eps^2)^3, in the same operation order,
+// below overflow.
+__device__ __forceinline__ bool self_term_is_finite(float m, float eps2) {
+  if (!(eps2 >= 1.17549435e-38f)) return false;
+  const float r = rsqrt_mufu(eps2);
+  return isfinite(m * ((r * r) * r));
+}
+
+__device__ __forceinline__ void source_tile(const SourceTile& s, float4 p, float eps2, bool guard,
+                                            float& hx, float& hy, float& hz, float& lx,
+                                            float& ly, float& lz) {
+  unsigned long long ax = 0ull, ay = 0ull, az = 0ull;  // {0.f, 0.f}
+  if (guard) {
+    source_terms<true>(s, p, eps2, ax, ay, az);
+  } else {
+    source_terms<false>(s, p, eps2, ax, ay, az);
+  }
+  float a, b;
+  unpack2(ax, a, b);
+  fold(hx, lx, a);
+  fold(hx, lx, b);
+  unpack2(ay, a, b);
+  fold(hy, ly, a);
+  fold(hy, ly, b);
+  unpack2(az, a, b);
+  fold(hz, lz, a);
+  fold(hz, lz, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -1020,9 +1140,15 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   return x ^ (x >> 31);
 }
 
+// The corrected walk evaluates the network once per (cell, 32-target group) at
+// the group centre, for cells whose distance from that centre exceeds the
+// group radius / kCorrGroup.
+constexpr float kCorrGroup = 0.3f;
+
 // Training pairs: sample k picks a random target and, walking the tree with the
-// reference criterion at theta_train, one of the cells that target accepts,
-// uniformly (reservoir sampling).  Up to 8 targets are tried per sample.
+// reference criterion at theta_train, one of the cells that target accepts and
+// its group would correct, uniformly (reservoir sampling).  Up to 8 targets
+// are tried per sample.
 __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, float theta,
                                  unsigned long long seed, int samples, int* __restrict__ target,
                                  int* __restrict__ cell, int* status) {
@@ -1036,6 +1162,22 @@ __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, 
     state = mix64(state + 0x9E3779B97F4A7C15ull);
     tgt = (int)(state % (unsigned long long)n);
     const float4 p = pos[tgt];
+    // the target's walk group (32 Morton-consecutive particles): only cells
+    // the corrected walk would correct for this group are sampled
+    const int g0 = tgt & ~31, g1 = min(g0 + 32, n);
+    float bx0 = p.x, bx1 = p.x, by0 = p.y, by1 = p.y, bz0 = p.z, bz1 = p.z;
+    for (int j = g0; j < g1; ++j) {
+      const float4 q = pos[j];
+      bx0 = fminf(bx0, q.x);
+      bx1 = fmaxf(bx1, q.x);
+      by0 = fminf(by0, q.y);
+      by1 = fmaxf(by1, q.y);
+      bz0 = fminf(bz0, q.z);
+      bz1 = fmaxf(bz1, q.z);
+    }
+    const float gx = 0.5f * (bx0 + bx1), gy = 0.5f * (by0 + by1), gz = 0.5f * (bz0 + bz1);
+    const float ex = 0.5f * (bx1 - bx0), ey = 0.5f * (by1 - by0), ez = 0.5f * (bz1 - bz0);
+    const float rg2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     unsigned count = 0;
     int node = 0, steps = 0;
     while ((unsigned)node < (unsigned)total) {
@@ -1044,7 +1186,7 @@ __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, 
         break;
       }
       const int4 info = t.info[node];
-      if (info.z > 0 || info.x <= node) {
+      if (info.x <= node || info.z == 1) {  // single particles are always exact
         node = info.x > node ? info.x : total;
         continue;
       }
@@ -1053,12 +1195,15 @@ __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, 
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float s = t.side[node];
       if (d2 > 0.f && s * s < th2 * d2 && c.w > 0.f) {
-        ++count;
-        state = mix64(state + 0x9E3779B97F4A7C15ull);
-        if (state % count == 0) chosen = node;
+        const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
+        if (kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2) {
+          ++count;
+          state = mix64(state + 0x9E3779B97F4A7C15ull);
+          if (state % count == 0) chosen = node;
+        }
         node = info.x;
       } else {
-        node = node + 1;
+        node = info.z > 0 ? info.x : node + 1;  // a failing bucket is summed exactly
       }
     }
   }
@@ -1195,17 +1340,21 @@ __global__ void mlp_stats_kernel(const float* __restrict__ feat, const float* __
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> stackless walk
+constexpr int kListStackCorr = 1024;  // with the network's buffers: 42 KiB per block
 
 // Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
 // traversal.  Each step the lanes pop up to 32 nodes from the warp's
 // shared-memory stack and test them IN PARALLEL: a node is accepted when every
 // target's own reference test (2h)^2 < theta^2 d^2 holds (d to the cell's
 // centre of mass) — first tried in one shot against the group's bounding box
-// (if the box's nearest point passes, every target does), else target by
-// target from shared memory — so the accepted cells are exactly those of the
-// stackless walk.  Leaves and accepted cells are appended to two lists that
-// are evaluated, whenever 32 have gathered, in dense loops where every lane
-// computes its own target's terms.  A warp whose stack would overflow restarts
+// (if the box's nearest point passes, every target does), else for each such
+// node in turn by the 32 lanes testing their own targets at once — so the
+// accepted cells are exactly those of the stackless walk.  Buckets that must be summed exactly and accepted cells are
+// appended to two lists; whenever 32 have gathered, the buckets' particles and
+// (monopole walk) the cells' centres of mass are copied with parallel loads
+// into a 64-source shared tile that every lane evaluates on its own target
+// with paired f32x2 arithmetic.  Quadrupole and corrected cells are evaluated
+// from their own staged list.  A warp whose stack would overflow restarts
 // with the stackless walk.
 //
 // CORR: the learned far-field correction.  At every cell flush the gathered
@@ -1213,7 +1362,9 @@ constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> sta
 // through the MLP 16 cells at a time (one m16 tile per mma.sync); each target
 // then adds (M / |d|^2) * y to its monopole term, y the de-standardised network
 // output and d its own distance to the cell's centre of mass.  Cells whose
-// features fall outside the range seen in training keep the plain monopole.
+// features fall outside the range seen in training, or that lie closer than
+// 1/kCorrGroup group radii to the group centre (where one evaluation cannot
+// stand for all 32 targets), keep the plain monopole.
 template <int ORDER, int STACK, bool CORR>
 __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
     const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
@@ -1221,23 +1372,29 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
     const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ int s_cells[kListThreads / 32][kListCap];
-  __shared__ int s_leaves[kListThreads / 32][kListCap];
+  __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
   __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
   __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
   __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
-  __shared__ float4 s_tgt[kListThreads / 32][32];
+  // ORDER 1: accepted cells are point masses in the tile; EXTRA: the quadrupole
+  // or the network's correction is evaluated from a separate list of cells
+  constexpr bool EXTRA = ORDER == 2 || CORR;
+  __shared__ __align__(16) SourceTile s_src[kListThreads / 32];
+  __shared__ float4 s_cc[kListThreads / 32][EXTRA ? kListCap : 1];
+  __shared__ float4 s_cq[kListThreads / 32][ORDER == 2 ? 2 * kListCap : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  SourceTile& src = s_src[wib];
+  int staged = 0;  // sources waiting in src (warp-uniform)
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
   int* stack = s_stack[wib];
   int* cells = s_cells[wib];
-  int* leaves = s_leaves[wib];
+  int2* leaves = s_leaves[wib];
   const int s = warp * 32 + lane;
   const bool active = s < n;
   const float4 p = pos[active ? s : n - 1];
   const unsigned lt = (1u << lane) - 1u;
-  const int nact = min(32, n - warp * 32);  // targets of this warp
-  s_tgt[wib][lane] = p;
+  const bool guard = !__all_sync(kFull, !active || self_term_is_finite(p.w, eps2));
 
   // group bounding box
   float bx0 = p.x, bx1 = p.x, by0 = p.y, by1 = p.y, bz0 = p.z, bz1 = p.z;
@@ -1251,6 +1408,7 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
   }
   const float gx = 0.5f * (bx0 + bx1), gy = 0.5f * (by0 + by1), gz = 0.5f * (bz0 + bz1);
   const float ex = 0.5f * (bx1 - bx0), ey = 0.5f * (by1 - by0), ez = 0.5f * (bz1 - bz0);
+  const float rg2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));  // group radius^2
 
   const int total = (int)t.offset[n];
   float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
@@ -1269,46 +1427,58 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       int node = lane < take ? stack[top - 1 - lane] : -1;
       top -= take;
       __syncwarp();
-      bool is_leaf = false, accept = false;
+      bool is_leaf = false, accept = false, test = false;
       int kids = 0;
+      int4 info = make_int4(0, 0, 0, 0);
+      float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+      float ro = 0.f;
       int4 ca = make_int4(-1, -1, -1, -1), cb = make_int4(-1, -1, -1, -1);
       if (node >= total) {
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         node = -1;
       }
       if (node >= 0) {
-        const int4 info = t.info[node];
-        if (info.z > 0) {
+        info = t.info[node];
+        if (info.z > 0 && (info.y < 0 || info.y + info.z > n)) {
+          atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        } else if (info.z == 1) {  // a single particle is always exact
           is_leaf = true;
-        } else {
-          const float4 c = t.com[node];
+        } else {  // cells and buckets of >= 2 particles take the opening test
+          c = t.com[node];
+          ro = t.ropen2[node];
           const float qx = fmaxf(fabsf(c.x - gx) - ex, 0.f);
           const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
           const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
           const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
-          const float ro = t.ropen2[node];
           accept = dmin2 > ro;  // the whole box passes: every target passes
-          if (!accept) {        // otherwise each target's own test decides
-            accept = true;
-            for (int k = 0; k < nact; ++k) {
-              const float4 q = s_tgt[wib][k];
-              const float ex2 = c.x - q.x, ey2 = c.y - q.y, ez2 = c.z - q.z;
-              if (!(fmaf(ex2, ex2, fmaf(ey2, ey2, ez2 * ez2)) > ro)) {
-                accept = false;
-                break;
-              }
-            }
-          }
-          if (!accept) {
-            ca = reinterpret_cast<const int4*>(t.children)[2 * node];
-            cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
-            kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) +
-                   (cb.y >= 0) + (cb.z >= 0) + (cb.w >= 0);
-          }
+          test = !accept;
+        }
+      }
+      // Nodes the box could not accept: every target's own test decides, one
+      // node at a time with the 32 targets tested in parallel.
+      for (unsigned pend = __ballot_sync(kFull, test); pend != 0u; pend &= pend - 1u) {
+        const int from = __ffs(pend) - 1;
+        const float cx = __shfl_sync(kFull, c.x, from);
+        const float cy = __shfl_sync(kFull, c.y, from);
+        const float cz = __shfl_sync(kFull, c.z, from);
+        const float r = __shfl_sync(kFull, ro, from);
+        const float dx = cx - p.x, dy = cy - p.y, dz = cz - p.z;
+        const bool fail = active && !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > r);
+        const bool any = __any_sync(kFull, fail);
+        if (lane == from) accept = !any;
+      }
+      if (test && !accept) {
+        if (info.z > 0) {
+          is_leaf = true;  // a failing bucket is summed exactly
+        } else {
+          ca = reinterpret_cast<const int4*>(t.children)[2 * node];
+          cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
+          kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) +
+                 (cb.y >= 0) + (cb.z >= 0) + (cb.w >= 0);
         }
       }
       unsigned m = __ballot_sync(kFull, is_leaf);
-      if (is_leaf) leaves[nleaf + __popc(m & lt)] = node;
+      if (is_leaf) leaves[nleaf + __popc(m & lt)] = make_int2(info.y, info.z);
       nleaf += __popc(m);
       m = __ballot_sync(kFull, accept);
       if (accept) cells[ncell + __popc(m & lt)] = node;
@@ -1332,7 +1502,8 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       __syncwarp();
     }
     const bool drain = top == 0;
-    if (ncell >= 32 || (drain && ncell > 0)) {
+    const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
+    if (EXTRA && flush_cells) {
       float px = 0.f, py = 0.f, pz = 0.f;
       if (CORR) {
         uint32_t* xs = s_x[wib];
@@ -1344,7 +1515,12 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
           bool ok = false;
           if (r < ncell) {
             const int node = cells[r];
-            ok = cell_features(t, node, t.com[node], gx, gy, gz, f);
+            const float4 c = t.com[node];
+            ok = cell_features(t, node, c, gx, gy, gz, f);
+            // the group centre must stand for every target: group radius
+            // below kCorrGroup of the distance, else the plain monopole
+            const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
+            ok = ok && kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2;
 #pragma unroll
             for (int q = 0; q < nbsp_mlp::kIn; ++q)
               ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
@@ -1376,10 +1552,21 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
         }
         __syncwarp();
       }
+      // stage the cells' data with parallel loads, then one dense loop
+      float4* cc = s_cc[wib];
+      float4* cq = s_cq[wib];
+      for (int r = lane; r < ncell; r += 32) {
+        const int node = cells[r];
+        cc[r] = t.com[node];
+        if (ORDER == 2) {
+          cq[2 * r] = t.quad[2 * node];
+          cq[2 * r + 1] = t.quad[2 * node + 1];
+        }
+      }
+      __syncwarp();
       for (int e = 0; e < ncell; ++e) {
-        const int node = cells[e];
-        const float4 c = t.com[node];
-        cell_term<ORDER>(t, node, c, p, eps2, px, py, pz);
+        const float4 c = cc[e];
+        if (ORDER == 2) cell_term_q<2>(c, cq[2 * e], cq[2 * e + 1].x, p, eps2, px, py, pz);
         if (CORR && s_ok[wib][e]) {
           const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
           const float scale = c.w / fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -1389,47 +1576,72 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
           pz = fmaf(scale, fmaf(ye[2], net->y_std[2], net->y_mean[2]), pz);
         }
       }
-      if (CORR) __syncwarp();
+      __syncwarp();
       fold(hx, lx, px);
       fold(hy, ly, py);
       fold(hz, lz, pz);
+      if (ORDER == 2) {
+        approx += active ? (unsigned)ncell : 0u;
+        ncell = 0;
+      }
+    }
+    if (ORDER == 1 && flush_cells) {
+      // a monopole cell is a point mass at its centre of mass: it joins the tile
+      for (int r0 = 0; r0 < ncell;) {
+        const int take = min(ncell - r0, kStage - staged);
+        for (int k = lane; k < take; k += 32) stage_source(src, staged + k, t.com[cells[r0 + k]]);
+        staged += take;
+        r0 += take;
+        if (staged == kStage) {
+          __syncwarp();
+          source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
+          staged = 0;
+          __syncwarp();
+        }
+      }
       approx += active ? (unsigned)ncell : 0u;
       ncell = 0;
     }
     if (nleaf >= 32 || (drain && nleaf > 0)) {
+      // Copy the buckets' particles into the tile with parallel loads.  The
+      // target itself contributes exactly 0 (d = 0; eps = 0 is guarded there).
       int e = 0;
-      while (e < nleaf) {  // consecutive leaves often abut: merge their particle ranges
-        const int4 first = t.info[leaves[e++]];
-        const int b = first.y;
-        int end = first.y + first.z;
-        while (e < nleaf) {
-          const int4 nx = t.info[leaves[e]];
-          if (nx.y != end) break;
-          end = nx.y + nx.z;
+      while (e < nleaf) {  // consecutive buckets often abut: merge their particle ranges
+        const int2 first = leaves[e++];
+        const int b = first.x;
+        int end = first.x + first.y;
+        while (e < nleaf && leaves[e].x == end) {
+          end += leaves[e].y;
           ++e;
         }
-        float px = 0.f, py = 0.f, pz = 0.f;
-        for (int j = b; j < end; ++j) {
-          const float4 q = pos[j];
-          const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-          const float rinv = j == s ? 0.f : rsqrt_mufu(r2);  // barnes_hut.c:572
-          const float w = q.w * (rinv * rinv * rinv);
-          px = fmaf(w, dx, px);
-          py = fmaf(w, dy, py);
-          pz = fmaf(w, dz, pz);
-        }
-        fold(hx, lx, px);
-        fold(hy, ly, py);
-        fold(hz, lz, pz);
         exact += active ? (unsigned)(end - b - ((s >= b && s < end) ? 1 : 0)) : 0u;
+        for (int j0 = b; j0 < end;) {
+          const int take = min(end - j0, kStage - staged);
+          for (int k = lane; k < take; k += 32) stage_source(src, staged + k, pos[j0 + k]);
+          staged += take;
+          j0 += take;
+          if (staged == kStage) {
+            __syncwarp();
+            source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
+            staged = 0;
+            __syncwarp();
+          }
+        }
       }
       nleaf = 0;
+    }
+    if (drain && staged > 0) {  // the last, partial tile: pad with massless far sources
+      for (int k = staged + lane; k < kStage; k += 32)
+        stage_source(src, k, make_float4(kFarAway, kFarAway, kFarAway, 0.f));
+      __syncwarp();
+      source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
+      staged = 0;
     }
     __syncwarp();
   }
   WalkAcc a;
   if (overflow) {
+    if (lane == 0) atomicAdd(&counters[5], 1ull);  // groups walked again
     stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
   } else {
     a.hx = hx;
@@ -1556,7 +1768,7 @@ void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int m
     float4* hi = (float4*)acc_hi;
     float4* lo = (float4*)acc_lo;
     if (net != nullptr) {  // the network corrects the monopole term
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true><<<blocks, kListThreads, 0, stream>>>(
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStackCorr, true><<<blocks, kListThreads, 0, stream>>>(
           p, (int)n, t, eps2, hi, lo, counters, status, net);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(

@@ -57,9 +57,10 @@ NBSP_HIDDEN NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** bh,
                                                     NBodySimProCudaTimings* timings,
                                                     NBodySimProError* error);
 
-/* After a stream synchronisation: fill stats / timings of the last evaluation. */
+/* After a stream synchronisation: fill stats / timings of the last evaluation
+ * and the number of 32-target groups the interaction-list walk restarted. */
 NBSP_HIDDEN void nbsp_bh_collect(NbspBarnesHut* bh, NBodySimProBarnesHutStats* stats,
-                                 NBodySimProCudaTimings* timings);
+                                 NBodySimProCudaTimings* timings, size_t* walk_restarts);
 
 /* Keys + sort only; copies the sorted keys / permutation / root to the host (synchronises). */
 NBSP_HIDDEN NBodySimProStatus nbsp_bh_morton(NbspBarnesHut** bh, const NbspBarnesHutState* s,

@@ -180,7 +180,7 @@ static double elapsed(const NbspBarnesHut* b, int from, int to) {
 }
 
 void nbsp_bh_collect(NbspBarnesHut* b, NBodySimProBarnesHutStats* stats,
-                     NBodySimProCudaTimings* timings) {
+                     NBodySimProCudaTimings* timings, size_t* walk_restarts) {
     if (b == NULL || !b->timed) return;
     const unsigned long long* c = b->host_counters;
     stats->accepted_approximations = (size_t)c[0];
@@ -189,6 +189,7 @@ void nbsp_bh_collect(NbspBarnesHut* b, NBodySimProBarnesHutStats* stats,
     stats->leaf_count = (size_t)c[3];
     stats->internal_node_count = (size_t)(c[2] - c[3]);
     stats->maximum_depth = (size_t)c[4];
+    *walk_restarts = (size_t)c[5];
     timings->bounds_ms = elapsed(b, 0, 1);
     timings->keys_ms = elapsed(b, 1, 2);
     timings->sort_ms = elapsed(b, 2, 3);
