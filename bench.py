@@ -9,7 +9,16 @@ dt = 1e-3 — one step = one kick-drift-force-kick of all N particles.
 Metric: particle-steps/s (N x steps / device time).
 
 Other workloads (parity configs, selectable): ``allpairs_plummer_16k``,
-``allpairs_precision_262k``.
+``allpairs_precision_262k``, ``ensemble_4096`` and ``bh_matched_10m`` (the
+same collision at N = 10M).
+
+`matched_accuracy` (Barnes-Hut workloads, skipped with --no-matched): on the
+initial state, the rms relative force error against the FP64 direct sum on
+4096 seeded targets is measured over a theta grid for the plain monopole walk
+and for the chosen quadrupole walk; each is then timed at the largest theta
+whose error is at most 1e-3.  ``bh_matched_10m`` adds the plain walk at
+theta 0.5 and the learned correction at theta 1.0 (network trained on 2^22
+cell-target pairs of the 1M collision).
 
 Timing: W untimed warm-up steps; then K steps, each a 1-step device-resident
 advance bracketed by CUDA events recorded by the library on its own stream;
@@ -52,7 +61,15 @@ WORKLOADS = {
                                     ic="uniform_log_mass", steps=3),
     "ensemble_4096": dict(n=None, algorithm="ensemble", systems=4096, lo=32, hi=4096, eps=0.01,
                           dt=1e-3, ic="ensemble", steps=1000),
+    "bh_matched_10m": dict(n=10_000_000, algorithm="barnes_hut", theta=0.5, eps=0.01, dt=1e-3,
+                           ic="collision", steps=3, order=1, matched=True, correction=True),
 }
+
+# Matched-accuracy study: the largest opening angle of this grid whose rms
+# relative force error (FP64 direct sum on 4096 seeded targets, initial state)
+# stays at or below RMS_TARGET, per method.
+RMS_TARGET = 1e-3
+THETA_GRID = (0.4, 0.45, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.8, 0.9, 1.0)
 
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
 FLOPS_PAIR = 20          # standard convention per softened pair interaction
@@ -354,11 +371,101 @@ def run_ours(args, wl, world, rank, local):
         e2e = run_e2e(nb, wl, pos, vel, mass, min(args.steps, 5), algo, ctx)
 
     ctx.close()
+    matched = None
+    if wl["algorithm"] == "barnes_hut" and not args.no_matched:
+        matched = matched_study(nb, torch, wl, system, g, min(args.steps, 5), 3, flush,
+                                with_correction=wl.get("correction", False))
     value = world * n * args.steps / (total_ms * 1e-3)
     return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
                 roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
                 interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
-                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms))
+                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms),
+                matched=matched)
+
+
+def rms_at_targets(nb, ctx, g, n, targets, ref):
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    sys_ = nb.ParticleSystem.zeros(n)
+    ctx.download(sys_)
+    acc = sys_.acc()[targets]
+    return float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
+
+
+def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None):
+    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order)."""
+    ctx = nb.CudaContext(theta=theta, multipole_order=order)
+    ctx.set_correction(correction)
+    ctx.upload(system)
+    for _ in range(warmup):
+        ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
+    ms = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
+        ms.append(ctx.timings()["total_ms"])
+    ctx.close()
+    return wl["n"] * steps / (sum(ms) * 1e-3), float(np.mean(ms))
+
+
+def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
+    """Plain (monopole) vs chosen (quadrupole) Barnes-Hut, each at the largest
+    theta of THETA_GRID meeting RMS_TARGET, both timed; optionally the learned
+    correction at theta 1.0 (trained on 2^22 pairs of the 1M collision) and the
+    plain walk at theta 0.5."""
+    n = wl["n"]
+    targets = np.random.default_rng(11).choice(n, min(4096, n), replace=False)
+    ctx = nb.CudaContext(theta=0.5)
+    ctx.upload(system)
+    ref = ctx.reference_acceleration(g, targets)
+    table = {}
+    for order in (1, 2):
+        ctx.set_multipole_order(order)
+        rows = []
+        for th in THETA_GRID:
+            ctx.theta = th
+            rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
+        table[order] = rows
+    ctx.close()
+    out = {"rms_target": RMS_TARGET, "oracle": "FP64 device direct sum, 4096 seeded targets, "
+           "initial state", "sweep": {f"order{o}": [[t, round(r, 6)] for t, r in rows]
+                                     for o, rows in table.items()}}
+    for name, order in (("plain", 1), ("chosen", 2)):
+        ok = [t for t, r in table[order] if r <= RMS_TARGET]
+        if not ok:
+            out[name] = None
+            continue
+        th = max(ok)
+        v, ms = timed_steps(nb, torch, system, g, wl, th, order, steps, warmup, flush)
+        out[name] = {"theta": th, "multipole_order": order,
+                     "rms": dict(table[order])[th], "value": v, "ms_per_step": round(ms, 4)}
+    if out["plain"] and out["chosen"]:
+        out["chosen_over_plain"] = round(out["chosen"]["value"] / out["plain"]["value"], 3)
+    if with_correction:
+        v, ms = timed_steps(nb, torch, system, g, wl, 0.5, 1, steps, warmup, flush)
+        out["plain_theta_0.5"] = {"theta": 0.5, "rms": dict(table[1])[0.5], "value": v,
+                                  "ms_per_step": round(ms, 4)}
+        pos1, vel1, mass1 = initial_conditions("collision", 1_000_000, seed=42)
+        with nb.CudaContext(theta=1.0) as c1, nb.CudaCorrection(seed=11) as corr:
+            c1.upload(nb.ParticleSystem.from_arrays(pos1, vel1, mass1))
+            t0 = time.time()
+            corr.generate(c1, g, theta=1.0, samples=1 << 22, seed=3)
+            tl, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
+            train_s = time.time() - t0
+            cctx = nb.CudaContext(theta=1.0)
+            cctx.set_correction(corr)
+            cctx.upload(system)
+            rms_c = rms_at_targets(nb, cctx, g, n, targets, ref)
+            cctx.close()
+            v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush,
+                                correction=corr)
+        out["corrected_theta_1.0"] = {"theta": 1.0, "rms": rms_c, "value": v,
+                                      "ms_per_step": round(ms, 4),
+                                      "plain_rms_at_theta_1.0": dict(table[1])[1.0],
+                                      "training": {"pairs": 1 << 22, "from": "collision N=1M",
+                                                   "epochs": 8, "final_validation_loss":
+                                                   float(vl[-1]), "seconds": round(train_s, 2)}}
+    return out
 
 
 def ensemble_ic(wl, seed=42):
@@ -482,6 +589,8 @@ def main(argv=None):
     ap.add_argument("--workload", default="bh_collision_1m", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-matched", action="store_true",
+                    help="skip the matched-accuracy study of the Barnes-Hut workloads")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--order", type=int, default=None, choices=[1, 2])
     ap.add_argument("--walk", default=None, choices=["lists", "stackless"])
@@ -558,6 +667,8 @@ def main(argv=None):
                 "interactions_per_s": r["interactions_per_s"], "stats": r["stats"],
                 "phase_ms": r["timings"], "roofline": r["roofline"], "cpu_baseline": cpu,
                 "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"]}
+        if r.get("matched") is not None:
+            line["matched_accuracy"] = r["matched"]
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -961,36 +961,6 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
   store_walk(a, s, active, lane, acc_hi, acc_lo, counters);
 }
 
-// Accepted-cell term (monopole, optionally + trace-free quadrupole), d = com - target:
-// a = G [ M d / r^3 - Q d / r^5 + 5/2 (d.Q.d) d / r^7 ],  r^2 = d^2 + eps^2.
-// c = (com, mass); qa = (Qxx, Qxy, Qxz, Qyy), qyz = Qyz (Qzz = -Qxx - Qyy).
-template <int ORDER>
-__device__ __forceinline__ void cell_term_q(float4 c, float4 qa, float qyz, float4 p, float eps2,
-                                            float& px, float& py, float& pz) {
-  const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-  const float rinv = rsqrt_mufu(r2);
-  const float rinv2 = rinv * rinv;
-  const float rinv3 = rinv * rinv2;
-  float w = c.w * rinv3;
-  if (ORDER == 2) {
-    const float qzz = -qa.x - qa.w;
-    const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
-    const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qyz * dz));
-    const float qdz = fmaf(qa.z, dx, fmaf(qyz, dy, qzz * dz));
-    const float dqd = fmaf(dx, qdx, fmaf(dy, qdy, dz * qdz));
-    const float rinv5 = rinv3 * rinv2;
-    const float rinv7 = rinv5 * rinv2;
-    w = fmaf(2.5f * dqd, rinv7, w);
-    px = fmaf(-qdx, rinv5, px);
-    py = fmaf(-qdy, rinv5, py);
-    pz = fmaf(-qdz, rinv5, pz);
-  }
-  px = fmaf(w, dx, px);
-  py = fmaf(w, dy, py);
-  pz = fmaf(w, dz, pz);
-}
-
 // Point sources (bucket particles and monopole cells) gathered per warp in
 // shared memory, interleaved by pairs so that one 16-byte load yields the
 // 64-bit operands {x_2i, x_2i+1} and {y_2i, y_2i+1} (resp. z and m) of the
@@ -1066,6 +1036,86 @@ __device__ __forceinline__ void source_terms(const SourceTile& s, float4 p, floa
     ay = fma2(W, dy, ay);
     az = fma2(W, dz, az);
   }
+}
+
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
+// Accepted cells of the quadrupole walk, pair-interleaved like SourceTile:
+// centre of mass, mass and the five independent trace-free components.
+struct QuadTile {
+  ulonglong2 xy[kStage / 2];         // {x}, {y}
+  ulonglong2 zm[kStage / 2];         // {z}, {m}
+  ulonglong2 qa[kStage / 2];         // {Qxx}, {Qxy}
+  ulonglong2 qb[kStage / 2];         // {Qxz}, {Qyy}
+  unsigned long long qc[kStage / 2];  // {Qyz}
+};
+
+// c = (com, mass); qa = (Qxx, Qxy, Qxz, Qyy); qyz = Qyz.
+__device__ __forceinline__ void stage_cell(QuadTile& s, int k, float4 c, float4 qa, float qyz) {
+  const int i = k >> 1, o = k & 1;
+  float* a = reinterpret_cast<float*>(&s.xy[i]) + o;
+  float* b = reinterpret_cast<float*>(&s.zm[i]) + o;
+  float* e = reinterpret_cast<float*>(&s.qa[i]) + o;
+  float* f = reinterpret_cast<float*>(&s.qb[i]) + o;
+  a[0] = c.x;
+  a[2] = c.y;
+  b[0] = c.z;
+  b[2] = c.w;
+  e[0] = qa.x;
+  e[2] = qa.y;
+  f[0] = qa.z;
+  f[2] = qa.w;
+  reinterpret_cast<float*>(&s.qc[i])[o] = qyz;
+}
+
+// The kStage cell terms of a full QuadTile on this lane's target, two cells per
+// instruction: a = G [ M d / r^3 - Q d / r^5 + 5/2 (d.Q.d) d / r^7 ],
+// d = com - target, r^2 = d^2 + eps^2, Qzz = -Qxx - Qyy.  Padding cells
+// (far away, massless, Q = 0) add exactly 0.
+__device__ __forceinline__ void quad_tile(const QuadTile& s, float4 p, float eps2, float& hx,
+                                          float& hy, float& hz, float& lx, float& ly, float& lz) {
+  const unsigned long long PX = pack2(p.x, p.x), PY = pack2(p.y, p.y), PZ = pack2(p.z, p.z);
+  const unsigned long long E2 = pack2(eps2, eps2), H = pack2(2.5f, 2.5f);
+  const unsigned long long ZERO = 0ull;
+  unsigned long long ax = 0ull, ay = 0ull, az = 0ull;
+#pragma unroll 8
+  for (int j = 0; j < kStage / 2; ++j) {
+    const ulonglong2 a = s.xy[j], b = s.zm[j], qa = s.qa[j], qb = s.qb[j];
+    const unsigned long long qyz = s.qc[j];
+    const unsigned long long dx = sub2(a.x, PX), dy = sub2(a.y, PY), dz = sub2(b.x, PZ);
+    const unsigned long long r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+    float r2a, r2b;
+    unpack2(r2, r2a, r2b);
+    const unsigned long long R = pack2(rsqrt_mufu(r2a), rsqrt_mufu(r2b));
+    const unsigned long long R2 = mul2(R, R);
+    const unsigned long long R3 = mul2(R2, R);
+    const unsigned long long R5 = mul2(R3, R2);
+    const unsigned long long R7 = mul2(R5, R2);
+    const unsigned long long qdx = fma2(qa.x, dx, fma2(qa.y, dy, mul2(qb.x, dz)));
+    const unsigned long long qdy = fma2(qa.y, dx, fma2(qb.y, dy, mul2(qyz, dz)));
+    const unsigned long long qdz =
+        sub2(fma2(qb.x, dx, mul2(qyz, dy)), mul2(add2(qa.x, qb.y), dz));
+    const unsigned long long dqd = fma2(dx, qdx, fma2(dy, qdy, mul2(dz, qdz)));
+    const unsigned long long w = fma2(mul2(H, dqd), R7, mul2(b.y, R3));
+    const unsigned long long nr5 = sub2(ZERO, R5);
+    ax = fma2(qdx, nr5, fma2(w, dx, ax));
+    ay = fma2(qdy, nr5, fma2(w, dy, ay));
+    az = fma2(qdz, nr5, fma2(w, dz, az));
+  }
+  float u, v;
+  unpack2(ax, u, v);
+  fold(hx, lx, u);
+  fold(hx, lx, v);
+  unpack2(ay, u, v);
+  fold(hy, ly, u);
+  fold(hy, ly, v);
+  unpack2(az, u, v);
+  fold(hz, lz, u);
+  fold(hz, lz, v);
 }
 
 // True when the target's own term in source_terms is W * 0 with W finite:
@@ -1376,15 +1426,16 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
   __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
   __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
   __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
-  // ORDER 1: accepted cells are point masses in the tile; EXTRA: the quadrupole
-  // or the network's correction is evaluated from a separate list of cells
-  constexpr bool EXTRA = ORDER == 2 || CORR;
+  // ORDER 1: accepted cells are point masses in the source tile (CORR: their
+  // corrections come from a separate list); ORDER 2: cells fill a QuadTile
+  static_assert(!(CORR && ORDER == 2), "the network corrects the monopole");
   __shared__ __align__(16) SourceTile s_src[kListThreads / 32];
-  __shared__ float4 s_cc[kListThreads / 32][EXTRA ? kListCap : 1];
-  __shared__ float4 s_cq[kListThreads / 32][ORDER == 2 ? 2 * kListCap : 1];
+  __shared__ __align__(16) QuadTile s_quad[ORDER == 2 ? kListThreads / 32 : 1];
+  __shared__ float4 s_cc[kListThreads / 32][CORR ? kListCap : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   SourceTile& src = s_src[wib];
-  int staged = 0;  // sources waiting in src (warp-uniform)
+  int staged = 0;   // sources waiting in src (warp-uniform)
+  int qstaged = 0;  // cells waiting in the QuadTile (ORDER 2)
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
   int* stack = s_stack[wib];
@@ -1503,7 +1554,7 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
     }
     const bool drain = top == 0;
     const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
-    if (EXTRA && flush_cells) {
+    if (CORR && flush_cells) {
       float px = 0.f, py = 0.f, pz = 0.f;
       if (CORR) {
         uint32_t* xs = s_x[wib];
@@ -1554,20 +1605,11 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       }
       // stage the cells' data with parallel loads, then one dense loop
       float4* cc = s_cc[wib];
-      float4* cq = s_cq[wib];
-      for (int r = lane; r < ncell; r += 32) {
-        const int node = cells[r];
-        cc[r] = t.com[node];
-        if (ORDER == 2) {
-          cq[2 * r] = t.quad[2 * node];
-          cq[2 * r + 1] = t.quad[2 * node + 1];
-        }
-      }
+      for (int r = lane; r < ncell; r += 32) cc[r] = t.com[cells[r]];
       __syncwarp();
       for (int e = 0; e < ncell; ++e) {
         const float4 c = cc[e];
-        if (ORDER == 2) cell_term_q<2>(c, cq[2 * e], cq[2 * e + 1].x, p, eps2, px, py, pz);
-        if (CORR && s_ok[wib][e]) {
+        if (s_ok[wib][e]) {
           const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
           const float scale = c.w / fmaf(dx, dx, fmaf(dy, dy, dz * dz));
           const float* ye = &s_y[wib][e * 4];
@@ -1580,10 +1622,26 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       fold(hx, lx, px);
       fold(hy, ly, py);
       fold(hz, lz, pz);
-      if (ORDER == 2) {
-        approx += active ? (unsigned)ncell : 0u;
-        ncell = 0;
+    }
+    if (ORDER == 2 && flush_cells) {
+      QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
+      for (int r0 = 0; r0 < ncell;) {
+        const int take = min(ncell - r0, kStage - qstaged);
+        for (int k = lane; k < take; k += 32) {
+          const int node = cells[r0 + k];
+          stage_cell(qt, qstaged + k, t.com[node], t.quad[2 * node], t.quad[2 * node + 1].x);
+        }
+        qstaged += take;
+        r0 += take;
+        if (qstaged == kStage) {
+          __syncwarp();
+          quad_tile(qt, p, eps2, hx, hy, hz, lx, ly, lz);
+          qstaged = 0;
+          __syncwarp();
+        }
       }
+      approx += active ? (unsigned)ncell : 0u;
+      ncell = 0;
     }
     if (ORDER == 1 && flush_cells) {
       // a monopole cell is a point mass at its centre of mass: it joins the tile
@@ -1636,6 +1694,15 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       __syncwarp();
       source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
       staged = 0;
+    }
+    if (ORDER == 2 && drain && qstaged > 0) {  // the same for the last cells
+      QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
+      for (int k = qstaged + lane; k < kStage; k += 32)
+        stage_cell(qt, k, make_float4(kFarAway, kFarAway, kFarAway, 0.f),
+                   make_float4(0.f, 0.f, 0.f, 0.f), 0.f);
+      __syncwarp();
+      quad_tile(qt, p, eps2, hx, hy, hz, lx, ly, lz);
+      qstaged = 0;
     }
     __syncwarp();
   }
