@@ -1389,8 +1389,7 @@ __global__ void mlp_stats_kernel(const float* __restrict__ feat, const float* __
 
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
-constexpr int kListStack = 1536;   // node ids per warp (6 KiB); overflow -> stackless walk
-constexpr int kListStackCorr = 1024;  // with the network's buffers: 42 KiB per block
+constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
 
 // Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
 // traversal.  Each step the lanes pop up to 32 nodes from the warp's
@@ -1415,13 +1414,16 @@ constexpr int kListStackCorr = 1024;  // with the network's buffers: 42 KiB per 
 // features fall outside the range seen in training, or that lie closer than
 // 1/kCorrGroup group radii to the group centre (where one evaluation cannot
 // stand for all 32 targets), keep the plain monopole.
+// Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
+// walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
 template <int ORDER, int STACK, bool CORR>
-__global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
     float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ int s_cells[kListThreads / 32][kListCap];
+  __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
   __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
   __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
@@ -1490,13 +1492,13 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
       }
       if (node >= 0) {
         info = t.info[node];
+        c = t.com[node];
+        ro = t.ropen2[node];
         if (info.z > 0 && (info.y < 0 || info.y + info.z > n)) {
           atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         } else if (info.z == 1) {  // a single particle is always exact
           is_leaf = true;
         } else {  // cells and buckets of >= 2 particles take the opening test
-          c = t.com[node];
-          ro = t.ropen2[node];
           const float qx = fmaxf(fabsf(c.x - gx) - ex, 0.f);
           const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
           const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
@@ -1505,20 +1507,25 @@ __global__ void __launch_bounds__(kListThreads) walk_lists_kernel(
           test = !accept;
         }
       }
-      // Nodes the box could not accept: every target's own test decides, one
-      // node at a time with the 32 targets tested in parallel.
+      // Nodes the box could not accept: a node that fails this lane's own
+      // target is opened at once; for the rest every target's own test
+      // decides, one node at a time with the 32 targets tested in parallel.
+      const bool opened = test && active && !(fmaf(c.x - p.x, c.x - p.x,
+                                                   fmaf(c.y - p.y, c.y - p.y,
+                                                        (c.z - p.z) * (c.z - p.z))) > ro);
+      test = test && !opened;
+      float4* probe = s_probe[wib];
+      if (test) probe[lane] = make_float4(c.x, c.y, c.z, ro);
+      __syncwarp();
       for (unsigned pend = __ballot_sync(kFull, test); pend != 0u; pend &= pend - 1u) {
         const int from = __ffs(pend) - 1;
-        const float cx = __shfl_sync(kFull, c.x, from);
-        const float cy = __shfl_sync(kFull, c.y, from);
-        const float cz = __shfl_sync(kFull, c.z, from);
-        const float r = __shfl_sync(kFull, ro, from);
-        const float dx = cx - p.x, dy = cy - p.y, dz = cz - p.z;
-        const bool fail = active && !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > r);
+        const float4 q = probe[from];
+        const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        const bool fail = active && !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > q.w);
         const bool any = __any_sync(kFull, fail);
         if (lane == from) accept = !any;
       }
-      if (test && !accept) {
+      if ((test || opened) && !accept) {
         if (info.z > 0) {
           is_leaf = true;  // a failing bucket is summed exactly
         } else {
@@ -1835,7 +1842,7 @@ void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int m
     float4* hi = (float4*)acc_hi;
     float4* lo = (float4*)acc_lo;
     if (net != nullptr) {  // the network corrects the monopole term
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStackCorr, true><<<blocks, kListThreads, 0, stream>>>(
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true><<<blocks, kListThreads, 0, stream>>>(
           p, (int)n, t, eps2, hi, lo, counters, status, net);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
