@@ -302,7 +302,7 @@ def run_ours(args, wl, world, rank, local):
         ctx.advance(g, wl["dt"], 1, algo)
     barrier_sync(world)
     launches0 = nb.kernel_launches()
-    step_ms, walk_ms, stats_acc = [], [], []
+    step_ms, walk_ms, stats_acc, phases = [], [], [], []
     torch.cuda.nvtx.range_push("timed_steps")  # profilers can select the timed launches
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
@@ -312,6 +312,7 @@ def run_ours(args, wl, world, rank, local):
             t = ctx.timings()
             step_ms.append(t["total_ms"])
             walk_ms.append(t["walk_ms"])
+            phases.append(t)
             st = ctx.stats()
             st["walk_restarts"] = ctx.walk_restarts()
             stats_acc.append(st)
@@ -381,7 +382,7 @@ def run_ours(args, wl, world, rank, local):
     return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
                 roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
                 interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
-                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms),
+                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms, phases),
                 matched=matched)
 
 
@@ -542,9 +543,13 @@ def run_ensemble(args, wl, world, rank, local):
                 timings={"advance_ms": round(ms, 3)})
 
 
-def ctx_timings_summary(step_ms, walk_ms):
-    return {"step_ms_mean": round(float(np.mean(step_ms)), 4),
-            "walk_ms_mean": round(float(np.mean(walk_ms)), 4)}
+def ctx_timings_summary(step_ms, walk_ms, phases=()):
+    out = {"step_ms_mean": round(float(np.mean(step_ms)), 4),
+           "walk_ms_mean": round(float(np.mean(walk_ms)), 4)}
+    for key in ("bounds_ms", "keys_ms", "sort_ms", "build_ms", "moments_ms", "integrate_ms"):
+        if phases:
+            out[key.replace("_ms", "_ms_mean")] = round(float(np.mean([p[key] for p in phases])), 4)
+    return out
 
 
 def run_e2e(nb, wl, pos, vel, mass, steps, algo, ctx):

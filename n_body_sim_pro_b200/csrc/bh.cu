@@ -140,21 +140,17 @@ __device__ __forceinline__ uint64_t spread3(uint64_t v) {
   return v;
 }
 
-__global__ void keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
-                            const double* __restrict__ z, size_t n,
-                            const double* __restrict__ geometry, uint64_t* __restrict__ keys,
-                            uint32_t* __restrict__ index) {
-  const double cx = geometry[0], cy = geometry[1], cz = geometry[2], h = geometry[3];
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    keys[i] = spread3(axis_code(x[i], cx, h)) | (spread3(axis_code(y[i], cy, h)) << 1) |
-              (spread3(axis_code(z[i], cz, h)) << 2);
-    index[i] = (uint32_t)i;
-  }
-}
-
 // ---------------------------------------------------------------------------
-// stable LSD radix sort, 8-bit digits
+// stable LSD radix sort, 8-bit digits, one kernel per pass
+//
+// The keys kernel also counts the 8 digit histograms (one read of the keys);
+// one block turns them into each pass's digit bases.  Every pass is then a
+// single kernel: tiles take tickets in launch order, rank their keys in shared
+// memory, and find their global offsets with a decoupled look-back over the
+// preceding tiles' published digit counts (flag A: this tile's count, flag P:
+// inclusive prefix).  A tile only waits on tiles with earlier tickets, which
+// are already resident; every wait is bounded and flags an error when it
+// runs out.
 // ---------------------------------------------------------------------------
 
 constexpr int kSortThreads = 256;
@@ -162,71 +158,120 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
 constexpr int kRadix = 256;
+constexpr int kSortPasses = 8;
+constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kCountMask = (1u << 30) - 1u;
+constexpr int kLookbackSpins = 1 << 22;  // ~ms per predecessor before the error flag
+constexpr int kKeysBlocks = 2 * 148;
 
-__global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(
-    const uint64_t* __restrict__ keys, size_t n, int shift, uint32_t* __restrict__ hist) {
-  __shared__ uint32_t h[kRadix];
-  h[threadIdx.x] = 0;
-  __syncthreads();
-  const size_t base = (size_t)blockIdx.x * kSortTile;
-  for (int k = threadIdx.x; k < kSortTile; k += kSortThreads) {
-    const size_t i = base + k;
-    if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & 0xffu], 1u);
-  }
-  __syncthreads();
-  hist[(size_t)blockIdx.x * kRadix + threadIdx.x] = h[threadIdx.x];
+// Sort scratch (32-bit words): hist[8][256] | base[8][256] | ticket[8] | status[8][tiles][256]
+struct SortScratch {
+  uint32_t* hist;
+  uint32_t* base;
+  uint32_t* ticket;
+  uint32_t* status;
+};
+__host__ __device__ inline size_t sort_tiles(size_t n) { return (n + kSortTile - 1) / kSortTile; }
+inline SortScratch sort_scratch(uint32_t* w, size_t n) {
+  SortScratch s;
+  s.hist = w;
+  s.base = w + kSortPasses * kRadix;
+  s.ticket = s.base + kSortPasses * kRadix;
+  s.status = s.ticket + kSortPasses;
+  (void)n;
+  return s;
+}
+inline size_t sort_scratch_words(size_t n) {
+  return 2 * kSortPasses * kRadix + kSortPasses + kSortPasses * sort_tiles(n) * kRadix;
 }
 
-// One block: per digit, exclusive prefix over tiles (in place); digit bases into
-// hist[tiles * 256 + d].
-__global__ void __launch_bounds__(kRadix) sort_scan_kernel(uint32_t* __restrict__ hist,
-                                                           int tiles) {
-  __shared__ uint32_t tot[kRadix];
+__global__ void __launch_bounds__(256) keys_kernel(
+    const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+    size_t n, const double* __restrict__ geometry, uint64_t* __restrict__ keys,
+    uint32_t* __restrict__ index, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[kSortPasses][kRadix];
+  for (int k = threadIdx.x; k < kSortPasses * kRadix; k += blockDim.x) (&h[0][0])[k] = 0;
+  __syncthreads();
+  const double cx = geometry[0], cy = geometry[1], cz = geometry[2], hs = geometry[3];
+  const unsigned lane = threadIdx.x & 31;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t first = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  // every lane runs the same number of iterations (match_any needs the whole warp)
+  const size_t rounds = (n + stride - 1) / stride;
+  for (size_t r = 0; r < rounds; ++r) {
+    const size_t i = first + r * stride;
+    const bool valid = i < n;
+    uint64_t key = 0;
+    if (valid) {
+      key = spread3(axis_code(x[i], cx, hs)) | (spread3(axis_code(y[i], cy, hs)) << 1) |
+            (spread3(axis_code(z[i], cz, hs)) << 2);
+      keys[i] = key;
+      index[i] = (uint32_t)i;
+    }
+#pragma unroll
+    for (int p = 0; p < kSortPasses; ++p) {  // warp-aggregated digit counts
+      const unsigned d = valid ? (unsigned)(key >> (8 * p)) & 0xffu : 0x100u;
+      const unsigned peers = __match_any_sync(kFull, d);
+      if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kSortPasses * kRadix; k += blockDim.x) {
+    const uint32_t v = (&h[0][0])[k];
+    if (v != 0) atomicAdd(&hist[k], v);
+  }
+}
+
+// One block of 256 threads: base[p][d] = number of keys whose digit p is < d.
+__global__ void __launch_bounds__(kRadix) sort_bases_kernel(const uint32_t* __restrict__ hist,
+                                                            uint32_t* __restrict__ base) {
+  __shared__ uint32_t sh[kRadix];
   const int d = threadIdx.x;
-  uint32_t run = 0;
-  for (int t = 0; t < tiles; ++t) {
-    const uint32_t c = hist[(size_t)t * kRadix + d];
-    hist[(size_t)t * kRadix + d] = run;
-    run += c;
-  }
-  tot[d] = run;
-  __syncthreads();
-  // exclusive scan of the 256 digit totals (Hillis-Steele on a copy)
-  uint32_t v = run;
-  for (int off = 1; off < kRadix; off <<= 1) {
+  for (int p = 0; p < kSortPasses; ++p) {
+    const uint32_t own = hist[p * kRadix + d];
+    uint32_t v = own;
+    sh[d] = v;
+    for (int off = 1; off < kRadix; off <<= 1) {
+      __syncthreads();
+      const uint32_t add = d >= off ? sh[d - off] : 0u;
+      __syncthreads();
+      v += add;
+      sh[d] = v;
+    }
+    base[p * kRadix + d] = v - own;
     __syncthreads();
-    const uint32_t add = d >= off ? tot[d - off] : 0u;
-    __syncthreads();
-    v += add;
-    tot[d] = v;
   }
-  hist[(size_t)tiles * kRadix + d] = v - run;
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
+__device__ __forceinline__ uint32_t load_volatile(const uint32_t* p) {
+  return *reinterpret_cast<const volatile uint32_t*>(p);
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(
     const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int shift,
-    const uint32_t* __restrict__ hist, int tiles, int* status) {
+    const uint32_t* __restrict__ base, uint32_t* ticket, uint32_t* status, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint64_t* sk = reinterpret_cast<uint64_t*>(smem);                     // kSortTile
   uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);           // kSortTile
   uint32_t* wc = sv + kSortTile;                                        // kSortWarps * 256
   uint32_t* start = wc + kSortWarps * kRadix;                           // 256
   uint32_t* gofs = start + kRadix;                                      // 256
+  __shared__ int s_tile;
 
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  if (t == 0) s_tile = (int)atomicAdd(ticket, 1u);
   for (int k = t; k < kSortWarps * kRadix; k += kSortThreads) wc[k] = 0;
-  gofs[t] = hist[(size_t)tiles * kRadix + t] + hist[(size_t)blockIdx.x * kRadix + t];
   __syncthreads();
+  const int tile = s_tile;
 
-  const size_t base = (size_t)blockIdx.x * kSortTile + (size_t)w * (kSortItems * 32);
+  const size_t base_i = (size_t)tile * kSortTile + (size_t)w * (kSortItems * 32);
   const unsigned lt = (1u << lane) - 1u;
   uint64_t key[kSortItems];
   uint32_t val[kSortItems];
   uint32_t rank[kSortItems];
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
-    const size_t i = base + (size_t)it * 32 + lane;
+    const size_t i = base_i + (size_t)it * 32 + lane;
     const bool valid = i < n;
     key[it] = valid ? keys_in[i] : 0ull;
     val[it] = valid ? vals_in[i] : 0u;
@@ -240,7 +285,8 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
     rank[it] = before + __popc(peers & lt);
   }
   __syncthreads();
-  {  // per digit: exclusive over warps; tile totals
+  uint32_t count;  // this tile's keys with digit t
+  {
     uint32_t run = 0;
     for (int ww = 0; ww < kSortWarps; ++ww) {
       const uint32_t c = wc[ww * kRadix + t];
@@ -248,9 +294,34 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
       run += c;
     }
     start[t] = run;
+    count = run;
   }
+  // publish, then look back for the keys with digit t in all earlier tiles
+  uint32_t* st = status + (size_t)tile * kRadix + t;
+  atomicExch(st, (tile == 0 ? kFlagP : kFlagA) | count);
+  uint32_t prefix = 0;
+  if (tile > 0) {
+    int j = tile - 1;
+    int spins = 0;
+    while (j >= 0) {
+      const uint32_t v = load_volatile(status + (size_t)j * kRadix + t);
+      const uint32_t flag = v & ~kCountMask;
+      if (flag == 0u) {
+        if (++spins > kLookbackSpins) {
+          atomicOr(err, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+          break;
+        }
+        continue;
+      }
+      prefix += v & kCountMask;
+      if (flag == kFlagP) break;
+      --j;
+    }
+    atomicExch(st, kFlagP | ((prefix + count) & kCountMask));
+  }
+  gofs[t] = base[t] + prefix;
   __syncthreads();
-  {  // exclusive scan of tile digit totals
+  {  // exclusive scan of the tile's digit totals
     const uint32_t own = start[t];
     uint32_t v = own;
     for (int off = 1; off < kRadix; off <<= 1) {
@@ -266,7 +337,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
   __syncthreads();
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
-    const size_t i = base + (size_t)it * 32 + lane;
+    const size_t i = base_i + (size_t)it * 32 + lane;
     if (i < n) {
       const unsigned digit = (unsigned)(key[it] >> shift) & 0xffu;
       const uint32_t pos = start[digit] + wc[w * kRadix + digit] + rank[it];
@@ -274,25 +345,29 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
         sk[pos] = key[it];
         sv[pos] = val[it];
       } else {
-        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        atomicOr(err, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
       }
     }
   }
   __syncthreads();
-  const size_t tile_base = (size_t)blockIdx.x * kSortTile;
-  const int count = (int)(n - tile_base < (size_t)kSortTile ? n - tile_base : (size_t)kSortTile);
-  for (int p = t; p < count; p += kSortThreads) {
-    const uint64_t k = sk[p];
+  const size_t tile_base = (size_t)tile * kSortTile;
+  const int count_all = (int)(n - tile_base < (size_t)kSortTile ? n - tile_base : (size_t)kSortTile);
+  for (int q = t; q < count_all; q += kSortThreads) {
+    const uint64_t k = sk[q];
     const unsigned digit = (unsigned)(k >> shift) & 0xffu;
-    const size_t dst = (size_t)gofs[digit] + (size_t)(p - (int)start[digit]);
+    const size_t dst = (size_t)gofs[digit] + (size_t)(q - (int)start[digit]);
     if (dst < n) {
       keys_out[dst] = k;
-      vals_out[dst] = sv[p];
+      vals_out[dst] = sv[q];
     } else {
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      atomicOr(err, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
     }
   }
 }
+
+constexpr size_t kDownsweepSmem =
+    (size_t)kSortTile * (sizeof(uint64_t) + sizeof(uint32_t)) +
+    (size_t)(kSortWarps * kRadix + 2 * kRadix) * sizeof(uint32_t);
 
 // The reference's insertion build fails with OVERFLOW when two particles share
 // a position (barnes_hut.c:149-153: more than 128 subdivisions).  Equal
@@ -320,9 +395,6 @@ __global__ void duplicates_kernel(const uint64_t* __restrict__ keys,
     }
   }
 }
-
-constexpr size_t kDownsweepSmem =
-    kSortTile * 8 + kSortTile * 4 + kSortWarps * kRadix * 4 + 2 * kRadix * 4;
 
 // ---------------------------------------------------------------------------
 // gather / scatter
@@ -1757,26 +1829,35 @@ void nbsp_bh_bounds(const double* x, const double* y, const double* z, const dou
   NBSP_COUNT_LAUNCH(1), bounds_final_kernel<<<1, kBoundsThreads, 0, stream>>>(partial, (int)blocks, geometry);
 }
 
+size_t nbsp_bh_sort_scratch_words(size_t n) { return sort_scratch_words(n); }
+
 void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
-                  const double* geometry, uint64_t* keys, uint32_t* index, cudaStream_t stream) {
-  NBSP_COUNT_LAUNCH(1), keys_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, y, z, n, geometry, keys, index);
+                  const double* geometry, uint64_t* keys, uint32_t* index, uint32_t* scratch,
+                  cudaStream_t stream) {
+  cudaMemsetAsync(scratch, 0, sort_scratch_words(n) * sizeof(uint32_t), stream);
+  const SortScratch sc = sort_scratch(scratch, n);
+  size_t blocks = (n + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (blocks > (size_t)kKeysBlocks) blocks = kKeysBlocks;
+  NBSP_COUNT_LAUNCH(1), keys_kernel<<<(unsigned)blocks, 256, 0, stream>>>(x, y, z, n, geometry, keys,
+                                                                          index, sc.hist);
 }
 
 void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt, uint32_t* index_alt,
-                  size_t n, uint32_t* hist, int* status, cudaStream_t stream) {
-  cudaFuncSetAttribute(sort_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                  size_t n, uint32_t* scratch, int* status, cudaStream_t stream) {
+  cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDownsweepSmem);
-  const int tiles = (int)((n + kSortTile - 1) / kSortTile);
+  const SortScratch sc = sort_scratch(scratch, n);
+  const size_t tiles = sort_tiles(n);
+  NBSP_COUNT_LAUNCH(1), sort_bases_kernel<<<1, kRadix, 0, stream>>>(sc.hist, sc.base);
   uint64_t* kin = keys;
   uint32_t* vin = index;
   uint64_t* kout = keys_alt;
   uint32_t* vout = index_alt;
-  for (int pass = 0; pass < 8; ++pass) {
-    const int shift = 8 * pass;
-    NBSP_COUNT_LAUNCH(1), sort_upsweep_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, hist);
-    NBSP_COUNT_LAUNCH(1), sort_scan_kernel<<<1, kRadix, 0, stream>>>(hist, tiles);
-    NBSP_COUNT_LAUNCH(1), sort_downsweep_kernel<<<tiles, kSortThreads, kDownsweepSmem, stream>>>(
-        kin, vin, kout, vout, n, shift, hist, tiles, status);
+  for (int pass = 0; pass < kSortPasses; ++pass) {
+    NBSP_COUNT_LAUNCH(1), sort_pass_kernel<<<(unsigned)tiles, kSortThreads, kDownsweepSmem, stream>>>(
+        kin, vin, kout, vout, n, 8 * pass, sc.base + pass * kRadix, sc.ticket + pass,
+        sc.status + (size_t)pass * tiles * kRadix, status);
     uint64_t* tk = kin;
     kin = kout;
     kout = tk;
@@ -1784,7 +1865,7 @@ void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt, uint32_t*
     vin = vout;
     vout = tv;
   }
-  // 8 passes (even): the result is back in (keys, index)
+  // kSortPasses = 8 (even): the result is back in (keys, index)
 }
 
 void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double* x,

@@ -80,13 +80,18 @@ NBSP_HIDDEN void nbsp_bh_bounds(const double* x, const double* y, const double* 
 
 NBSP_HIDDEN void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
                               const double* geometry, uint64_t* keys, uint32_t* index,
-                              cudaStream_t stream);
+                              uint32_t* sort_scratch, cudaStream_t stream);
 
-/* Stable LSD radix sort of (keys, index) by all 64 key bits.  `keys`/`index`
- * are ping-ponged with `keys_alt`/`index_alt`; the sorted result ends in the
- * first pair.  `hist` >= 256 * ceil(n / 4096) + 256 words. */
+/* 32-bit words of sort scratch for n keys (digit histograms, pass bases, tile
+ * tickets and look-back status words). */
+NBSP_HIDDEN size_t nbsp_bh_sort_scratch_words(size_t n);
+
+/* Stable LSD radix sort of (keys, index) by all 64 key bits, after nbsp_bh_keys
+ * filled `sort_scratch` (nbsp_bh_sort_scratch_words(n) words) on the same stream.
+ * `keys`/`index` are ping-ponged with `keys_alt`/`index_alt`; the sorted result
+ * ends in the first pair. */
 NBSP_HIDDEN void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt,
-                              uint32_t* index_alt, size_t n, uint32_t* hist, int* status,
+                              uint32_t* index_alt, size_t n, uint32_t* sort_scratch, int* status,
                               cudaStream_t stream);
 
 /* Flag NBSP_DEVICE_ERROR_DUPLICATE_POSITION when two particles share a position. */

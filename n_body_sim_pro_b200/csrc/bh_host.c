@@ -98,14 +98,13 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
     if (n <= b->capacity) return N_BODY_SIM_PRO_STATUS_OK;
     release_buffers(b);
     const size_t cap = n < 1024 ? 1024 : n;
-    const size_t tiles = (cap + 4095) / 4096;
     BH_TRY(cudaMalloc((void**)&b->partial, 1024 * 10 * sizeof(double)));
     BH_TRY(cudaMalloc((void**)&b->geometry, 8 * sizeof(double)));
     BH_TRY(cudaMalloc((void**)&b->keys, cap * sizeof(uint64_t)));
     BH_TRY(cudaMalloc((void**)&b->keys_alt, cap * sizeof(uint64_t)));
     BH_TRY(cudaMalloc((void**)&b->index, cap * sizeof(uint32_t)));
     BH_TRY(cudaMalloc((void**)&b->index_alt, cap * sizeof(uint32_t)));
-    BH_TRY(cudaMalloc((void**)&b->hist, (256 * tiles + 256) * sizeof(uint32_t)));
+    BH_TRY(cudaMalloc((void**)&b->hist, nbsp_bh_sort_scratch_words(cap) * sizeof(uint32_t)));
     BH_TRY(cudaMalloc(&b->pos4, cap * 16));
     BH_TRY(cudaMalloc(&b->tree, nbsp_bh_tree_bytes(cap)));
     BH_TRY(cudaMalloc(&b->acc_hi, cap * 16));
@@ -118,7 +117,7 @@ static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, i
                                 cudaStream_t stream) {
     nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status, stream);
     cudaEventRecord(b->events[1], stream);
-    nbsp_bh_keys(s->x, s->y, s->z, s->n, b->geometry, b->keys, b->index, stream);
+    nbsp_bh_keys(s->x, s->y, s->z, s->n, b->geometry, b->keys, b->index, b->hist, stream);
     cudaEventRecord(b->events[2], stream);
     nbsp_bh_sort(b->keys, b->index, b->keys_alt, b->index_alt, s->n, b->hist, status, stream);
     cudaEventRecord(b->events[3], stream);
