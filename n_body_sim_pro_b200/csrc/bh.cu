@@ -24,6 +24,7 @@
 #include "mlp.cuh"
 
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <stdint.h>
 
 namespace {
@@ -722,7 +723,13 @@ __global__ void place_kernel(Tree t, int leaf_capacity, int* status) {
       atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
       return;
     }
-    atomicAdd(&t.nchild[parent_node], 1);
+    // children in arrival order; the moments pass sorts them into depth-first order
+    const int slot = atomicAdd(&t.nchild[parent_node], 1);
+    if (slot < 8) {
+      t.children[8 * parent_node + slot] = node;
+    } else {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    }
   }
   t.info[node] = make_int4(next, begin, leaf ? count : 0, parent_node);
   t.level[node] = lvl;
@@ -761,109 +768,156 @@ __device__ __forceinline__ double4 ldcg_d4(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+__device__ __forceinline__ void swap_if_greater(int& a, int& b) {
+  const int lo = min(a, b), hi = max(a, b);
+  a = lo;
+  b = hi;
+}
+
 // Bottom-up moments: leaves sum their particles, the last child to finish
-// combines its parent (children read in depth-first order: deterministic).
-__global__ void moments_kernel(const float4* __restrict__ pos, Tree t,
-                               const double* __restrict__ geometry, double inv_theta2,
-                               int* status) {
+// combines its parent.  place_kernel recorded the children in arrival order;
+// the combine sorts them into depth-first (= octant) order, so the sums run in
+// a fixed order and the result is deterministic, loads all of them at once and
+// writes the sorted list back for the interaction-list walk.
+__global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
+                                                      const double* __restrict__ geometry,
+                                                      double inv_theta2, int* status) {
   const int total = (int)t.offset[t.n];
-  const int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= total) return;
-  const int4 info = t.info[node];
-  if (info.z == 0) return;  // internal nodes are finished by their last child
-  if (info.z < 0 || info.y < 0 || info.y + info.z > t.n) {
-    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-    return;
-  }
   const double root_size = 2.0 * geometry[3];
-  Moments mo;
-  {
-    double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int j = info.y; j < info.y + info.z; ++j) {
-      const float4 p = pos[j];
-      m += (double)p.w;
-      sx += (double)p.w * (double)p.x;
-      sy += (double)p.w * (double)p.y;
-      sz += (double)p.w * (double)p.z;
-    }
-    mo.m = m;
-    mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
-    mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
-    mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
-    for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
-    mo.t2 = 0.0;
-    for (int j = info.y; j < info.y + info.z; ++j) {
-      const float4 p = pos[j];
-      const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const double w = (double)p.w;
-      mo.t2 += w * r2;
-      mo.q[0] += w * (3.0 * dx * dx - r2);
-      mo.q[1] += w * (3.0 * dx * dy);
-      mo.q[2] += w * (3.0 * dx * dz);
-      mo.q[3] += w * (3.0 * dy * dy - r2);
-      mo.q[4] += w * (3.0 * dy * dz);
-      mo.q[5] += w * (3.0 * dz * dz - r2);
-    }
-  }
-  finish_node(t, node, mo, root_size, inv_theta2, t.level[node]);
-  int h = 1;
-  int parent = info.w;
-  for (int climb = 0; parent >= 0; ++climb) {
-    if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < total;
+       node += gridDim.x * blockDim.x) {
+    const int4 info = t.info[node];
+    if (info.z == 0) continue;  // internal nodes are finished by their last child
+    if (info.z < 0 || info.y < 0 || info.y + info.z > t.n) {
       atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-      return;
+      continue;
     }
-    __threadfence();
-    const int arrived = atomicAdd(&t.arrive[parent], 1);
-    if (arrived != __ldcg(&t.nchild[parent]) - 1) return;
-    __threadfence();
-    // combine children of `parent` (first child = parent + 1, then skip links)
-    const int4 pinfo = __ldcg(&t.info[parent]);
-    double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-    int hmax = 0;
-    int c = parent + 1, guard = 0;
-    while (c != pinfo.x) {
-      if (++guard > 8 || c < 0 || c >= total) {
-        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-        return;
+    Moments mo;
+    {
+      double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
+      for (int j = info.y; j < info.y + info.z; ++j) {
+        const float4 p = pos[j];
+        m += (double)p.w;
+        sx += (double)p.w * (double)p.x;
+        sy += (double)p.w * (double)p.y;
+        sz += (double)p.w * (double)p.z;
       }
-      t.children[8 * parent + guard - 1] = c;
-      const double4 cm = ldcg_d4(&t.mom[c]);
-      m += cm.x;
-      sx += cm.x * cm.y;
-      sy += cm.x * cm.z;
-      sz += cm.x * cm.w;
-      hmax = max(hmax, __ldcg(&t.height[c]));
-      c = __ldcg(&t.info[c]).x;
+      mo.m = m;
+      mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
+      mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
+      mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
+      for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
+      mo.t2 = 0.0;
+#pragma unroll 4
+      for (int j = info.y; j < info.y + info.z; ++j) {
+        const float4 p = pos[j];
+        const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double w = (double)p.w;
+        mo.t2 += w * r2;
+        mo.q[0] += w * (3.0 * dx * dx - r2);
+        mo.q[1] += w * (3.0 * dx * dy);
+        mo.q[2] += w * (3.0 * dx * dz);
+        mo.q[3] += w * (3.0 * dy * dy - r2);
+        mo.q[4] += w * (3.0 * dy * dz);
+        mo.q[5] += w * (3.0 * dz * dz - r2);
+      }
     }
-    for (int k = guard; k < 8; ++k) t.children[8 * parent + k] = -1;
-    Moments pm;
-    pm.m = m;
-    pm.cx = m != 0.0 ? sx / m : 0.0;
-    pm.cy = m != 0.0 ? sy / m : 0.0;
-    pm.cz = m != 0.0 ? sz / m : 0.0;
-    for (int k = 0; k < 6; ++k) pm.q[k] = 0.0;
-    pm.t2 = 0.0;
-    c = parent + 1;
-    while (c != pinfo.x) {
-      const double4 cm = ldcg_d4(&t.mom[c]);
-      const double dx = cm.y - pm.cx, dy = cm.z - pm.cy, dz = cm.w - pm.cz;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const double w = cm.x;
-      pm.t2 += __ldcg(&t.trace64[c]) + w * r2;
-      pm.q[0] += __ldcg(&t.quad64[6 * c + 0]) + w * (3.0 * dx * dx - r2);
-      pm.q[1] += __ldcg(&t.quad64[6 * c + 1]) + w * (3.0 * dx * dy);
-      pm.q[2] += __ldcg(&t.quad64[6 * c + 2]) + w * (3.0 * dx * dz);
-      pm.q[3] += __ldcg(&t.quad64[6 * c + 3]) + w * (3.0 * dy * dy - r2);
-      pm.q[4] += __ldcg(&t.quad64[6 * c + 4]) + w * (3.0 * dy * dz);
-      pm.q[5] += __ldcg(&t.quad64[6 * c + 5]) + w * (3.0 * dz * dz - r2);
-      c = __ldcg(&t.info[c]).x;
+    finish_node(t, node, mo, root_size, inv_theta2, t.level[node]);
+    int parent = info.w;
+    for (int climb = 0; parent >= 0; ++climb) {
+      if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        break;
+      }
+      __threadfence();
+      const int nc = __ldcg(&t.nchild[parent]);
+      const int arrived = atomicAdd(&t.arrive[parent], 1);
+      if (arrived != nc - 1) break;
+      __threadfence();
+      if (nc < 1 || nc > 8) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        break;
+      }
+      const int4 pinfo = __ldcg(&t.info[parent]);
+      const int4 ca = __ldcg(reinterpret_cast<const int4*>(t.children) + 2 * parent);
+      const int4 cb = __ldcg(reinterpret_cast<const int4*>(t.children) + 2 * parent + 1);
+      int ch[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k >= nc) ch[k] = INT_MAX;
+      // sorting network for 8 keys (19 compare-exchanges)
+      swap_if_greater(ch[0], ch[2]); swap_if_greater(ch[1], ch[3]);
+      swap_if_greater(ch[4], ch[6]); swap_if_greater(ch[5], ch[7]);
+      swap_if_greater(ch[0], ch[4]); swap_if_greater(ch[1], ch[5]);
+      swap_if_greater(ch[2], ch[6]); swap_if_greater(ch[3], ch[7]);
+      swap_if_greater(ch[0], ch[1]); swap_if_greater(ch[2], ch[3]);
+      swap_if_greater(ch[4], ch[5]); swap_if_greater(ch[6], ch[7]);
+      swap_if_greater(ch[2], ch[4]); swap_if_greater(ch[3], ch[5]);
+      swap_if_greater(ch[1], ch[4]); swap_if_greater(ch[3], ch[6]);
+      swap_if_greater(ch[1], ch[2]); swap_if_greater(ch[3], ch[4]);
+      swap_if_greater(ch[5], ch[6]);
+      bool bad = false;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) bad |= k < nc && (ch[k] <= parent || ch[k] >= total);
+      if (bad) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        break;
+      }
+      double4 cm[8];
+      int hmax = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        cm[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (k < nc) {
+          cm[k] = ldcg_d4(&t.mom[ch[k]]);
+          hmax = max(hmax, __ldcg(&t.height[ch[k]]));
+        }
+      }
+      double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k < nc) {
+          m += cm[k].x;
+          sx += cm[k].x * cm[k].y;
+          sy += cm[k].x * cm[k].z;
+          sz += cm[k].x * cm[k].w;
+        }
+      }
+      Moments pm;
+      pm.m = m;
+      pm.cx = m != 0.0 ? sx / m : 0.0;
+      pm.cy = m != 0.0 ? sy / m : 0.0;
+      pm.cz = m != 0.0 ? sz / m : 0.0;
+      for (int k = 0; k < 6; ++k) pm.q[k] = 0.0;
+      pm.t2 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k < nc) {
+          const int c = ch[k];
+          const double dx = cm[k].y - pm.cx, dy = cm[k].z - pm.cy, dz = cm[k].w - pm.cz;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const double w = cm[k].x;
+          pm.t2 += __ldcg(&t.trace64[c]) + w * r2;
+          pm.q[0] += __ldcg(&t.quad64[6 * c + 0]) + w * (3.0 * dx * dx - r2);
+          pm.q[1] += __ldcg(&t.quad64[6 * c + 1]) + w * (3.0 * dx * dy);
+          pm.q[2] += __ldcg(&t.quad64[6 * c + 2]) + w * (3.0 * dx * dz);
+          pm.q[3] += __ldcg(&t.quad64[6 * c + 3]) + w * (3.0 * dy * dy - r2);
+          pm.q[4] += __ldcg(&t.quad64[6 * c + 4]) + w * (3.0 * dy * dz);
+          pm.q[5] += __ldcg(&t.quad64[6 * c + 5]) + w * (3.0 * dz * dz - r2);
+        }
+      }
+      // the sorted children, -1 after the last (the walk pushes the first `kids`)
+      reinterpret_cast<int4*>(t.children)[2 * parent] =
+          make_int4(ch[0], nc > 1 ? ch[1] : -1, nc > 2 ? ch[2] : -1, nc > 3 ? ch[3] : -1);
+      reinterpret_cast<int4*>(t.children)[2 * parent + 1] =
+          make_int4(nc > 4 ? ch[4] : -1, nc > 5 ? ch[5] : -1, nc > 6 ? ch[6] : -1,
+                    nc > 7 ? ch[7] : -1);
+      t.height[parent] = hmax + 1;
+      finish_node(t, parent, pm, root_size, inv_theta2, __ldcg(&t.level[parent]));
+      parent = pinfo.w;
     }
-    h = hmax + 1;
-    t.height[parent] = h;
-    finish_node(t, parent, pm, root_size, inv_theta2, __ldcg(&t.level[parent]));
-    parent = pinfo.w;
   }
 }
 
@@ -1908,7 +1962,9 @@ void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry, double 
   Tree t = tree_view(tree, n);
   const size_t nb = 2 * n - 1;
   const double inv_theta2 = theta > 0.0 ? 1.0 / (theta * theta) : INFINITY;
-  NBSP_COUNT_LAUNCH(1), moments_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>((const float4*)pos4, t,
+  size_t blocks = (nb + 255) / 256;  // grid-stride over the octree nodes (<= 2n - 1)
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  NBSP_COUNT_LAUNCH(1), moments_kernel<<<(unsigned)blocks, 256, 0, stream>>>((const float4*)pos4, t,
                                                                    geometry, inv_theta2, status);
 }
 
