@@ -71,6 +71,15 @@ WORKLOADS = {
 RMS_TARGET = 1e-3
 THETA_GRID = (0.4, 0.45, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.8, 0.9, 1.0)
 
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu
+# capture of exactly this configuration (the file under profiles/ gives the command).
+PROFILED_TRAFFIC = {
+    ("bh_collision_1m", 0.7, 1, "lists", 16): (
+        29_660_928, "profiles/walk_lists_kernel_bh_collision_1m.md"),
+    ("allpairs_plummer_16k", None, 1, "lists", 16): (
+        273_152, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
+}
+
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
 FLOPS_PAIR = 20          # standard convention per softened pair interaction
 FLOPS_QUAD = 58          # monopole + trace-free quadrupole per accepted cell
@@ -367,6 +376,31 @@ def run_ours(args, wl, world, rank, local):
                              f"(sm_max_mhz of {peak_kind} MEASURED_PEAKS.json)",
                 "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4),
                 "traffic": None}
+    measured = PROFILED_TRAFFIC.get((args.workload, wl.get("theta"), wl.get("order", 1),
+                                     wl.get("walk", "lists"), wl.get("leaf", 16)))
+    if measured is not None:
+        roofline["traffic"] = measured[0]
+        roofline["traffic_source"] = measured[1]
+    stages = None
+    if wl["algorithm"] == "barnes_hut" and phases:
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        nodes = float(stats_acc[-1]["node_count"])
+        stages = {}
+        for name, key, nbytes in (
+                ("bounds", "bounds_ms", 32.0 * n),
+                ("keys", "keys_ms", 36.0 * n),
+                ("sort", "sort_ms", 8 * 24.0 * n),
+                ("moments", "moments_ms", 32.0 * n + 120.0 * nodes),
+                ("integrate", "integrate_ms", 36.0 * n + 24.0 * n + 120.0 * n)):
+            ms = float(np.mean([ph[key] for ph in phases]))
+            gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+            stages[name] = {"ms": round(ms, 4), "algorithmic_bytes": nbytes,
+                            "gbs": round(gbs, 1) if gbs else None,
+                            "frac_of_hbm": round(gbs / hbm, 4) if gbs else None}
+        stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes: "
+                           "bounds 32/particle, keys 24+12, sort 8 passes x (12+12), moments "
+                           "2 x 16 per particle + 120 per node, integrate scatter 36 + kick-drift "
+                           "24 + 120 per particle")
 
     # e2e through the plugin call on pinned host arrays
     e2e = None
@@ -383,7 +417,7 @@ def run_ours(args, wl, world, rank, local):
                 roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
                 interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
                 stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms, phases),
-                matched=matched)
+                matched=matched, stages=stages)
 
 
 def rms_at_targets(nb, ctx, g, n, targets, ref):
@@ -678,6 +712,8 @@ def main(argv=None):
                 "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"]}
         if r.get("matched") is not None:
             line["matched_accuracy"] = r["matched"]
+        if r.get("stages") is not None:
+            line["stages_hbm"] = r["stages"]
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -139,6 +139,45 @@ typedef struct NBodySimProDiagnosticsQuantities {
 } NBodySimProDiagnosticsQuantities;
 #endif
 
+#ifndef N_BODY_SIM_PRO_GENERATION_PRESETS_H
+/* include/n_body_sim_pro/generation/presets.h:27-46 */
+typedef enum NBodySimProSimulationPreset {
+    N_BODY_SIM_PRO_PRESET_TWO_BODY,
+    N_BODY_SIM_PRO_PRESET_RANDOM_CLOUD,
+    N_BODY_SIM_PRO_PRESET_SOLAR_SYSTEM,
+    N_BODY_SIM_PRO_PRESET_OPEN_CLUSTER,
+    N_BODY_SIM_PRO_PRESET_GLOBULAR_CLUSTER,
+    N_BODY_SIM_PRO_PRESET_SPIRAL_GALAXY,
+    N_BODY_SIM_PRO_PRESET_ELLIPTICAL_GALAXY,
+    N_BODY_SIM_PRO_PRESET_GALAXY_COLLISION,
+    N_BODY_SIM_PRO_PRESET_TRIPLE_GALAXY,
+    N_BODY_SIM_PRO_PRESET_COUNT
+} NBodySimProSimulationPreset;
+
+typedef struct NBodySimProPresetParameters {
+    size_t particle_count;
+    uint64_t random_seed;
+} NBodySimProPresetParameters;
+#endif
+
+#ifndef N_BODY_SIM_PRO_CHECKPOINT_CHECKPOINT_H
+/* include/n_body_sim_pro/checkpoint/checkpoint.h:27-41 */
+enum { N_BODY_SIM_PRO_CHECKPOINT_MAGIC = 0x53504348, N_BODY_SIM_PRO_CHECKPOINT_VERSION = 1 };
+
+typedef struct NBodySimProCheckpointHeader {
+    uint32_t magic;
+    uint32_t version;
+    size_t particle_count;
+    double simulation_time;
+    double timestep;
+    int32_t integrator;
+    double theta;
+    int32_t barnes_hut_enabled;
+    uint64_t random_seed;
+    int32_t preset;
+} NBodySimProCheckpointHeader;
+#endif
+
 /* ---- context ----------------------------------------------------------------- */
 
 /*
@@ -249,6 +288,51 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_barnes_hut_compute_acce
     NBodySimProError* error);
 
 /* ---- device-resident stepping ---------------------------------------------------- */
+
+/*
+ * Replaces n_body_sim_pro_preset_generate_parallel (generation/presets.h:73,
+ * src/c/generation/presets_parallel.c) for device-resident systems: generates
+ * the preset directly into the context's device state (no host arrays, no
+ * upload), one thread per particle with the reference's per-particle
+ * generators (xoshiro256** seeded from mix_seed(seed, index)), then removes
+ * each block's mean velocity as the reference does.  Integer random streams
+ * are identical to the reference's; the FP64 transcendental functions (log,
+ * cos, sin, pow, cbrt) are CUDA's, so values agree to a few ulp.  Particles
+ * the reference leaves unfilled (the last n % 2 of galaxy_collision, n % 3 of
+ * triple_galaxy) are zero apart from the collision's approach velocity;
+ * accelerations are zero.  Same argument errors as the reference (two_body
+ * needs exactly 2 particles).
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_preset_generate_parallel(
+    NBodySimProCudaContext* context, NBodySimProSimulationPreset preset,
+    const NBodySimProPresetParameters* parameters, NBodySimProError* error);
+
+/*
+ * Replaces n_body_sim_pro_checkpoint_write (checkpoint/checkpoint.h:43-46,
+ * src/c/checkpoint/checkpoint.c:9-76) for device-resident state: the file is
+ * the reference's format — magic, version, the header struct as stored in
+ * memory, then x, y, z, vx, vy, vz, ax, ay, az, m as FP64 arrays — written
+ * straight from the device through two pinned staging buffers, so the
+ * device-to-host copy of one chunk overlaps the file write of the previous
+ * one.  For the same state and header the bytes equal the reference's file.
+ * Errors as the reference: NULL arguments or a header count different from the
+ * resident count -> INVALID_ARGUMENT, file failures -> IO_ERROR; no resident
+ * state -> INVALID_STATE.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_checkpoint_write(
+    NBodySimProCudaContext* context, const char* path, const NBodySimProCheckpointHeader* header,
+    NBodySimProError* error);
+
+/*
+ * Replaces n_body_sim_pro_checkpoint_read (checkpoint.h:51-54, checkpoint.c:131-206):
+ * the file's state becomes the context's resident state (chunks read into
+ * pinned buffers and copied to the device while the next chunk is read) and
+ * `header` receives the stored header.  Bad magic or version -> INVALID_STATE,
+ * short or unreadable files -> IO_ERROR.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_checkpoint_read(
+    NBodySimProCudaContext* context, const char* path, NBodySimProCheckpointHeader* header,
+    NBodySimProError* error);
 
 /* Copy positions, velocities, masses and accelerations of `view` to the device. */
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_upload(

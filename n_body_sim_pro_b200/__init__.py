@@ -133,6 +133,23 @@ class EnsembleInfo(C.Structure):
         return d
 
 
+class CheckpointHeader(C.Structure):
+    """NBodySimProCheckpointHeader (checkpoint/checkpoint.h:29-40), C layout with padding."""
+
+    _fields_ = [("magic", C.c_uint32), ("version", C.c_uint32), ("particle_count", C.c_size_t),
+                ("simulation_time", C.c_double), ("timestep", C.c_double),
+                ("integrator", C.c_int32), ("theta", C.c_double),
+                ("barnes_hut_enabled", C.c_int32), ("random_seed", C.c_uint64),
+                ("preset", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+CHECKPOINT_MAGIC = 0x53504348
+CHECKPOINT_VERSION = 1
+
+
 class CudaError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{Status(status).name}: {message}")
@@ -151,7 +168,14 @@ EXPORTS = (
     "n_body_sim_pro_cuda_reference_acceleration", "n_body_sim_pro_cuda_morton_order",
     "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
     "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
+    "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
+    "n_body_sim_pro_cuda_checkpoint_read",
 )
+
+# NBodySimProSimulationPreset (generation/presets.h:27-38)
+PRESETS = {"two_body": 0, "random_cloud": 1, "solar_system": 2, "open_cluster": 3,
+           "globular_cluster": 4, "spiral_galaxy": 5, "elliptical_galaxy": 6,
+           "galaxy_collision": 7, "triple_galaxy": 8}
 
 
 def kernel_launches() -> int:
@@ -192,6 +216,12 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
+        "n_body_sim_pro_cuda_preset_generate_parallel": (C.c_int, [vp, C.c_int,
+                                                                   C.POINTER(C.c_size_t * 2), pe]),
+        "n_body_sim_pro_cuda_checkpoint_write": (C.c_int, [vp, C.c_char_p,
+                                                           C.POINTER(CheckpointHeader), pe]),
+        "n_body_sim_pro_cuda_checkpoint_read": (C.c_int, [vp, C.c_char_p,
+                                                          C.POINTER(CheckpointHeader), pe]),
         "n_body_sim_pro_gravity_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
         "n_body_sim_pro_barnes_hut_compute_acceleration_cuda": (st, [pv, pg, vp, pe]),
         "n_body_sim_pro_cuda_upload": (st, [vp, pv, pe]),
@@ -409,6 +439,31 @@ class CudaContext:
         t = Timings()
         library().n_body_sim_pro_cuda_context_timings(self.handle, C.byref(t))
         return t.as_dict()
+
+    def generate_preset(self, preset: "str | int", n: int, seed: int) -> None:
+        """presets_parallel.c on the device: the preset becomes the resident state."""
+        pid = PRESETS[preset] if isinstance(preset, str) else int(preset)
+        params = (C.c_size_t * 2)(n, seed)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_preset_generate_parallel(self.handle, pid,
+                                                                       C.byref(params),
+                                                                       C.byref(err)), err)
+        self.n = n
+
+    def checkpoint_write(self, path: str, header: CheckpointHeader) -> None:
+        """The resident state to `path` in the reference's checkpoint format."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_checkpoint_write(
+            self.handle, os.fsencode(path), C.byref(header), C.byref(err)), err)
+
+    def checkpoint_read(self, path: str) -> CheckpointHeader:
+        """A checkpoint file becomes the resident state; returns its header."""
+        header = CheckpointHeader()
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_checkpoint_read(
+            self.handle, os.fsencode(path), C.byref(header), C.byref(err)), err)
+        self.n = header.particle_count
+        return header
 
     def walk_restarts(self) -> int:
         """Groups of the last Barnes-Hut evaluation that the interaction-list

@@ -28,6 +28,9 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                      "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
+# presets.cu follows the reference's FP64 generation formulas, which are
+# compiled without FMA: no contraction there.
+FILE_FLAGS = {"presets.cu": ["--fmad=false"]}
 CC_FLAGS = ["-O2", "-std=c17", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wextra",
             "-Wno-unused-parameter", "-I" + CSRC, "-I" + INCLUDE]
 
@@ -76,7 +79,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, src, deps):
-            _run([nvcc, "-ccbin", _cc()] + NVCC_FLAGS + ["-c", src, "-o", obj], verbose)
+            extra = FILE_FLAGS.get(os.path.basename(src), [])
+            _run([nvcc, "-ccbin", _cc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj], verbose)
     for src in sorted(glob.glob(os.path.join(CSRC, "*.c"))):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)

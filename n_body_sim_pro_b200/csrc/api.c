@@ -602,6 +602,42 @@ NBodySimProStatus n_body_sim_pro_cuda_upload(NBodySimProCudaContext* c,
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
+NBodySimProStatus n_body_sim_pro_cuda_preset_generate_parallel(
+    NBodySimProCudaContext* c, NBodySimProSimulationPreset preset,
+    const NBodySimProPresetParameters* parameters, NBodySimProError* error) {
+    /* presets_parallel.c:314-326 argument checks */
+    if (c == NULL || parameters == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "particle system and parameters must not be null");
+    const size_t n = parameters->particle_count;
+    if ((int)preset < 0 || (int)preset >= (int)N_BODY_SIM_PRO_PRESET_COUNT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown preset");
+    if (preset == N_BODY_SIM_PRO_PRESET_TWO_BODY && n != 2) /* :343-347 */
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "two_body preset requires exactly 2 particles");
+    if (n == 0 || (preset == N_BODY_SIM_PRO_PRESET_GALAXY_COLLISION && n < 2) ||
+        (preset == N_BODY_SIM_PRO_PRESET_TRIPLE_GALAXY && n < 3))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "too few particles for the preset");
+    CUDA_TRY(cudaSetDevice(c->device));
+    NBodySimProStatus st = ensure_capacity(c, n, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if ((st = ensure_scratch(c, nbsp_preset_scratch_doubles(n), error)) != N_BODY_SIM_PRO_STATUS_OK)
+        return st;
+    c->n = n;
+    c->n_padded = round_up(n, 256);
+    /* unfilled tails (collision, triple) and accelerations start at zero */
+    double* arrays[] = {c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, c->m};
+    for (size_t k = 0; k < sizeof(arrays) / sizeof(arrays[0]); ++k)
+        CUDA_TRY(cudaMemsetAsync(arrays[k], 0, n * sizeof(double), c->stream));
+    if (nbsp_preset_generate((int)preset, n, parameters->random_seed, c->x, c->y, c->z, c->vx,
+                             c->vy, c->vz, c->m, c->scratch, c->stream) != 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "too few particles for the preset");
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->resident = 1;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
 NBodySimProStatus n_body_sim_pro_cuda_download(NBodySimProCudaContext* c,
                                                const NBodySimProParticleSystemView* view,
                                                NBodySimProError* error) {
@@ -895,5 +931,187 @@ NBodySimProStatus n_body_sim_pro_cuda_synchronize(NBodySimProCudaContext* c,
     if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* ---- checkpoints (checkpoint/checkpoint.h, src/c/checkpoint/checkpoint.c) ---------- */
+
+enum { CHECKPOINT_ARRAYS = 10, CHECKPOINT_CHUNK = 8 << 20 /* bytes per staging buffer */ };
+
+/* Two pinned staging buffers and their events; released by staging_free. */
+typedef struct Staging {
+    void* buffer[2];
+    cudaEvent_t done[2];
+} Staging;
+
+static void staging_free(Staging* s) {
+    for (int k = 0; k < 2; ++k) {
+        if (s->buffer[k] != NULL) cudaFreeHost(s->buffer[k]);
+        if (s->done[k] != NULL) cudaEventDestroy(s->done[k]);
+        s->buffer[k] = NULL;
+        s->done[k] = NULL;
+    }
+}
+
+static NBodySimProStatus staging_alloc(Staging* s, NBodySimProError* error) {
+    memset(s, 0, sizeof(*s));
+    for (int k = 0; k < 2; ++k) {
+        cudaError_t code = cudaMallocHost(&s->buffer[k], CHECKPOINT_CHUNK);
+        if (code == cudaSuccess) code = cudaEventCreateWithFlags(&s->done[k], cudaEventDisableTiming);
+        if (code != cudaSuccess) {
+            staging_free(s);
+            return cuda_fail(error, code, "checkpoint staging", __FILE__, __LINE__);
+        }
+    }
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* The state arrays in file order (checkpoint.c:49-53). */
+static void checkpoint_arrays(NBodySimProCudaContext* c, double* out[CHECKPOINT_ARRAYS]) {
+    double* const a[CHECKPOINT_ARRAYS] = {c->x, c->y, c->z, c->vx, c->vy, c->vz,
+                                          c->ax, c->ay, c->az, c->m};
+    memcpy(out, a, sizeof(a));
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_checkpoint_write(NBodySimProCudaContext* c,
+                                                       const char* path,
+                                                       const NBodySimProCheckpointHeader* header,
+                                                       NBodySimProError* error) {
+    if (c == NULL || path == NULL || header == NULL) /* checkpoint.c:13-17 */
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "path, view, and header must not be null");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    if (header->particle_count != c->n) /* :18-22 */
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "checkpoint particle count does not match the view");
+    CUDA_TRY(cudaSetDevice(c->device));
+    Staging st;
+    NBodySimProStatus s = staging_alloc(&st, error);
+    if (s != N_BODY_SIM_PRO_STATUS_OK) return s;
+    FILE* file = fopen(path, "wb");
+    if (file == NULL) {
+        staging_free(&st);
+        return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to open checkpoint file for writing");
+    }
+    const uint32_t magic = N_BODY_SIM_PRO_CHECKPOINT_MAGIC;
+    const uint32_t version = N_BODY_SIM_PRO_CHECKPOINT_VERSION;
+    const NBodySimProCheckpointHeader stored = *header;
+    int ok = fwrite(&magic, sizeof(magic), 1, file) == 1 &&
+             fwrite(&version, sizeof(version), 1, file) == 1 &&
+             fwrite(&stored, sizeof(stored), 1, file) == 1;
+    double* arrays[CHECKPOINT_ARRAYS];
+    checkpoint_arrays(c, arrays);
+    const size_t bytes = c->n * sizeof(double);
+    const size_t per_array = (bytes + CHECKPOINT_CHUNK - 1) / CHECKPOINT_CHUNK;
+    const size_t chunks = per_array * CHECKPOINT_ARRAYS;
+    cudaError_t code = cudaSuccess;
+    /* chunk j: array j / per_array, bytes [o, o + len) of it; copy j + 1 is in
+     * flight while chunk j is written */
+#define CHUNK_SPAN(j, arr, off, len)                                                 \
+    const size_t arr = (j) / per_array;                                             \
+    const size_t off = ((j) % per_array) * (size_t)CHECKPOINT_CHUNK;                \
+    const size_t len = bytes - off < (size_t)CHECKPOINT_CHUNK ? bytes - off : (size_t)CHECKPOINT_CHUNK
+    if (ok && chunks > 0) {
+        CHUNK_SPAN(0, a0, o0, l0);
+        code = cudaMemcpyAsync(st.buffer[0], (const char*)arrays[a0] + o0, l0,
+                               cudaMemcpyDeviceToHost, c->stream);
+        if (code == cudaSuccess) code = cudaEventRecord(st.done[0], c->stream);
+    }
+    for (size_t j = 0; ok && code == cudaSuccess && j < chunks; ++j) {
+        if (j + 1 < chunks) {
+            CHUNK_SPAN(j + 1, an, on, ln);
+            const int b = (int)((j + 1) & 1);
+            code = cudaMemcpyAsync(st.buffer[b], (const char*)arrays[an] + on, ln,
+                                   cudaMemcpyDeviceToHost, c->stream);
+            if (code == cudaSuccess) code = cudaEventRecord(st.done[b], c->stream);
+            if (code != cudaSuccess) break;
+        }
+        CHUNK_SPAN(j, aj, oj, lj);
+        (void)aj;
+        (void)oj;
+        code = cudaEventSynchronize(st.done[j & 1]);
+        if (code != cudaSuccess) break;
+        ok = fwrite(st.buffer[j & 1], lj, 1, file) == 1;
+    }
+#undef CHUNK_SPAN
+    cudaStreamSynchronize(c->stream);
+    staging_free(&st);
+    const int closed = fclose(file) == 0;
+    if (code != cudaSuccess) return cuda_fail(error, code, "checkpoint copy", __FILE__, __LINE__);
+    if (!ok) return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to write checkpoint array");
+    if (!closed) return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to close checkpoint file");
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_checkpoint_read(NBodySimProCudaContext* c, const char* path,
+                                                      NBodySimProCheckpointHeader* header,
+                                                      NBodySimProError* error) {
+    if (c == NULL || path == NULL || header == NULL) /* checkpoint.c:134-138 */
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "path, header, and particle system must not be null");
+    CUDA_TRY(cudaSetDevice(c->device));
+    FILE* file = fopen(path, "rb");
+    if (file == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to open checkpoint file for reading");
+    uint32_t magic = 0, version = 0;
+    if (fread(&magic, sizeof(magic), 1, file) != 1 || fread(&version, sizeof(version), 1, file) != 1) {
+        fclose(file);
+        return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to read checkpoint magic");
+    }
+    if (magic != N_BODY_SIM_PRO_CHECKPOINT_MAGIC) { /* :88-92 */
+        fclose(file);
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "not an N-Body Sim Pro checkpoint file");
+    }
+    if (version != N_BODY_SIM_PRO_CHECKPOINT_VERSION) {
+        fclose(file);
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "unsupported checkpoint version");
+    }
+    NBodySimProCheckpointHeader stored;
+    if (fread(&stored, sizeof(stored), 1, file) != 1) {
+        fclose(file);
+        return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to read checkpoint metadata");
+    }
+    NBodySimProStatus s = ensure_capacity(c, stored.particle_count, error);
+    if (s != N_BODY_SIM_PRO_STATUS_OK) {
+        fclose(file);
+        return s;
+    }
+    Staging st;
+    if ((s = staging_alloc(&st, error)) != N_BODY_SIM_PRO_STATUS_OK) {
+        fclose(file);
+        return s;
+    }
+    double* arrays[CHECKPOINT_ARRAYS];
+    checkpoint_arrays(c, arrays);
+    const size_t bytes = stored.particle_count * sizeof(double);
+    const size_t per_array = (bytes + CHECKPOINT_CHUNK - 1) / CHECKPOINT_CHUNK;
+    const size_t chunks = per_array * CHECKPOINT_ARRAYS;
+    cudaError_t code = cudaSuccess;
+    int ok = 1;
+    for (size_t j = 0; j < chunks; ++j) {
+        const size_t arr = j / per_array;
+        const size_t off = (j % per_array) * (size_t)CHECKPOINT_CHUNK;
+        const size_t len = bytes - off < (size_t)CHECKPOINT_CHUNK ? bytes - off : (size_t)CHECKPOINT_CHUNK;
+        const int b = (int)(j & 1);
+        if (j >= 2 && (code = cudaEventSynchronize(st.done[b])) != cudaSuccess) break;
+        if (fread(st.buffer[b], len, 1, file) != 1) { /* the copy of chunk j - 1 runs meanwhile */
+            ok = 0;
+            break;
+        }
+        code = cudaMemcpyAsync((char*)arrays[arr] + off, st.buffer[b], len, cudaMemcpyHostToDevice,
+                               c->stream);
+        if (code == cudaSuccess) code = cudaEventRecord(st.done[b], c->stream);
+        if (code != cudaSuccess) break;
+    }
+    cudaStreamSynchronize(c->stream);
+    staging_free(&st);
+    const int closed = fclose(file) == 0;
+    if (code != cudaSuccess) return cuda_fail(error, code, "checkpoint copy", __FILE__, __LINE__);
+    if (!ok) return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to read checkpoint array");
+    if (!closed) return FAIL(N_BODY_SIM_PRO_STATUS_IO_ERROR, "failed to close checkpoint file");
+    c->n = stored.particle_count;
+    c->n_padded = round_up(c->n, 256);
+    c->resident = 1;
+    *header = stored;
     return N_BODY_SIM_PRO_STATUS_OK;
 }

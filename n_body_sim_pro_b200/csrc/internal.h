@@ -124,6 +124,18 @@ NBSP_HIDDEN void nbsp_reference_subset(const double* x, const double* y, const d
 /* Write `bytes` of junk into `buffer` (used to flush L2 between timed runs). */
 NBSP_HIDDEN void nbsp_touch(void* buffer, size_t bytes, cudaStream_t stream);
 
+/* ---- device preset generation (presets.cu) -------------------------------- */
+
+/* FP64 scratch words nbsp_preset_generate needs for n particles. */
+NBSP_HIDDEN size_t nbsp_preset_scratch_doubles(size_t n);
+
+/* presets_parallel.c on the device into the FP64 state arrays (length n):
+ * `preset` is an NBodySimProSimulationPreset value.  Returns 0, or 1 when the
+ * count does not fit the preset (as the reference's INVALID_ARGUMENT). */
+NBSP_HIDDEN int nbsp_preset_generate(int preset, size_t n, uint64_t seed, double* x, double* y,
+                                     double* z, double* vx, double* vy, double* vz, double* m,
+                                     double* scratch, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -237,6 +237,189 @@ int oracle_preset_plummer_collision(OracleView* v, uint64_t seed, double scale_r
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Parallel presets: src/c/generation/presets_parallel.c.  Every particle draws */
+/* from its own generator seeded with mix_seed(master, index) (:36-41), so the */
+/* result does not depend on how the particles are split across threads.      */
+/* ------------------------------------------------------------------------- */
+
+/* Subtract the mean velocity of [start, start+count) given its running sums. */
+static void par_subtract_mean(OracleView* v, size_t start, size_t count, double sx, double sy,
+                              double sz) {
+    sx /= (double)count;
+    sy /= (double)count;
+    sz /= (double)count;
+    for (size_t k = 0; k < count; ++k) {
+        v->velocities_x[start + k] -= sx;
+        v->velocities_y[start + k] -= sy;
+        v->velocities_z[start + k] -= sz;
+    }
+}
+
+/* presets_parallel.c:91-155 (Plummer block; centre added, :428-431). */
+static void par_plummer_block(OracleView* v, uint64_t master, size_t start, size_t count,
+                              double a, double a2, double total_mass, double particle_mass,
+                              const double* centre) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (size_t k = 0; k < count; ++k) {
+        const size_t i = start + k;
+        OracleRng rng;
+        oracle_rng_init(&rng, oracle_mix_seed(master, i));
+        const double u = 1.0 - oracle_rng_next_double(&rng);
+        const double r = a / sqrt(pow(u, -2.0 / 3.0) - 1.0);
+        double dx, dy, dz;
+        unit_vector(&rng, &dx, &dy, &dz);
+        double px = r * dx, py = r * dy, pz = r * dz;
+        if (centre != NULL) {
+            px = px + centre[0];
+            py = py + centre[1];
+            pz = pz + centre[2];
+        }
+        const double sigma = sqrt(1.0 * total_mass / (6.0 * sqrt(a2 + r * r)));
+        const double vx = oracle_rng_next_gaussian(&rng) * sigma;
+        const double vy = oracle_rng_next_gaussian(&rng) * sigma;
+        const double vz = oracle_rng_next_gaussian(&rng) * sigma;
+        put(v, i, px, py, pz, vx, vy, vz, particle_mass);
+        sx += vx;
+        sy += vy;
+        sz += vz;
+    }
+    par_subtract_mean(v, start, count, sx, sy, sz);
+}
+
+/* presets_parallel.c:158-217 (exponential disk block, optional arms). */
+static void par_disk_block(OracleView* v, uint64_t master, size_t start, size_t count, double a,
+                           double h, double vc, double sigma, double twist, int arms,
+                           double particle_mass) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (size_t k = 0; k < count; ++k) {
+        const size_t i = start + k;
+        OracleRng rng;
+        oracle_rng_init(&rng, oracle_mix_seed(master, i));
+        const double e1 = -log(1.0 - oracle_rng_next_double(&rng));
+        const double e2 = -log(1.0 - oracle_rng_next_double(&rng));
+        const double r = a * (e1 + e2);
+        double phi = 2.0 * M_PI * oracle_rng_next_double(&rng);
+        if (twist > 0.0 && arms > 0) {
+            const double arm = oracle_rng_next_double(&rng) * (double)arms;
+            const double arm_phi = 2.0 * M_PI * arm / (double)arms + twist * r / a;
+            phi = arm_phi + oracle_rng_next_gaussian(&rng) * 0.15;
+        }
+        const double z = oracle_rng_next_gaussian(&rng) * h;
+        const double tx = -sin(phi), ty = cos(phi);
+        const double px = r * cos(phi), py = r * sin(phi);
+        const double vx = vc * tx + oracle_rng_next_gaussian(&rng) * sigma;
+        const double vy = vc * ty + oracle_rng_next_gaussian(&rng) * sigma;
+        const double vz = oracle_rng_next_gaussian(&rng) * sigma * 0.5;
+        put(v, i, px, py, z, vx, vy, vz, particle_mass);
+        sx += vx;
+        sy += vy;
+        sz += vz;
+    }
+    par_subtract_mean(v, start, count, sx, sy, sz);
+}
+
+int oracle_preset_parallel(OracleView* v, int preset, uint64_t seed) {
+    const size_t n = v->particle_count;
+    switch (preset) {
+        case 0: /* two body, :43-57 */
+            return oracle_preset_two_body(v);
+        case 1: { /* random cloud, :219-272 */
+            if (n == 0) return 1;
+            const double mass = 1.0 / (double)n;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            for (size_t i = 0; i < n; ++i) {
+                OracleRng rng;
+                oracle_rng_init(&rng, oracle_mix_seed(seed, i));
+                double dx, dy, dz;
+                unit_vector(&rng, &dx, &dy, &dz);
+                const double r = cbrt(oracle_rng_next_double(&rng));
+                const double vx = rng_range(&rng, -0.05, 0.05);
+                const double vy = rng_range(&rng, -0.05, 0.05);
+                const double vz = rng_range(&rng, -0.05, 0.05);
+                put(v, i, r * dx, r * dy, r * dz, vx, vy, vz, mass);
+                sx += vx;
+                sy += vy;
+                sz += vz;
+            }
+            par_subtract_mean(v, 0, n, sx, sy, sz);
+            return 0;
+        }
+        case 2: { /* solar system, :59-89: one sequential stream seeded with `seed` */
+            if (n == 0) return 1;
+            OracleRng rng;
+            oracle_rng_init(&rng, seed);
+            put(v, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0);
+            const size_t planets = n - 1;
+            for (size_t k = 0; k < planets; ++k) {
+                const double r = 1.0 + 3.0 * (double)k / (double)planets;
+                const double speed = sqrt(1 / r);
+                const double phi = 2.0 * M_PI * oracle_rng_next_double(&rng);
+                put(v, k + 1, r * cos(phi), r * sin(phi), 0.0, -speed * sin(phi),
+                    speed * cos(phi), 0.0, 0.001);
+            }
+            return 0;
+        }
+        case 3: { /* open cluster, :274-311 */
+            if (n == 0) return 1;
+            const double mass = 1.0 / (double)n;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            for (size_t i = 0; i < n; ++i) {
+                OracleRng rng;
+                oracle_rng_init(&rng, oracle_mix_seed(seed, i));
+                const double px = oracle_rng_next_gaussian(&rng) * 0.3;
+                const double py = oracle_rng_next_gaussian(&rng) * 0.3;
+                const double pz = oracle_rng_next_gaussian(&rng) * 0.3;
+                const double vx = oracle_rng_next_gaussian(&rng) * 0.02;
+                const double vy = oracle_rng_next_gaussian(&rng) * 0.02;
+                const double vz = oracle_rng_next_gaussian(&rng) * 0.02;
+                put(v, i, px, py, pz, vx, vy, vz, mass);
+                sx += vx;
+                sy += vy;
+                sz += vz;
+            }
+            par_subtract_mean(v, 0, n, sx, sy, sz);
+            return 0;
+        }
+        case 4: /* globular cluster, :372-376 */
+        case 6: /* elliptical galaxy */
+            if (n == 0) return 1;
+            if (preset == 4) {
+                par_plummer_block(v, seed, 0, n, 1.0, 1.0 * 1.0, 1.0, 1.0 / (double)n, NULL);
+            } else {
+                par_plummer_block(v, seed, 0, n, 2.0, 2.0 * 2.0, 1.0, 1.0 / (double)n, NULL);
+            }
+            return 0;
+        case 5: /* spiral galaxy, :378-383 */
+            if (n == 0) return 1;
+            par_disk_block(v, seed, 0, n, 0.7, 0.1, 1.0, 0.12, 3.5, 2, 1.0 / (double)n);
+            return 0;
+        case 7: { /* galaxy collision, :384-396: particles past 2 * (n / 2) are left as they are */
+            const size_t half = n / 2;
+            if (half == 0) return 1;
+            const double mass = 0.5 / (double)half;
+            par_disk_block(v, oracle_mix_seed(seed, 0), 0, half, 0.7, 0.1, 1.0, 0.12, 0.0, 0, mass);
+            par_disk_block(v, oracle_mix_seed(seed, 1), half, half, 0.7, 0.1, 1.0, 0.12, 0.0, 0,
+                           mass);
+            for (size_t i = 0; i < n; ++i) v->velocities_x[i] += i < half ? 0.35 : -0.35;
+            return 0;
+        }
+        case 8: { /* triple galaxy, :397-471: particles past 3 * (n / 3) are left as they are */
+            const size_t third = n / 3;
+            if (third == 0) return 1;
+            const double centres[3][3] = {{-1.8, 0.0, 0.0}, {1.8, 0.0, 0.0}, {0.0, 1.8, 0.0}};
+            for (int g = 0; g < 3; ++g) {
+                /* a = 0.7 with the literal 0.49 in the dispersion (:446), galaxy mass 1/3 */
+                par_plummer_block(v, oracle_mix_seed(seed, (uint64_t)g), (size_t)g * third, third,
+                                  0.7, 0.49, 1.0 / 3.0, (1.0 / 3.0) / (double)third, centres[g]);
+            }
+            return 0;
+        }
+        default:
+            return 1;
+    }
+}
+
 int oracle_preset_uniform_log_mass(OracleView* v, uint64_t seed) {
     const size_t n = v->particle_count;
     if (n == 0) return 1;

@@ -62,6 +62,10 @@ int oracle_preset_plummer_collision(OracleView* view, uint64_t seed, double scal
                                     double separation, double relative_speed);
 /* Uniform positions in [0,1)^3, masses 10^U(-3,0) normalised to 1, zero velocity. */
 int oracle_preset_uniform_log_mass(OracleView* view, uint64_t seed);
+/* src/c/generation/presets_parallel.c (n_body_sim_pro_preset_generate_parallel,
+ * include/n_body_sim_pro/generation/presets.h:73): preset ids as the reference's
+ * NBodySimProSimulationPreset enum (presets.h:27-38). 0 on success. */
+int oracle_preset_parallel(OracleView* view, int preset, uint64_t seed);
 /* Size of ensemble member k: round(exp(U(ln lo, ln hi))) from rng(mix_seed(master, k)). */
 size_t oracle_ensemble_member_size(uint64_t master_seed, uint64_t k, size_t lo, size_t hi);
 /* Plummer sphere (a = 1, M = 1) for ensemble member k, same stream as the size draw. */

@@ -193,6 +193,11 @@ def ref() -> C.CDLL:
         R.n_body_sim_pro_particle_system_view.argtypes = [C.c_void_p, pv, pe]
         R.n_body_sim_pro_preset_generate.restype = C.c_int
         R.n_body_sim_pro_preset_generate.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t * 2), pe]
+        R.n_body_sim_pro_checkpoint_write.restype = C.c_int
+        R.n_body_sim_pro_checkpoint_write.argtypes = [C.c_char_p, pv, C.POINTER(CheckpointHeader), pe]
+        R.n_body_sim_pro_preset_generate_parallel.restype = C.c_int
+        R.n_body_sim_pro_preset_generate_parallel.argtypes = [C.c_void_p, C.c_int,
+                                                              C.POINTER(C.c_size_t * 2), pe]
         R.ref_shim_morton_order.restype = C.c_int
         R.ref_shim_morton_order.argtypes = [pv, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                             C.POINTER(C.c_double), C.POINTER(C.c_size_t)]
@@ -230,6 +235,31 @@ def preset(name: str, n: int, seed: int) -> Particles:
     return p
 
 
+# NBodySimProSimulationPreset (include/n_body_sim_pro/generation/presets.h:27-38)
+PRESET_IDS = {"two_body": 0, "random_cloud": 1, "solar_system": 2, "open_cluster": 3,
+              "globular_cluster": 4, "spiral_galaxy": 5, "elliptical_galaxy": 6,
+              "galaxy_collision": 7, "triple_galaxy": 8}
+
+
+def preset_parallel(name: str, n: int, seed: int) -> Particles:
+    """presets_parallel.c restated (per-particle generators seeded by index)."""
+    p = Particles.zeros(n)
+    v = p.view()
+    if lib().oracle_preset_parallel(C.byref(v), PRESET_IDS[name], seed) != 0:
+        raise RuntimeError(f"oracle parallel preset {name} failed")
+    return p
+
+
+def filled_count(name: str, n: int) -> int:
+    """Particles the parallel generator writes (galaxy_collision and
+    triple_galaxy leave the last n % 2 / n % 3 untouched)."""
+    if name == "galaxy_collision":
+        return 2 * (n // 2)
+    if name == "triple_galaxy":
+        return 3 * (n // 3)
+    return n
+
+
 def ensemble_member(master_seed: int, k: int, lo: int = 32, hi: int = 4096) -> Particles:
     L = lib()
     n = L.oracle_ensemble_member_size(master_seed, k, lo, hi)
@@ -240,13 +270,19 @@ def ensemble_member(master_seed: int, k: int, lo: int = 32, hi: int = 4096) -> P
     return p
 
 
-def ref_preset(name: str, n: int, seed: int) -> Particles:
-    """The same preset produced by the reference engine itself."""
+def ref_preset(name: str, n: int, seed: int, parallel: bool = False) -> Particles:
+    """The same preset produced by the reference engine itself (`parallel`:
+    n_body_sim_pro_preset_generate_parallel; unfilled entries come back as
+    whatever the reference's allocation held)."""
     R = ref()
     ps = R.n_body_sim_pro_particle_system_create(n)
     err = Error()
     params = (C.c_size_t * 2)(n, seed)
-    rc = R.n_body_sim_pro_preset_generate(ps, PRESETS[name], C.byref(params), C.byref(err))
+    if parallel:
+        rc = R.n_body_sim_pro_preset_generate_parallel(ps, PRESET_IDS[name], C.byref(params),
+                                                       C.byref(err))
+    else:
+        rc = R.n_body_sim_pro_preset_generate(ps, PRESETS[name], C.byref(params), C.byref(err))
     if rc != 0:
         R.n_body_sim_pro_particle_system_destroy(ps)
         raise RuntimeError(f"reference preset failed: {err.message!r}")
@@ -371,6 +407,44 @@ def ref_barnes_hut(p: Particles, G: float, eps: float, theta: float):
     if rc != 0:
         raise RuntimeError(err.message)
     return p.acc(), {f: int(getattr(st, f)) for f, _ in BHStats._fields_[:6]}
+
+
+# ---------------------------------------------------------------------------
+# Checkpoint files: src/c/checkpoint/checkpoint.c:9-76
+# ---------------------------------------------------------------------------
+
+class CheckpointHeader(C.Structure):
+    """NBodySimProCheckpointHeader (include/n_body_sim_pro/checkpoint/checkpoint.h:29-40)."""
+
+    _fields_ = [("magic", C.c_uint32), ("version", C.c_uint32), ("particle_count", C.c_size_t),
+                ("simulation_time", C.c_double), ("timestep", C.c_double),
+                ("integrator", C.c_int32), ("theta", C.c_double),
+                ("barnes_hut_enabled", C.c_int32), ("random_seed", C.c_uint64),
+                ("preset", C.c_int32)]
+
+
+CHECKPOINT_MAGIC = 0x53504348   # checkpoint.h:27
+CHECKPOINT_VERSION = 1
+
+
+def checkpoint_bytes(header: CheckpointHeader, p: Particles) -> bytes:
+    """The file n_body_sim_pro_checkpoint_write produces: magic and version
+    (u32 each), the header struct as stored (padding included), then the ten
+    FP64 arrays x y z vx vy vz ax ay az m (checkpoint.c:31-72)."""
+    out = bytearray()
+    out += np.uint32(CHECKPOINT_MAGIC).tobytes() + np.uint32(CHECKPOINT_VERSION).tobytes()
+    out += bytes(header)
+    for f in FIELDS:
+        out += np.ascontiguousarray(getattr(p, f), dtype=np.float64).tobytes()
+    return bytes(out)
+
+
+def ref_checkpoint_write(path: str, header: CheckpointHeader, p: Particles) -> int:
+    """The reference's own writer on the same state (status code)."""
+    v = p.view()
+    err = Error()
+    return ref().n_body_sim_pro_checkpoint_write(os.fsencode(path), C.byref(v), C.byref(header),
+                                                 C.byref(err))
 
 
 def rms_relative_error(a: np.ndarray, ref_a: np.ndarray) -> float:

@@ -32,6 +32,29 @@ def test_presets_bit_identical_to_reference(name, n, seed):
         assert np.array_equal(getattr(a, f), getattr(b, f)), f
 
 
+def _reference_openmp_single_thread():
+    """The reference's random_cloud sums velocities in an OpenMP reduction
+    (presets_parallel.c:232); with one thread that sum runs in index order."""
+    import ctypes
+    ctypes.CDLL("libgomp.so.1").omp_set_num_threads(1)
+
+
+@needs_ref
+@pytest.mark.parametrize("name,n,seed", [
+    ("two_body", 2, 1), ("random_cloud", 777, 42), ("solar_system", 9, 3),
+    ("open_cluster", 500, 5), ("globular_cluster", 1500, 42), ("spiral_galaxy", 640, 99),
+    ("elliptical_galaxy", 333, 8), ("galaxy_collision", 801, 12), ("triple_galaxy", 1001, 4)])
+def test_parallel_presets_bit_identical_to_reference(name, n, seed):
+    """presets_parallel.c restated: every filled particle equals the reference's."""
+    _reference_openmp_single_thread()
+    a, b = O.preset_parallel(name, n, seed), O.ref_preset(name, n, seed, parallel=True)
+    k = O.filled_count(name, n)
+    for f in STATE:
+        assert np.array_equal(getattr(a, f)[:k], getattr(b, f)[:k]), f
+    if k < n:  # the unfilled tail only gets the approach velocity (collision)
+        assert np.all(a.x[k:] == 0.0)
+
+
 @needs_ref
 @pytest.mark.parametrize("eps", [0.02, 0.0])
 def test_gravity_bit_identical_to_reference(eps):
@@ -235,3 +258,22 @@ def test_golden_barnes_hut():
     assert [s[k] for k in ("node_count", "leaf_count", "internal_node_count",
                            "accepted_approximations", "exact_interactions",
                            "maximum_depth")] == list(g["stats_theta07"])
+
+
+def _header(n: int) -> "O.CheckpointHeader":
+    h = O.CheckpointHeader()
+    h.magic, h.version, h.particle_count = O.CHECKPOINT_MAGIC, O.CHECKPOINT_VERSION, n
+    h.simulation_time, h.timestep, h.integrator = 0.125, 1e-3, 1
+    h.theta, h.barnes_hut_enabled, h.random_seed, h.preset = 0.7, 1, 42, 4
+    return h
+
+
+@needs_ref
+def test_checkpoint_format_equals_reference_writer(tmp_path):
+    """checkpoint.c:9-76 restated: the oracle's bytes are the reference's file."""
+    p = O.preset("globular_cluster", 1000, 42)
+    O.gravity_reference(p, 1.0, 0.01)
+    path = str(tmp_path / "ref.hpcs")
+    assert O.ref_checkpoint_write(path, _header(p.n), p) == 0
+    with open(path, "rb") as f:
+        assert f.read() == O.checkpoint_bytes(_header(p.n), p)
