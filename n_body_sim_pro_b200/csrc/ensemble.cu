@@ -27,6 +27,32 @@ __device__ __forceinline__ float rsqrt_mufu(float x) {
   return r;
 }
 
+// Paired FP32 (sm_100 .f32x2): two targets share every add / mul / fma.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
 __device__ __forceinline__ void fold(float& hi, float& lo, float a) {
   const float s = __fadd_rn(hi, a);
   const float bp = __fsub_rn(s, hi);
@@ -51,11 +77,18 @@ struct EnsembleArgs {
   int steps;
 };
 
-constexpr int kTile = 32;  // sources per compensated fold
+constexpr int kTile = 32;         // sources per compensated fold
+constexpr float kFarAway = 1e30f;  // padding sources: r^2 overflows to inf, rsqrt(inf) = 0
 
-template <int BLOCK, int K>
+// GUARD: drop r^2 = 0 terms (eps = 0, or m / eps^3 could overflow); otherwise
+// a target's own entry has d = 0 and adds W * 0 = 0.
+template <int BLOCK, int K, bool GUARD>
 __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
-  extern __shared__ float4 sp[];  // BLOCK * K positions
+  static_assert(K % 2 == 0, "targets are processed in pairs");
+  constexpr int P = K / 2;
+  // BLOCK * K particles, each as two float4 (x, x, y, y), (z, z, m, m): one
+  // 16-byte load yields the broadcast operands of two paired instructions
+  extern __shared__ float4 sp[];
   __shared__ int s_item;
   const int tid = threadIdx.x;
   for (int guard = 0;; ++guard) {
@@ -80,7 +113,7 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
       if (lane == 0) atomicOr(a.status, NBSP_DEVICE_ERROR_ENSEMBLE_LIMIT);
       n = G * K;
     }
-    float4* pos = sp + sub * (G * K);
+    float4* pos = sp + 2 * sub * (G * K);  // particle i at pos[2 i], pos[2 i + 1]
     const double cx = has ? a.centre[3 * sys] : 0.0;
     const double cy = has ? a.centre[3 * sys + 1] : 0.0;
     const double cz = has ? a.centre[3 * sys + 2] : 0.0;
@@ -89,45 +122,75 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
       const int i = lane + k * G;
       if (i < n) {
         const long long p = off + i;
-        pos[i] = make_float4((float)__dsub_rn(a.x[p], cx), (float)__dsub_rn(a.y[p], cy),
-                             (float)__dsub_rn(a.z[p], cz), (float)a.m[p]);
+        const float px = (float)__dsub_rn(a.x[p], cx), py = (float)__dsub_rn(a.y[p], cy);
+        const float pz = (float)__dsub_rn(a.z[p], cz), pm = (float)a.m[p];
+        pos[2 * i] = make_float4(px, px, py, py);
+        pos[2 * i + 1] = make_float4(pz, pz, pm, pm);
       }
     }
+    // pad the system to whole tiles with massless far sources (fixed-count loops)
+    const int n_pad = (n + kTile - 1) / kTile * kTile;  // <= G * K (a multiple of 128)
+    for (int i = n + lane; i < n_pad; i += G) {
+      pos[2 * i] = make_float4(kFarAway, kFarAway, kFarAway, kFarAway);
+      pos[2 * i + 1] = make_float4(kFarAway, kFarAway, 0.f, 0.f);
+    }
     __syncthreads();
+    const unsigned long long E2 = pack2(a.eps2, a.eps2);
     for (int step = 0; step <= a.steps; ++step) {
-      float xi[K], yi[K], zi[K], hx[K], hy[K], hz[K], lx[K], ly[K], lz[K];
+      unsigned long long X[P], Y[P], Z[P];
+      float hx[K], hy[K], hz[K], lx[K], ly[K], lz[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int i = lane + k * G;
-        const float4 q = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        xi[k] = q.x;
-        yi[k] = q.y;
-        zi[k] = q.z;
-        hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+      for (int q = 0; q < P; ++q) {
+        const int i0 = lane + (2 * q) * G, i1 = lane + (2 * q + 1) * G;
+        const float4 u0 = i0 < n ? pos[2 * i0] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 u1 = i0 < n ? pos[2 * i0 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v0 = i1 < n ? pos[2 * i1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v1 = i1 < n ? pos[2 * i1 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        X[q] = pack2(u0.x, v0.x);
+        Y[q] = pack2(u0.z, v0.z);
+        Z[q] = pack2(u1.x, v1.x);
       }
-      for (int j0 = 0; j0 < n; j0 += kTile) {
-        const int j1 = min(j0 + kTile, n);
-        float px[K], py[K], pz[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) px[k] = py[k] = pz[k] = 0.f;
-        for (int j = j0; j < j1; ++j) {
-          const float4 s = pos[j];
+      for (int k = 0; k < K; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+      for (int j0 = 0; j0 < n_pad; j0 += kTile) {
+        unsigned long long AX[P], AY[P], AZ[P];
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const float dx = s.x - xi[k], dy = s.y - yi[k], dz = s.z - zi[k];
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, a.eps2)));
-            const float rinv = r2 > 0.f ? rsqrt_mufu(r2) : 0.f;  // self pair contributes 0
-            const float wgt = s.w * (rinv * rinv * rinv);
-            px[k] = fmaf(wgt, dx, px[k]);
-            py[k] = fmaf(wgt, dy, py[k]);
-            pz[k] = fmaf(wgt, dz, pz[k]);
+        for (int q = 0; q < P; ++q) AX[q] = AY[q] = AZ[q] = 0ull;
+#pragma unroll 8
+        for (int j = 0; j < kTile; ++j) {
+          const ulonglong2 s0 = reinterpret_cast<const ulonglong2*>(pos)[2 * (j0 + j)];
+          const ulonglong2 s1 = reinterpret_cast<const ulonglong2*>(pos)[2 * (j0 + j) + 1];
+          const unsigned long long SX = s0.x, SY = s0.y, SZ = s1.x, SW = s1.y;
+#pragma unroll
+          for (int q = 0; q < P; ++q) {
+            const unsigned long long dx = sub2(SX, X[q]), dy = sub2(SY, Y[q]), dz = sub2(SZ, Z[q]);
+            const unsigned long long r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+            float r2a, r2b;
+            unpack2(r2, r2a, r2b);
+            float ra = rsqrt_mufu(r2a), rb = rsqrt_mufu(r2b);
+            if (GUARD) {  // the self pair (r^2 = 0 when eps = 0) contributes 0
+              ra = r2a > 0.f ? ra : 0.f;
+              rb = r2b > 0.f ? rb : 0.f;
+            }
+            const unsigned long long R = pack2(ra, rb);
+            const unsigned long long W = mul2(SW, mul2(mul2(R, R), R));
+            AX[q] = fma2(W, dx, AX[q]);
+            AY[q] = fma2(W, dy, AY[q]);
+            AZ[q] = fma2(W, dz, AZ[q]);
           }
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          fold(hx[k], lx[k], px[k]);
-          fold(hy[k], ly[k], py[k]);
-          fold(hz[k], lz[k], pz[k]);
+        for (int q = 0; q < P; ++q) {
+          float u, v;
+          unpack2(AX[q], u, v);
+          fold(hx[2 * q], lx[2 * q], u);
+          fold(hx[2 * q + 1], lx[2 * q + 1], v);
+          unpack2(AY[q], u, v);
+          fold(hy[2 * q], ly[2 * q], u);
+          fold(hy[2 * q + 1], ly[2 * q + 1], v);
+          unpack2(AZ[q], u, v);
+          fold(hz[2 * q], lz[2 * q], u);
+          fold(hz[2 * q + 1], lz[2 * q + 1], v);
         }
       }
       float4 next[K];
@@ -171,7 +234,10 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const int i = lane + k * G;
-          if (i < n) pos[i] = next[k];
+          if (i < n) {
+            pos[2 * i] = make_float4(next[k].x, next[k].x, next[k].y, next[k].y);
+            pos[2 * i + 1] = make_float4(next[k].z, next[k].z, next[k].w, next[k].w);
+          }
         }
       }
       __syncthreads();
@@ -181,10 +247,10 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
 
 typedef void (*EnsembleKernel)(EnsembleArgs);
 
-EnsembleKernel select(int block, int k) {
-  if (block == 512 && k == 8) return ensemble_kernel<512, 8>;
-  if (block == 1024 && k == 4) return ensemble_kernel<1024, 4>;
-  if (block == 256 && k == 16) return ensemble_kernel<256, 16>;
+EnsembleKernel select(int block, int k, bool guard) {
+  if (block == 512 && k == 8) return guard ? ensemble_kernel<512, 8, true> : ensemble_kernel<512, 8, false>;
+  if (block == 1024 && k == 4) return guard ? ensemble_kernel<1024, 4, true> : ensemble_kernel<1024, 4, false>;
+  if (block == 256 && k == 16) return guard ? ensemble_kernel<256, 16, true> : ensemble_kernel<256, 16, false>;
   return nullptr;
 }
 
@@ -193,13 +259,13 @@ EnsembleKernel select(int block, int k) {
 extern "C" {
 
 int nbsp_ensemble_shape_supported(int block, int per_thread) {
-  return select(block, per_thread) != nullptr;
+  return select(block, per_thread, false) != nullptr;
 }
 
 int nbsp_ensemble_resident_ctas(int block, int per_thread) {
-  EnsembleKernel k = select(block, per_thread);
+  EnsembleKernel k = select(block, per_thread, true);
   if (k == nullptr) return 0;
-  const int smem = block * per_thread * 16;
+  const int smem = block * per_thread * 32;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   int ctas = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, k, block, smem) != cudaSuccess) return 0;
@@ -211,8 +277,8 @@ void nbsp_ensemble_advance(int block, int per_thread, int grid, double* x, doubl
                            const double* m, const long long* offset, const double* centre,
                            const int* item_start, const int* item_systems, const int* item_group,
                            int items, int* counter, int* status, double g, float eps2, double dt,
-                           int steps, cudaStream_t stream) {
-  EnsembleKernel k = select(block, per_thread);
+                           int steps, int guard, cudaStream_t stream) {
+  EnsembleKernel k = select(block, per_thread, guard != 0);
   if (k == nullptr) return;
   EnsembleArgs a;
   a.x = x;
@@ -238,7 +304,7 @@ void nbsp_ensemble_advance(int block, int per_thread, int grid, double* x, doubl
   a.dt = dt;
   a.eps2 = eps2;
   a.steps = steps;
-  const int smem = block * per_thread * 16;
+  const int smem = block * per_thread * 32;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   NBSP_COUNT_LAUNCH(1), k<<<grid, block, smem, stream>>>(a);
 }

@@ -14,6 +14,7 @@
 #include "internal.h"
 
 #include <cuda_runtime_api.h>
+#include <float.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -29,7 +30,7 @@ NBSP_HIDDEN void nbsp_ensemble_advance(int block, int per_thread, int grid, doub
                                        const int* item_start, const int* item_systems,
                                        const int* item_group, int items, int* counter,
                                        int* status, double g, float eps2, double dt, int steps,
-                                       cudaStream_t stream);
+                                       int guard, cudaStream_t stream);
 
 enum { ENS_MAX_SYSTEM = 4096, ENS_SHAPES = 3 };
 
@@ -48,6 +49,7 @@ struct NBodySimProCudaEnsemble {
     cudaEvent_t ev[2];
     size_t systems, particles;
     double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *m, *centre;
+    double max_mass; /* largest |m|: decides whether the self pair needs a guard */
     long long* offset;      /* device */
     long long* host_offset; /* host */
     int *d_item_start, *d_item_systems, *d_item_group;
@@ -345,6 +347,8 @@ NBodySimProStatus n_body_sim_pro_cuda_ensemble_upload(NBodySimProCudaEnsemble* e
         return efail(error, N_BODY_SIM_PRO_STATUS_OUT_OF_MEMORY, __LINE__, "ensemble tables");
     }
     for (size_t s = 0; s <= systems; ++s) e->host_offset[s] = (long long)offsets[s];
+    e->max_mass = 0.0;
+    for (size_t i = 0; i < n; ++i) e->max_mass = fmax(e->max_mass, fabs(view->masses[i]));
     /* FP64 centre of mass of every system: the origin of its FP32 coordinates */
     for (size_t s = 0; s < systems; ++s) {
         double mt = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
@@ -396,13 +400,21 @@ NBodySimProStatus n_body_sim_pro_cuda_ensemble_download(NBodySimProCudaEnsemble*
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
+/* The unguarded kernel relies on the self pair adding W * 0 = 0: eps^2 a
+ * normal float and m / eps^3 far from overflow. */
+static int self_pair_needs_guard(const NBodySimProCudaEnsemble* e, float eps2) {
+    if (!(eps2 >= FLT_MIN)) return 1;
+    const double inv_eps3 = 1.0 / ((double)eps2 * sqrt((double)eps2));
+    return !(e->max_mass * inv_eps3 < 1e30);
+}
+
 static void enqueue_persistent(NBodySimProCudaEnsemble* e, double g, float eps2, double dt,
                                int steps) {
     cudaMemsetAsync(e->counter, 0, sizeof(int), e->stream);
     nbsp_ensemble_advance(e->block, e->per_thread, e->grid, e->x, e->y, e->z, e->vx, e->vy, e->vz,
                           e->ax, e->ay, e->az, e->m, e->offset, e->centre, e->d_item_start,
                           e->d_item_systems, e->d_item_group, e->items, e->counter, e->status, g,
-                          eps2, dt, steps, e->stream);
+                          eps2, dt, steps, self_pair_needs_guard(e, eps2), e->stream);
 }
 
 /* One launch per system per phase (the baseline the persistent launch replaces). */
