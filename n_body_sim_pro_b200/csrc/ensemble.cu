@@ -77,7 +77,7 @@ struct EnsembleArgs {
   int steps;
 };
 
-constexpr int kTile = 32;         // sources per compensated fold
+constexpr int kTile = 64;         // sources per compensated fold
 constexpr float kFarAway = 1e30f;  // padding sources: r^2 overflows to inf, rsqrt(inf) = 0
 
 // GUARD: drop r^2 = 0 terms (eps = 0, or m / eps^3 could overflow); otherwise
@@ -109,9 +109,9 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
     const int sys = has ? a.item_systems[first + sub] : 0;
     const long long off = has ? a.offset[sys] : 0;
     int n = has ? (int)(a.offset[sys + 1] - off) : 0;
-    if (n > G * K) {  // the host sizes G so this cannot happen
+    if ((n + kTile - 1) / kTile * kTile > G * K) {  // the host sizes G so this cannot happen
       if (lane == 0) atomicOr(a.status, NBSP_DEVICE_ERROR_ENSEMBLE_LIMIT);
-      n = G * K;
+      n = 0;  // the padded system would not fit its shared-memory slots: skip it
     }
     float4* pos = sp + 2 * sub * (G * K);  // particle i at pos[2 i], pos[2 i + 1]
     const double cx = has ? a.centre[3 * sys] : 0.0;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
       }
     }
     // pad the system to whole tiles with massless far sources (fixed-count loops)
-    const int n_pad = (n + kTile - 1) / kTile * kTile;  // <= G * K (a multiple of 128)
+    const int n_pad = (n + kTile - 1) / kTile * kTile;  // <= G * K (checked above)
     for (int i = n + lane; i < n_pad; i += G) {
       pos[2 * i] = make_float4(kFarAway, kFarAway, kFarAway, kFarAway);
       pos[2 * i + 1] = make_float4(kFarAway, kFarAway, 0.f, 0.f);
@@ -193,13 +193,19 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
           fold(hz[2 * q + 1], lz[2 * q + 1], v);
         }
       }
+      // the FP64 origin and offset are reloaded here (L1 hits) rather than held
+      // in registers through the force loop
+      const long long off_e = has ? a.offset[sys] : 0;
+      const double cxe = has ? a.centre[3 * sys] : 0.0;
+      const double cye = has ? a.centre[3 * sys + 1] : 0.0;
+      const double cze = has ? a.centre[3 * sys + 2] : 0.0;
       float4 next[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int i = lane + k * G;
         next[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (i >= n) continue;
-        const long long p = off + i;
+        const long long p = off_e + i;
         const double a0 = a.g * ((double)hx[k] + (double)lx[k]);
         const double a1 = a.g * ((double)hy[k] + (double)ly[k]);
         const double a2 = a.g * ((double)hz[k] + (double)lz[k]);
@@ -222,8 +228,8 @@ __global__ void __launch_bounds__(BLOCK, 1) ensemble_kernel(EnsembleArgs a) {
           a.x[p] = nx;
           a.y[p] = ny;
           a.z[p] = nz;
-          next[k] = make_float4((float)__dsub_rn(nx, cx), (float)__dsub_rn(ny, cy),
-                                (float)__dsub_rn(nz, cz), (float)a.m[p]);
+          next[k] = make_float4((float)__dsub_rn(nx, cxe), (float)__dsub_rn(ny, cye),
+                                (float)__dsub_rn(nz, cze), (float)a.m[p]);
         }
         a.vx[p] = u;
         a.vy[p] = v;

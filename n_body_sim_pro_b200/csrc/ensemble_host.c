@@ -32,7 +32,7 @@ NBSP_HIDDEN void nbsp_ensemble_advance(int block, int per_thread, int grid, doub
                                        int* status, double g, float eps2, double dt, int steps,
                                        int guard, cudaStream_t stream);
 
-enum { ENS_MAX_SYSTEM = 4096, ENS_SHAPES = 3 };
+enum { ENS_MAX_SYSTEM = 4096, ENS_SHAPES = 3, ENS_TILE = 64 /* = kTile in ensemble.cu */ };
 
 static const int kEnsShapes[ENS_SHAPES][2] = {{512, 8}, {1024, 4}, {256, 16}};
 
@@ -193,6 +193,14 @@ static int by_cost_desc(const void* a, const void* b) {
     return x->index - y->index;
 }
 
+/* Threads of the subgroup that owns a system of n particles: the kernel pads
+ * each system to whole tiles of ENS_TILE sources (ensemble.cu kTile), and the
+ * subgroup's G * k shared-memory slots must hold the padded system. */
+static int group_threads(long long n, int k) {
+    const long long padded = (n + ENS_TILE - 1) / ENS_TILE * ENS_TILE;
+    return (int)next_pow2((unsigned)((padded + k - 1) / k));
+}
+
 /* Bundle systems into work items for threads-per-CTA `block` and `k` targets
  * per thread; items ordered by cost (sum n^2), largest first. */
 static int build_items(const long long* off, size_t systems, int block, int k, Items* out) {
@@ -218,7 +226,7 @@ static int build_items(const long long* off, size_t systems, int block, int k, I
     int* cursor = list;
     while (s < systems) {
         const long long n = order[s].cost;
-        const int g = (int)next_pow2((unsigned)((n + k - 1) / k));
+        const int g = group_threads(n, k);
         const int per_item = block / g;
         tmp_start[items] = (int)(cursor - list);
         tmp_group[items] = g;
@@ -226,7 +234,7 @@ static int build_items(const long long* off, size_t systems, int block, int k, I
         int taken = 0;
         while (s < systems && taken < per_item) {
             const long long m = order[s].cost;
-            if ((int)next_pow2((unsigned)((m + k - 1) / k)) != g) break;
+            if (group_threads(m, k) != g) break;
             *cursor++ = order[s].index;
             c += m * m;
             ++taken;

@@ -73,6 +73,20 @@ def test_ensemble_matches_per_system_oracle(cuda, per_system):
         assert sum(1 for t in info["autotune_ms"] if t > 0) >= 2
 
 
+def test_ensemble_many_tiny_systems(cuda):
+    """Hundreds of 1..40-particle systems share work items: each is padded to
+    whole source tiles inside its own shared-memory slots."""
+    members, s, offsets = make_ensemble(cuda, sizes_seed=21, count=300, lo=1, hi=40)
+    g = cuda.gravity_init(1.0, 0.01)
+    expected = oracle_run(members, 0.01, 1e-3, 5)
+    with cuda.CudaEnsemble() as e:
+        e.upload(s, offsets)
+        e.advance(g, 1e-3, 5)
+        out = cuda.ParticleSystem.zeros(s.n)
+        e.download(out)
+    check(cuda, out, offsets, expected, span=5e-3)
+
+
 def test_ensemble_repeated_advance_and_graph_reuse(cuda):
     members, s, offsets = make_ensemble(cuda, count=24)
     g = cuda.gravity_init(1.0, 0.01)
