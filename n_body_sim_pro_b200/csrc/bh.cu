@@ -1513,6 +1513,25 @@ __global__ void mlp_stats_kernel(const float* __restrict__ feat, const float* __
   }
 }
 
+// Particle index of slot f of the concatenated buckets: the last bucket e
+// with pref[e] <= f (pref: exclusive prefix of the counts, all counts >= 1).
+__device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves, int nleaf,
+                                             int f) {
+  int lo = 0, hi = nleaf - 1;
+#pragma unroll
+  for (int it = 0; it < 6; ++it) {  // nleaf <= 64
+    const int mid = (lo + hi + 1) >> 1;
+    if (lo < hi) {
+      if (pref[mid] <= f) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+  }
+  return leaves[lo].x + (f - pref[lo]);
+}
+
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
@@ -1522,15 +1541,18 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // shared-memory stack and test them IN PARALLEL: a node is accepted when every
 // target's own reference test (2h)^2 < theta^2 d^2 holds (d to the cell's
 // centre of mass) — first tried in one shot against the group's bounding box
-// (if the box's nearest point passes, every target does), else for each such
-// node in turn by the 32 lanes testing their own targets at once — so the
-// accepted cells are exactly those of the stackless walk.  Buckets that must be summed exactly and accepted cells are
-// appended to two lists; whenever 32 have gathered, the buckets' particles and
-// (monopole walk) the cells' centres of mass are copied with parallel loads
-// into a 64-source shared tile that every lane evaluates on its own target
-// with paired f32x2 arithmetic.  Quadrupole and corrected cells are evaluated
-// from their own staged list.  A warp whose stack would overflow restarts
-// with the stackless walk.
+// (if the box's nearest point passes, every target does), then against the
+// lane's own target (fails: opened), else for each remaining node in turn by
+// the 32 lanes testing their own targets at once — so the accepted cells are
+// exactly those of the stackless walk.  An accepted monopole cell is written,
+// from the registers of the lane that tested it, straight into a 64-source
+// shared tile that every lane evaluates on its own target with paired f32x2
+// arithmetic whenever it is full.  Buckets that must be summed exactly are
+// listed (first particle, count); whenever 32 have gathered, their particles
+// are gathered into the same tile, one slot per lane located by binary search
+// over the counts' prefix sums, so all loads of a tile are in flight together.
+// Quadrupole cells are listed and staged with their moments into a QuadTile.
+// A warp whose stack would overflow restarts with the stackless walk.
 //
 // CORR: the learned far-field correction.  At every cell flush the gathered
 // cells' features are taken at the group centre, standardised, and pushed
@@ -1548,9 +1570,10 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
     float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
-  __shared__ int s_cells[kListThreads / 32][kListCap];
+  __shared__ int s_cells[kListThreads / 32][CORR || ORDER == 2 ? kListCap : 1];
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
+  __shared__ int s_pref[kListThreads / 32][kListCap];     // exclusive prefix of the counts
   __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
   __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
   __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
@@ -1664,9 +1687,39 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
       unsigned m = __ballot_sync(kFull, is_leaf);
       if (is_leaf) leaves[nleaf + __popc(m & lt)] = make_int2(info.y, info.z);
       nleaf += __popc(m);
+      {  // targets whose own particle is in one of these buckets: one term fewer
+        unsigned own = 0u;
+        if (is_leaf) {
+          const int lo = max(info.y - warp * 32, 0), hi = min(info.y + info.z - warp * 32, 32);
+          if (hi > lo) own = (hi >= 32 ? kFull : (1u << hi) - 1u) & ~((1u << lo) - 1u);
+        }
+        own = __reduce_or_sync(kFull, own);
+        if (active && ((own >> lane) & 1u)) exact -= 1u;
+      }
       m = __ballot_sync(kFull, accept);
-      if (accept) cells[ncell + __popc(m & lt)] = node;
-      ncell += __popc(m);
+      if (ORDER == 1) {
+        // A monopole cell is a point mass at its centre of mass, already in
+        // this lane's registers from the opening test: it goes straight into
+        // the source tile (evaluated whenever 64 sources have gathered).  The
+        // corrected walk also lists the cell for its network evaluation.
+        if (CORR && accept) cells[ncell + __popc(m & lt)] = node;
+        if (CORR) ncell += __popc(m);
+        const int nacc = __popc(m), rank = __popc(m & lt), room = kStage - staged;
+        if (accept && rank < room) stage_source(src, staged + rank, c);
+        if (nacc >= room) {
+          __syncwarp();
+          source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
+          __syncwarp();
+          if (accept && rank >= room) stage_source(src, rank - room, c);
+          staged = nacc - room;
+        } else {
+          staged += nacc;
+        }
+        approx += active ? (unsigned)nacc : 0u;
+      } else {  // quadrupole cells: listed, staged with their moments at the flush
+        if (accept) cells[ncell + __popc(m & lt)] = node;
+        ncell += __popc(m);
+      }
       int incl = kids;
       for (int off = 1; off < 32; off <<= 1) {
         const int v = __shfl_up_sync(kFull, incl, off);
@@ -1776,47 +1829,44 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
       approx += active ? (unsigned)ncell : 0u;
       ncell = 0;
     }
-    if (ORDER == 1 && flush_cells) {
-      // a monopole cell is a point mass at its centre of mass: it joins the tile
-      for (int r0 = 0; r0 < ncell;) {
-        const int take = min(ncell - r0, kStage - staged);
-        for (int k = lane; k < take; k += 32) stage_source(src, staged + k, t.com[cells[r0 + k]]);
+    if (CORR && flush_cells) ncell = 0;  // monopoles already staged, corrections applied
+    if (nleaf >= 32 || (drain && nleaf > 0)) {
+      // The buckets' particles, concatenated, fill the tile: each lane finds
+      // the bucket of its slot by binary search over the exclusive prefix of
+      // the counts and loads its particles, all loads of a tile in flight at
+      // once.  The target's own particle adds exactly 0 (d = 0).
+      int* pref = s_pref[wib];
+      const int c0 = lane < nleaf ? leaves[lane].y : 0;
+      const int c1 = lane + 32 < nleaf ? leaves[lane + 32].y : 0;
+      int i0 = c0, i1 = c1;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v0 = __shfl_up_sync(kFull, i0, off), v1 = __shfl_up_sync(kFull, i1, off);
+        if (lane >= off) {
+          i0 += v0;
+          i1 += v1;
+        }
+      }
+      i1 += __shfl_sync(kFull, i0, 31);
+      const int total_src = __shfl_sync(kFull, i1, 31);
+      if (lane < nleaf) pref[lane] = i0 - c0;
+      if (lane + 32 < nleaf) pref[lane + 32] = i1 - c1;
+      __syncwarp();
+      exact += active ? (unsigned)total_src : 0u;  // own particles were taken off above
+      for (int f0 = 0; f0 < total_src;) {
+        const int take = min(total_src - f0, kStage - staged);
+        const bool h0 = lane < take, h1 = lane + 32 < take;
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0;
+        if (h0) q0 = pos[bucket_source(pref, leaves, nleaf, f0 + lane)];
+        if (h1) q1 = pos[bucket_source(pref, leaves, nleaf, f0 + lane + 32)];
+        if (h0) stage_source(src, staged + lane, q0);
+        if (h1) stage_source(src, staged + lane + 32, q1);
         staged += take;
-        r0 += take;
+        f0 += take;
         if (staged == kStage) {
           __syncwarp();
           source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
           staged = 0;
           __syncwarp();
-        }
-      }
-      approx += active ? (unsigned)ncell : 0u;
-      ncell = 0;
-    }
-    if (nleaf >= 32 || (drain && nleaf > 0)) {
-      // Copy the buckets' particles into the tile with parallel loads.  The
-      // target itself contributes exactly 0 (d = 0; eps = 0 is guarded there).
-      int e = 0;
-      while (e < nleaf) {  // consecutive buckets often abut: merge their particle ranges
-        const int2 first = leaves[e++];
-        const int b = first.x;
-        int end = first.x + first.y;
-        while (e < nleaf && leaves[e].x == end) {
-          end += leaves[e].y;
-          ++e;
-        }
-        exact += active ? (unsigned)(end - b - ((s >= b && s < end) ? 1 : 0)) : 0u;
-        for (int j0 = b; j0 < end;) {
-          const int take = min(end - j0, kStage - staged);
-          for (int k = lane; k < take; k += 32) stage_source(src, staged + k, pos[j0 + k]);
-          staged += take;
-          j0 += take;
-          if (staged == kStage) {
-            __syncwarp();
-            source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
-            staged = 0;
-            __syncwarp();
-          }
         }
       }
       nleaf = 0;
