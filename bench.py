@@ -75,7 +75,7 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.8, 0.9, 1.0)
 # capture of exactly this configuration (the file under profiles/ gives the command).
 PROFILED_TRAFFIC = {
     ("bh_collision_1m", 0.7, 1, "lists", 16): (
-        29_660_928, "profiles/walk_lists_kernel_bh_collision_1m.md"),
+        29_787_392, "profiles/walk_lists_kernel_bh_collision_1m.md"),
     ("allpairs_plummer_16k", None, 1, "lists", 16): (
         273_152, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
 }
