@@ -209,10 +209,17 @@ __global__ void __launch_bounds__(256) keys_kernel(
       index[i] = (uint32_t)i;
     }
 #pragma unroll
-    for (int p = 0; p < kSortPasses; ++p) {  // warp-aggregated digit counts
-      const unsigned d = valid ? (unsigned)(key >> (8 * p)) & 0xffu : 0x100u;
-      const unsigned peers = __match_any_sync(kFull, d);
-      if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    // digit counts: the low six bytes of the keys of one warp are spread over
+    // many values (plain shared atomics); the top two bytes (the first octree
+    // levels) repeat, so they are aggregated per warp first
+    for (int p = 0; p < kSortPasses; ++p) {
+      if (p < 6) {
+        if (valid) atomicAdd(&h[p][(unsigned)(key >> (8 * p)) & 0xffu], 1u);
+      } else {
+        const unsigned d = valid ? (unsigned)(key >> (8 * p)) & 0xffu : 0x100u;
+        const unsigned peers = __match_any_sync(kFull, d);
+        if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+      }
     }
   }
   __syncthreads();

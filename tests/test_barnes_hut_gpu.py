@@ -188,3 +188,29 @@ def test_barnes_hut_kdk_steps(cuda, ctx, walk):
     ctx.download(s)
     assert O.rms_relative_error(s.acc(), q.acc()) < 5e-3
     assert np.max(np.abs(s.x - q.x)) < 1e-7
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_zero_softening_is_finite_and_accurate(cuda, ctx, walk, order):
+    """simd_equivalence_test.c:160-196 for the tree: eps = 0, the staged tiles
+    drop each target's own r^2 = 0 term instead of dividing by zero."""
+    p = O.preset("random_cloud", 3000, 7)
+    ref = O.gravity_reference(p.copy(), 1.0, 0.0)
+    cpu, _ = O.barnes_hut(p.copy(), 1.0, 0.0, 0.5)
+    a, st = bh(cuda, p, 0.0, 0.5, ctx, order=order, walk=walk)
+    assert np.all(np.isfinite(a))
+    e_gpu, e_cpu = O.rms_relative_error(a, ref), O.rms_relative_error(cpu, ref)
+    print(f"eps=0 order={order} gpu={e_gpu:.3e} cpu={e_cpu:.3e}")
+    assert e_gpu <= e_cpu + 1e-6 and e_gpu < 1e-2
+
+
+def test_heavy_masses_take_the_guarded_tiles(cuda, ctx, walk):
+    """m / eps^3 beyond FP32 range (1e30 x 1e12): the self term cannot be
+    W * 0, so the guarded tile loop runs; forces stay finite and scale with m."""
+    p = O.preset("random_cloud", 2000, 3)
+    light, _ = bh(cuda, p, 1e-4, 0.5, ctx, walk=walk)
+    q = p.copy()
+    q.m *= 1e30
+    heavy, _ = bh(cuda, q, 1e-4, 0.5, ctx, walk=walk)
+    assert np.all(np.isfinite(heavy))
+    assert O.rms_relative_error(heavy / 1e30, light) < 1e-5

@@ -87,6 +87,20 @@ def test_ensemble_many_tiny_systems(cuda):
     check(cuda, out, offsets, expected, span=5e-3)
 
 
+def test_ensemble_zero_softening(cuda):
+    """eps = 0: the guarded kernel drops each target's own r^2 = 0 pair."""
+    members, s, offsets = make_ensemble(cuda, sizes_seed=3, count=12, lo=32, hi=200)
+    g = cuda.gravity_init(1.0, 0.0)
+    expected = oracle_run(members, 0.0, 1e-4, 3)
+    with cuda.CudaEnsemble() as e:
+        e.upload(s, offsets)
+        e.advance(g, 1e-4, 3)
+        out = cuda.ParticleSystem.zeros(s.n)
+        e.download(out)
+    assert all(np.all(np.isfinite(getattr(out, f))) for f in O.FIELDS)
+    check(cuda, out, offsets, expected, span=3e-4)
+
+
 def test_ensemble_repeated_advance_and_graph_reuse(cuda):
     members, s, offsets = make_ensemble(cuda, count=24)
     g = cuda.gravity_init(1.0, 0.01)
