@@ -1251,6 +1251,59 @@ __device__ __forceinline__ void quad_tile(const QuadTile& s, float4 p, float eps
   fold(hz, lz, v);
 }
 
+// Corrections of the learned walk: per cell its centre of mass and Y = M y
+// (the network's residual in units of M / |d|^2), pair-interleaved.
+struct CorrTile {
+  ulonglong2 xy[kStage / 2];  // {x}, {y}
+  ulonglong2 zu[kStage / 2];  // {z}, {Yx}
+  ulonglong2 vw[kStage / 2];  // {Yy}, {Yz}
+};
+
+__device__ __forceinline__ void stage_correction(CorrTile& s, int k, float4 c, float yx, float yy,
+                                                 float yz) {
+  const int i = k >> 1, o = k & 1;
+  float* a = reinterpret_cast<float*>(&s.xy[i]) + o;
+  float* b = reinterpret_cast<float*>(&s.zu[i]) + o;
+  float* e = reinterpret_cast<float*>(&s.vw[i]) + o;
+  a[0] = c.x;
+  a[2] = c.y;
+  b[0] = c.z;
+  b[2] = yx;
+  e[0] = yy;
+  e[2] = yz;
+}
+
+// a += Y / |d|^2 for the kStage corrections of a CorrTile (d = com - target,
+// unsoftened: accepted cells have |d| > 2h / theta > 0); far padding adds 0.
+__device__ __forceinline__ void corr_tile(const CorrTile& s, float4 p, float& hx, float& hy,
+                                          float& hz, float& lx, float& ly, float& lz) {
+  const unsigned long long PX = pack2(p.x, p.x), PY = pack2(p.y, p.y), PZ = pack2(p.z, p.z);
+  unsigned long long ax = 0ull, ay = 0ull, az = 0ull;
+#pragma unroll 8
+  for (int j = 0; j < kStage / 2; ++j) {
+    const ulonglong2 a = s.xy[j], b = s.zu[j], e = s.vw[j];
+    const unsigned long long dx = sub2(a.x, PX), dy = sub2(a.y, PY), dz = sub2(b.x, PZ);
+    const unsigned long long d2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    float d2a, d2b;
+    unpack2(d2, d2a, d2b);
+    const unsigned long long R = pack2(rsqrt_mufu(d2a), rsqrt_mufu(d2b));
+    const unsigned long long R2 = mul2(R, R);
+    ax = fma2(R2, b.y, ax);
+    ay = fma2(R2, e.x, ay);
+    az = fma2(R2, e.y, az);
+  }
+  float u, v;
+  unpack2(ax, u, v);
+  fold(hx, lx, u);
+  fold(hx, lx, v);
+  unpack2(ay, u, v);
+  fold(hy, ly, u);
+  fold(hy, ly, v);
+  unpack2(az, u, v);
+  fold(hz, lz, u);
+  fold(hz, lz, v);
+}
+
 // True when the target's own term in source_terms is W * 0 with W finite:
 // eps^2 a normal number and m * rsqrt(eps^2)^3, in the same operation order,
 // below overflow.
@@ -1589,7 +1642,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
   static_assert(!(CORR && ORDER == 2), "the network corrects the monopole");
   __shared__ __align__(16) SourceTile s_src[kListThreads / 32];
   __shared__ __align__(16) QuadTile s_quad[ORDER == 2 ? kListThreads / 32 : 1];
-  __shared__ float4 s_cc[kListThreads / 32][CORR ? kListCap : 1];
+  __shared__ __align__(16) CorrTile s_corr[CORR ? kListThreads / 32 : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   SourceTile& src = s_src[wib];
   int staged = 0;   // sources waiting in src (warp-uniform)
@@ -1748,8 +1801,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
     const bool drain = top == 0;
     const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
     if (CORR && flush_cells) {
-      float px = 0.f, py = 0.f, pz = 0.f;
-      if (CORR) {
+      {
         uint32_t* xs = s_x[wib];
         float* ys = s_y[wib];
         int* oks = s_ok[wib];
@@ -1796,25 +1848,30 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
         }
         __syncwarp();
       }
-      // stage the cells' data with parallel loads, then one dense loop
-      float4* cc = s_cc[wib];
-      for (int r = lane; r < ncell; r += 32) cc[r] = t.com[cells[r]];
-      __syncwarp();
-      for (int e = 0; e < ncell; ++e) {
-        const float4 c = cc[e];
-        if (s_ok[wib][e]) {
-          const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
-          const float scale = c.w / fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const float* ye = &s_y[wib][e * 4];
-          px = fmaf(scale, fmaf(ye[0], net->y_std[0], net->y_mean[0]), px);
-          py = fmaf(scale, fmaf(ye[1], net->y_std[1], net->y_mean[1]), py);
-          pz = fmaf(scale, fmaf(ye[2], net->y_std[2], net->y_mean[2]), pz);
+      // Each cell becomes a correction source (centre of mass, Y = M y, or
+      // Y = 0 out of range) in a CorrTile, padded with far zero sources;
+      // every lane adds Y / |d|^2 for its own target, two cells per
+      // instruction.
+      CorrTile& ct = s_corr[CORR ? wib : 0];
+      const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
+      const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
+      for (int r = lane; r < kStage; r += 32) {
+        float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
+        float yx = 0.f, yy = 0.f, yz = 0.f;
+        if (r < ncell) {
+          c = t.com[cells[r]];
+          if (s_ok[wib][r]) {
+            const float* ye = &s_y[wib][r * 4];
+            yx = c.w * fmaf(ye[0], ys0, ym0);
+            yy = c.w * fmaf(ye[1], ys1, ym1);
+            yz = c.w * fmaf(ye[2], ys2, ym2);
+          }
         }
+        stage_correction(ct, r, c, yx, yy, yz);
       }
       __syncwarp();
-      fold(hx, lx, px);
-      fold(hy, ly, py);
-      fold(hz, lz, pz);
+      corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
+      __syncwarp();
     }
     if (ORDER == 2 && flush_cells) {
       QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
