@@ -413,9 +413,14 @@ def run_ours(args, wl, world, rank, local):
         matched = matched_study(nb, torch, wl, system, g, min(args.steps, 5), 3, flush,
                                 with_correction=wl.get("correction", False))
     value = world * n * args.steps / (total_ms * 1e-3)
+    split = None
+    if wl["algorithm"] == "barnes_hut":  # particle-cell and particle-particle terms apart
+        per_s = world * args.steps / (total_ms * 1e-3)
+        split = {"particle_cell_per_s": approx * per_s, "particle_particle_per_s": exact * per_s}
     return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
                 roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
                 interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
+                interactions_split=split,
                 stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms, phases),
                 matched=matched, stages=stages)
 
@@ -715,6 +720,8 @@ def main(argv=None):
             line["matched_accuracy"] = r["matched"]
         if r.get("stages") is not None:
             line["stages_hbm"] = r["stages"]
+        if r.get("interactions_split") is not None:
+            line["interactions_split"] = r["interactions_split"]
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
