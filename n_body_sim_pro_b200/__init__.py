@@ -481,6 +481,17 @@ class CudaContext:
         v = system.view()
         _check(library().n_body_sim_pro_cuda_download(self.handle, C.byref(v), C.byref(err)), err)
 
+    def download_accelerations(self) -> np.ndarray:
+        """Only the resident accelerations, (n, 3) float64 (the view's other
+        arrays are NULL, which download skips)."""
+        out = np.zeros((3, self.n), dtype=np.float64)
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        null = C.POINTER(C.c_double)()
+        v = View(self.n, null, null, null, null, null, null, p(out[0]), p(out[1]), p(out[2]), null)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_download(self.handle, C.byref(v), C.byref(err)), err)
+        return out.T.copy()
+
     def compute_acceleration(self, gravity: Gravity, algorithm: Algorithm) -> None:
         err = Error()
         _check(library().n_body_sim_pro_cuda_compute_acceleration(
