@@ -241,7 +241,10 @@ ForceKernel pick_paired(bool zero_softening) {
 
 ForceKernel select_kernel(NbspAllPairsShape s, bool zero_softening) {
   if (s.paired) {
+    if (s.block == 64 && s.per_thread == 4) return pick_paired<64, 4>(zero_softening);
     if (s.block == 64 && s.per_thread == 8) return pick_paired<64, 8>(zero_softening);
+    if (s.block == 128 && s.per_thread == 2) return pick_paired<128, 2>(zero_softening);
+    if (s.block == 256 && s.per_thread == 2) return pick_paired<256, 2>(zero_softening);
     if (s.block == 128 && s.per_thread == 4) return pick_paired<128, 4>(zero_softening);
     if (s.block == 128 && s.per_thread == 8) return pick_paired<128, 8>(zero_softening);
     if (s.block == 256 && s.per_thread == 4) return pick_paired<256, 4>(zero_softening);
