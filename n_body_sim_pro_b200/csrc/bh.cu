@@ -1699,22 +1699,23 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         node = -1;
       }
-      if (node >= 0) {
-        info = t.info[node];
-        c = t.com[node];
-        ro = t.ropen2[node];
-        if (info.z > 0 && (info.y < 0 || info.y + info.z > n)) {
-          atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-        } else if (info.z == 1) {  // a single particle is always exact
-          is_leaf = true;
-        } else {  // cells and buckets of >= 2 particles take the opening test
-          const float qx = fmaxf(fabsf(c.x - gx) - ex, 0.f);
-          const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
-          const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
-          const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
-          accept = dmin2 > ro;  // the whole box passes: every target passes
-          test = !accept;
-        }
+      {  // every lane loads a node (idle lanes the root) so no branch diverges
+        const bool valid = node >= 0;
+        const int at = valid ? node : 0;
+        info = t.info[at];
+        c = t.com[at];
+        ro = t.ropen2[at];
+        const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
+        if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        const bool ok = valid && !bad;
+        is_leaf = ok && info.z == 1;
+        const float qx = fmaxf(fabsf(c.x - gx) - ex, 0.f);
+        const float qy = fmaxf(fabsf(c.y - gy) - ey, 0.f);
+        const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
+        const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+        const bool cellish = ok && info.z != 1;
+        accept = cellish && dmin2 > ro;
+        test = cellish && !(dmin2 > ro);
       }
       // Nodes the box could not accept: a node that fails this lane's own
       // target is opened at once; for the rest every target's own test
@@ -1734,26 +1735,22 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
         const bool any = __any_sync(kFull, fail);
         if (lane == from) accept = !any;
       }
-      if ((test || opened) && !accept) {
-        if (info.z > 0) {
-          is_leaf = true;  // a failing bucket is summed exactly
-        } else {
-          ca = reinterpret_cast<const int4*>(t.children)[2 * node];
-          cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
-          kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) +
-                 (cb.y >= 0) + (cb.z >= 0) + (cb.w >= 0);
-        }
+      const bool open = (test || opened) && !accept;
+      is_leaf = is_leaf || (open && info.z > 0);  // a failing bucket is summed exactly
+      if (open && info.z == 0) {                   // an opened cell pushes its children
+        ca = reinterpret_cast<const int4*>(t.children)[2 * node];
+        cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
       }
+      kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) + (cb.y >= 0) +
+             (cb.z >= 0) + (cb.w >= 0);
       unsigned m = __ballot_sync(kFull, is_leaf);
       if (is_leaf) leaves[nleaf + __popc(m & lt)] = make_int2(info.y, info.z);
       nleaf += __popc(m);
       {  // targets whose own particle is in one of these buckets: one term fewer
-        unsigned own = 0u;
-        if (is_leaf) {
-          const int lo = max(info.y - warp * 32, 0), hi = min(info.y + info.z - warp * 32, 32);
-          if (hi > lo) own = (hi >= 32 ? kFull : (1u << hi) - 1u) & ~((1u << lo) - 1u);
-        }
-        own = __reduce_or_sync(kFull, own);
+        const int lo = max(info.y - warp * 32, 0), hi = min(info.y + info.z - warp * 32, 32);
+        const unsigned span = hi >= 32 ? kFull : (1u << max(hi, 0)) - 1u;
+        const unsigned own = __reduce_or_sync(
+            kFull, is_leaf && hi > lo ? span & ~((1u << min(lo, 31)) - 1u) : 0u);
         if (active && ((own >> lane) & 1u)) exact -= 1u;
       }
       m = __ballot_sync(kFull, accept);
