@@ -1611,7 +1611,7 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // listed (first particle, count); whenever 32 have gathered, their particles
 // are gathered into the same tile, one slot per lane located by binary search
 // over the counts' prefix sums, so all loads of a tile are in flight together.
-// Quadrupole cells are listed and staged with their moments into a QuadTile.
+// A quadrupole cell goes into a QuadTile with its moments when it is accepted.
 // A warp whose stack would overflow restarts with the stackless walk.
 //
 // CORR: the learned far-field correction.  At every cell flush the gathered
@@ -1630,7 +1630,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
     float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
-  __shared__ int s_cells[kListThreads / 32][CORR || ORDER == 2 ? kListCap : 1];
+  __shared__ int s_cells[kListThreads / 32][CORR ? kListCap : 1];
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
   __shared__ int s_pref[kListThreads / 32][kListCap];     // exclusive prefix of the counts
@@ -1773,9 +1773,26 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
           staged += nacc;
         }
         approx += active ? (unsigned)nacc : 0u;
-      } else {  // quadrupole cells: listed, staged with their moments at the flush
-        if (accept) cells[ncell + __popc(m & lt)] = node;
-        ncell += __popc(m);
+      } else {  // a quadrupole cell goes into the QuadTile with its moments
+        QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
+        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f);
+        float qyz = 0.f;
+        if (accept) {
+          qa = t.quad[2 * node];
+          qyz = t.quad[2 * node + 1].x;
+        }
+        const int nacc = __popc(m), rank = __popc(m & lt), room = kStage - qstaged;
+        if (accept && rank < room) stage_cell(qt, qstaged + rank, c, qa, qyz);
+        if (nacc >= room) {
+          __syncwarp();
+          quad_tile(qt, p, eps2, hx, hy, hz, lx, ly, lz);
+          __syncwarp();
+          if (accept && rank >= room) stage_cell(qt, rank - room, c, qa, qyz);
+          qstaged = nacc - room;
+        } else {
+          qstaged += nacc;
+        }
+        approx += active ? (unsigned)nacc : 0u;
       }
       int incl = kids;
       for (int off = 1; off < 32; off <<= 1) {
@@ -1869,26 +1886,6 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
       __syncwarp();
       corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
       __syncwarp();
-    }
-    if (ORDER == 2 && flush_cells) {
-      QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
-      for (int r0 = 0; r0 < ncell;) {
-        const int take = min(ncell - r0, kStage - qstaged);
-        for (int k = lane; k < take; k += 32) {
-          const int node = cells[r0 + k];
-          stage_cell(qt, qstaged + k, t.com[node], t.quad[2 * node], t.quad[2 * node + 1].x);
-        }
-        qstaged += take;
-        r0 += take;
-        if (qstaged == kStage) {
-          __syncwarp();
-          quad_tile(qt, p, eps2, hx, hy, hz, lx, ly, lz);
-          qstaged = 0;
-          __syncwarp();
-        }
-      }
-      approx += active ? (unsigned)ncell : 0u;
-      ncell = 0;
     }
     if (CORR && flush_cells) ncell = 0;  // monopoles already staged, corrections applied
     if (nleaf >= 32 || (drain && nleaf > 0)) {
