@@ -14,10 +14,12 @@ same collision at N = 10M).
 
 `matched_accuracy` (Barnes-Hut workloads, skipped with --no-matched): on the
 initial state, the rms relative force error against the FP64 direct sum on
-4096 seeded targets is measured over a theta grid for the plain monopole walk
-and for the chosen quadrupole walk; each is then timed at the largest theta
-whose error is at most 1e-3.  ``bh_matched_10m`` adds the plain walk at
-theta 0.5 and the learned correction at theta 1.0 (network trained on 2^22
+4096 seeded targets is measured over a theta grid for the monopole and the
+quadrupole walk under the reference's opening test and under the offset test;
+each method is then timed at the largest theta whose error is at most 1e-3.
+"plain" is the monopole walk with the reference's test, "chosen" the fastest
+method.  ``bh_matched_10m`` adds the plain walk at theta 0.5 and the learned
+correction at theta 1.0 under both opening tests (network trained on 2^22
 cell-target pairs of the 1M collision).
 
 Timing: W untimed warm-up steps; then K steps, each a 1-step device-resident
@@ -444,9 +446,10 @@ def rms_at_targets(nb, ctx, g, n, targets, ref):
     return float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
 
 
-def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None):
-    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order)."""
-    ctx = nb.CudaContext(theta=theta, multipole_order=order)
+def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None,
+                opening=0):
+    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order, opening)."""
+    ctx = nb.CudaContext(theta=theta, multipole_order=order, opening=opening)
     ctx.set_correction(correction)
     ctx.upload(system)
     for _ in range(warmup):
@@ -461,63 +464,82 @@ def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, co
     return wl["n"] * steps / (sum(ms) * 1e-3), float(np.mean(ms))
 
 
+OPENINGS = {"reference": 0, "offset": 1}
+
+
 def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
-    """Plain (monopole) vs chosen (quadrupole) Barnes-Hut, each at the largest
-    theta of THETA_GRID meeting RMS_TARGET, both timed; optionally the learned
-    correction at theta 1.0 (trained on 2^22 pairs of the 1M collision) and the
-    plain walk at theta 0.5."""
+    """Plain Barnes-Hut (monopole, the reference's opening test) vs the chosen
+    method — the fastest of {monopole, quadrupole} x {reference, offset opening
+    test} — each at the largest theta of THETA_GRID meeting RMS_TARGET, all
+    timed; optionally the learned correction at theta 1.0 (trained on 2^22
+    pairs of the 1M collision) under either opening test and the plain walk at
+    theta 0.5."""
     n = wl["n"]
     targets = np.random.default_rng(11).choice(n, min(4096, n), replace=False)
     ctx = nb.CudaContext(theta=0.5)
     ctx.upload(system)
     ref = ctx.reference_acceleration(g, targets)
     table = {}
-    for order in (1, 2):
-        ctx.set_multipole_order(order)
-        rows = []
-        for th in THETA_GRID:
-            ctx.theta = th
-            rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
-        table[order] = rows
+    for oname, opening in OPENINGS.items():
+        ctx.set_opening(opening)
+        for order in (1, 2):
+            ctx.set_multipole_order(order)
+            rows = []
+            for th in THETA_GRID:
+                ctx.theta = th
+                rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
+            table[(order, oname)] = rows
     ctx.close()
     out = {"rms_target": RMS_TARGET, "oracle": "FP64 device direct sum, 4096 seeded targets, "
-           "initial state", "sweep": {f"order{o}": [[t, round(r, 6)] for t, r in rows]
-                                     for o, rows in table.items()}}
-    for name, order in (("plain", 1), ("chosen", 2)):
-        ok = [t for t, r in table[order] if r <= RMS_TARGET]
+           "initial state",
+           "sweep": {f"order{o}_{on}": [[t, round(r, 6)] for t, r in rows]
+                     for (o, on), rows in table.items()}}
+    methods = {}
+    for (order, oname), rows in table.items():
+        ok = [t for t, r in rows if r <= RMS_TARGET]
         if not ok:
-            out[name] = None
             continue
         th = max(ok)
-        v, ms = timed_steps(nb, torch, system, g, wl, th, order, steps, warmup, flush)
-        out[name] = {"theta": th, "multipole_order": order,
-                     "rms": dict(table[order])[th], "value": v, "ms_per_step": round(ms, 4)}
+        v, ms = timed_steps(nb, torch, system, g, wl, th, order, steps, warmup, flush,
+                            opening=OPENINGS[oname])
+        methods[(order, oname)] = {"theta": th, "multipole_order": order, "opening": oname,
+                                   "rms": dict(rows)[th], "value": v,
+                                   "ms_per_step": round(ms, 4)}
+    out["methods"] = list(methods.values())
+    out["plain"] = methods.get((1, "reference"))
+    out["chosen"] = max(methods.values(), key=lambda m: m["value"]) if methods else None
     if out["plain"] and out["chosen"]:
         out["chosen_over_plain"] = round(out["chosen"]["value"] / out["plain"]["value"], 3)
     if with_correction:
         v, ms = timed_steps(nb, torch, system, g, wl, 0.5, 1, steps, warmup, flush)
-        out["plain_theta_0.5"] = {"theta": 0.5, "rms": dict(table[1])[0.5], "value": v,
-                                  "ms_per_step": round(ms, 4)}
+        out["plain_theta_0.5"] = {"theta": 0.5, "rms": dict(table[(1, "reference")])[0.5],
+                                  "value": v, "ms_per_step": round(ms, 4)}
         pos1, vel1, mass1 = initial_conditions("collision", 1_000_000, seed=42)
-        with nb.CudaContext(theta=1.0) as c1, nb.CudaCorrection(seed=11) as corr:
-            c1.upload(nb.ParticleSystem.from_arrays(pos1, vel1, mass1))
-            t0 = time.time()
-            corr.generate(c1, g, theta=1.0, samples=1 << 22, seed=3)
-            tl, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
-            train_s = time.time() - t0
-            cctx = nb.CudaContext(theta=1.0)
-            cctx.set_correction(corr)
-            cctx.upload(system)
-            rms_c = rms_at_targets(nb, cctx, g, n, targets, ref)
-            cctx.close()
-            v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush,
-                                correction=corr)
-        out["corrected_theta_1.0"] = {"theta": 1.0, "rms": rms_c, "value": v,
-                                      "ms_per_step": round(ms, 4),
-                                      "plain_rms_at_theta_1.0": dict(table[1])[1.0],
-                                      "training": {"pairs": 1 << 22, "from": "collision N=1M",
-                                                   "epochs": 8, "final_validation_loss":
-                                                   float(vl[-1]), "seconds": round(train_s, 2)}}
+        system1 = nb.ParticleSystem.from_arrays(pos1, vel1, mass1)
+        corrected = {}
+        for oname, opening in OPENINGS.items():
+            with nb.CudaContext(theta=1.0, opening=opening) as c1, \
+                    nb.CudaCorrection(seed=11) as corr:
+                c1.upload(system1)
+                t0 = time.time()
+                corr.generate(c1, g, theta=1.0, samples=1 << 22, seed=3)
+                tl, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
+                train_s = time.time() - t0
+                cctx = nb.CudaContext(theta=1.0, opening=opening)
+                cctx.set_correction(corr)
+                cctx.upload(system)
+                rms_c = rms_at_targets(nb, cctx, g, n, targets, ref)
+                cctx.close()
+                v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush,
+                                    correction=corr, opening=opening)
+            corrected[oname] = {
+                "theta": 1.0, "opening": oname, "rms": rms_c, "value": v,
+                "ms_per_step": round(ms, 4),
+                "uncorrected_rms_at_theta_1.0": dict(table[(1, oname)])[1.0],
+                "training": {"pairs": 1 << 22, "from": "collision N=1M", "epochs": 8,
+                             "final_validation_loss": float(vl[-1]),
+                             "seconds": round(train_s, 2)}}
+        out["corrected_theta_1.0"] = corrected
     return out
 
 

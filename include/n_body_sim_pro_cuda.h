@@ -247,6 +247,21 @@ typedef enum NBodySimProCudaWalk {
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(
     NBodySimProCudaContext* context, int walk, NBodySimProError* error);
 
+/* Opening test of the Barnes-Hut walk (a target-cell pair at distance d from the
+ * cell's centre of mass, cell side 2h):
+ *   REFERENCE  accept when (2h)^2 < theta^2 d^2 (barnes_hut.c:596-599; default);
+ *   OFFSET     accept when 2h / theta + shift < d, shift = the distance from the
+ *              cell's geometric centre to its centre of mass (Barnes 1994), so no
+ *              target inside the cell accepts it at any theta <= 1.
+ * Every cell OFFSET accepts, REFERENCE accepts too. */
+typedef enum NBodySimProCudaOpening {
+    N_BODY_SIM_PRO_CUDA_OPENING_REFERENCE = 0,
+    N_BODY_SIM_PRO_CUDA_OPENING_OFFSET = 1
+} NBodySimProCudaOpening;
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_opening(
+    NBodySimProCudaContext* context, int opening, NBodySimProError* error);
+
 /* Replaces n_body_sim_pro_barnes_hut_tree_stats (barnes_hut/barnes_hut.h:116-117):
  * 0 on success, non-zero when an argument is NULL. */
 N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_stats(

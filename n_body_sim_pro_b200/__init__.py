@@ -55,6 +55,12 @@ class Algorithm(IntEnum):
     BARNES_HUT = 1
 
 
+class Opening(IntEnum):
+    """NBodySimProCudaOpening: the Barnes-Hut opening test."""
+    REFERENCE = 0
+    OFFSET = 1
+
+
 class View(C.Structure):
     """NBodySimProParticleSystemView (include/n_body_sim_pro/core/particle_system.h:38-50)."""
 
@@ -169,7 +175,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
     "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
-    "n_body_sim_pro_cuda_checkpoint_read",
+    "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
 )
 
 # NBodySimProSimulationPreset (generation/presets.h:27-38)
@@ -213,6 +219,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_set_multipole_order": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_leaf_capacity": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_walk": (st, [vp, C.c_int, pe]),
+        "n_body_sim_pro_cuda_context_set_opening": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
@@ -366,7 +373,7 @@ class CudaContext:
     """NBodySimProCudaContext: device-resident state, stepping and diagnostics."""
 
     def __init__(self, theta: float | None = None, multipole_order: int | None = None,
-                 leaf_capacity: int | None = None):
+                 leaf_capacity: int | None = None, opening: int | None = None):
         L = library()
         err = Error()
         h = L.n_body_sim_pro_cuda_context_create(C.byref(err))
@@ -381,6 +388,8 @@ class CudaContext:
             self.set_multipole_order(multipole_order)
         if leaf_capacity is not None:
             self.set_leaf_capacity(leaf_capacity)
+        if opening is not None:
+            self.set_opening(opening)
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -417,6 +426,13 @@ class CudaContext:
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_walk(self.handle, int(walk),
                                                               C.byref(err)), err)
+
+    def set_opening(self, opening: int) -> None:
+        """Opening.REFERENCE: (2h)^2 < theta^2 d^2 (default); Opening.OFFSET:
+        2h / theta + shift < d with shift the cell's centre-of-mass offset."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_opening(self.handle, int(opening),
+                                                                 C.byref(err)), err)
 
     def set_correction(self, correction: "CudaCorrection | None") -> None:
         err = Error()

@@ -42,6 +42,11 @@ __device__ __forceinline__ void fold(float& hi, float& lo, float a) {
   lo = __fadd_rn(lo, err);
 }
 
+// Source chunks start and end on multiples of kChunkAlign sources, so a chunk's
+// last tile may be partial; the packed array is padded to a multiple of 256
+// with massless sources.
+constexpr int kChunkAlign = NBSP_ALLPAIRS_CHUNK_ALIGN;
+
 template <int BLOCK, int K, bool ZERO_SOFTENING>
 __global__ void __launch_bounds__(BLOCK) allpairs_force_kernel(
     const float4* __restrict__ packed, int n, int n_padded, int chunk_len, float eps2,
@@ -66,16 +71,18 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_kernel(
 
   const int j0 = blockIdx.y * chunk_len;
   const int j1 = min(j0 + chunk_len, n_padded);
-  float4 next = j0 < j1 ? packed[j0 + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 next = j0 + tid < j1 ? packed[j0 + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int jt = j0; jt < j1; jt += BLOCK) {
     __syncthreads();
     tile[tid] = next;
     __syncthreads();
-    if (jt + BLOCK < j1) next = packed[jt + BLOCK + tid];
+    next = jt + BLOCK + tid < j1 ? packed[jt + BLOCK + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < K; ++k) ax[k] = ay[k] = az[k] = 0.f;
-#pragma unroll 8
-    for (int j = 0; j < BLOCK; ++j) {
+    const int count = min(BLOCK, j1 - jt);  // a multiple of kChunkAlign
+    for (int j8 = 0; j8 < count; j8 += kChunkAlign)
+#pragma unroll
+    for (int j = j8; j < j8 + kChunkAlign; ++j) {
       const float4 s = tile[j];
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -165,17 +172,19 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
 
   const int j0 = blockIdx.y * chunk_len;
   const int j1 = min(j0 + chunk_len, n_padded);
-  float4 next = j0 < j1 ? packed[j0 + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 next = j0 + tid < j1 ? packed[j0 + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int jt = j0; jt < j1; jt += BLOCK) {
     __syncthreads();
     tile[tid] = next;
     __syncthreads();
-    if (jt + BLOCK < j1) next = packed[jt + BLOCK + tid];
+    next = jt + BLOCK + tid < j1 ? packed[jt + BLOCK + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
     unsigned long long AX[P], AY[P], AZ[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) AX[p] = AY[p] = AZ[p] = 0ull;
-#pragma unroll 8
-    for (int j = 0; j < BLOCK; ++j) {
+    const int count = min(BLOCK, j1 - jt);  // a multiple of kChunkAlign
+    for (int j8 = 0; j8 < count; j8 += kChunkAlign)
+#pragma unroll
+    for (int j = j8; j < j8 + kChunkAlign; ++j) {
       const float4 s = tile[j];
       const unsigned long long SX = pack2(s.x, s.x), SY = pack2(s.y, s.y), SZ = pack2(s.z, s.z);
       const unsigned long long SW = pack2(s.w, s.w);
@@ -636,9 +645,7 @@ void nbsp_allpairs_force(const void* packed, size_t n, size_t n_padded, float so
                          cudaStream_t stream) {
   ForceKernel k = select_kernel(shape, softening_squared == 0.f);
   const int targets_per_cta = shape.block * shape.per_thread;
-  const int tiles = (int)(n_padded / shape.block);
-  const int tiles_per_chunk = (tiles + shape.chunks - 1) / shape.chunks;
-  const int chunk_len = tiles_per_chunk * shape.block;
+  const int chunk_len = (int)nbsp_allpairs_chunk_len(n_padded, shape.chunks);
   dim3 grid((unsigned)((n + targets_per_cta - 1) / targets_per_cta), (unsigned)shape.chunks);
   NBSP_COUNT_LAUNCH(1), k<<<grid, shape.block, 0, stream>>>((const float4*)packed, (int)n, (int)n_padded, chunk_len,
                                       softening_squared, (float4*)partial_hi,

@@ -103,6 +103,7 @@ struct NBodySimProCudaContext {
     int multipole_order;
     int leaf_capacity;
     int walk_mode;
+    int opening;
     const void* correction; /* device network of the learned correction, or NULL */
     NbspBarnesHut* bh;
     int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
@@ -145,6 +146,7 @@ NBodySimProCudaContext* n_body_sim_pro_cuda_context_create(NBodySimProError* err
     c->multipole_order = 1;
     c->leaf_capacity = 16;
     c->walk_mode = NBSP_BH_WALK_LISTS;
+    c->opening = NBSP_BH_OPENING_REFERENCE;
     const char* tune = getenv("NBSP_AUTOTUNE");
     c->autotune = !(tune != NULL && tune[0] == '0');
     struct cudaDeviceProp prop;
@@ -230,6 +232,16 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(NBodySimProCudaContext* c
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown Barnes-Hut walk");
     c->walk_mode = walk == N_BODY_SIM_PRO_CUDA_WALK_STACKLESS ? NBSP_BH_WALK_STACKLESS
                                                               : NBSP_BH_WALK_LISTS;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_opening(NBodySimProCudaContext* c, int opening,
+                                                          NBodySimProError* error) {
+    if (c == NULL || (opening != N_BODY_SIM_PRO_CUDA_OPENING_REFERENCE &&
+                      opening != N_BODY_SIM_PRO_CUDA_OPENING_OFFSET))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown opening criterion");
+    c->opening = opening == N_BODY_SIM_PRO_CUDA_OPENING_OFFSET ? NBSP_BH_OPENING_OFFSET
+                                                              : NBSP_BH_OPENING_REFERENCE;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
@@ -351,7 +363,9 @@ static const NbspAllPairsShape kShapes[] = {
     {256, 4, 1, 1}, {64, 4, 1, 1},  {128, 2, 1, 1}, {256, 2, 1, 1},
 };
 
-/* Source chunks so that (target blocks x chunks) fills whole waves of resident CTAs. */
+/* Source chunks so that (target blocks x chunks) fills whole waves of resident
+ * CTAs: the busiest CTA slot's sources (chunks end on 8-source boundaries) against
+ * the average, less a small cost per chunk (one more partial per target). */
 static NbspAllPairsShape fit_chunks(const NBodySimProCudaContext* c, NbspAllPairsShape s,
                                     size_t n) {
     const size_t per_cta = (size_t)s.block * (size_t)s.per_thread;
@@ -359,17 +373,16 @@ static NbspAllPairsShape fit_chunks(const NBodySimProCudaContext* c, NbspAllPair
     int resident = nbsp_allpairs_resident_ctas(s);
     if (resident < 1) resident = 1;
     const size_t slots = (size_t)c->sm_count * (size_t)resident;
-    const size_t tiles = round_up(n, 256) / (size_t)s.block;
+    const size_t n_padded = round_up(n, 256);
     size_t best_chunks = 1;
     double best_eff = 0.0;
-    for (size_t chunks = 1; chunks <= 64 && chunks <= tiles; ++chunks) {
-        const size_t tiles_per_chunk = (tiles + chunks - 1) / chunks;
-        if (chunks > 1 && tiles_per_chunk < 2) break;
+    for (size_t chunks = 1; chunks <= 64; ++chunks) {
+        const size_t len = nbsp_allpairs_chunk_len(n_padded, (int)chunks);
+        if (chunks > 1 && len < 2 * (size_t)s.block) break;
         const size_t ctas = target_blocks * chunks;
         const size_t waves = (ctas + slots - 1) / slots;
-        /* useful work / work the busiest SM slot does, minus a small cost per chunk */
-        const double work = (double)target_blocks * (double)tiles;
-        const double span = (double)waves * (double)tiles_per_chunk * (double)slots;
+        const double work = (double)target_blocks * (double)n_padded;
+        const double span = (double)waves * (double)len * (double)slots;
         const double eff = work / span - 0.002 * (double)chunks;
         if (eff > best_eff + 1e-9) {
             best_eff = eff;
@@ -468,6 +481,7 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.multipole_order = c->multipole_order;
         p.leaf_capacity = c->leaf_capacity;
         p.walk_mode = c->walk_mode;
+        p.opening = c->opening;
         p.correction = c->correction;
         NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
         c->bh_pending = 1;
@@ -923,6 +937,7 @@ NBodySimProStatus nbsp_context_tree(NBodySimProCudaContext* c, const NBodySimPro
     out->n = c->n;
     out->stream = c->stream;
     out->status = c->status;
+    out->opening = c->opening;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 

@@ -474,6 +474,7 @@ struct Tree {
   double* trace64;    // sum m |x - com|^2 per node (FP64)
   float* side;        // cell side 2h = root side / 2^level
   float* spread;      // sum m |x - com|^2 / (M side^2): the correction MLP's 10th feature
+  float* shift;       // distance from the cell's geometric centre to its centre of mass
   unsigned long long* leaves;  // [1]
 };
 
@@ -516,6 +517,7 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.trace64 = carve<double>(p, nb);
   t.side = carve<float>(p, nb);
   t.spread = carve<float>(p, nb);
+  t.shift = carve<float>(p, nb);
   t.leaves = carve<unsigned long long>(p, 1);
   if (end != nullptr) *end = p;
   return t;
@@ -752,17 +754,52 @@ struct Moments {
   double t2;    // sum m |x - com|^2
 };
 
-__device__ void finish_node(const Tree& t, int node, const Moments& mo, double root_size,
-                            double inv_theta2, int lvl) {
+// Inverse of spread3: bits 0, 3, 6, ... of v gathered into the low 21 bits.
+__device__ __forceinline__ uint32_t compact3(uint64_t v) {
+  v &= 0x1249249249249249ull;
+  v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ull;
+  v = (v ^ (v >> 4)) & 0x100f00f00f00f00full;
+  v = (v ^ (v >> 8)) & 0x001f0000ff0000ffull;
+  v = (v ^ (v >> 16)) & 0x001f00000000ffffull;
+  v = (v ^ (v >> 32)) & 0x1fffffull;
+  return (uint32_t)v;
+}
+
+// What the opening test of every node is built from.
+struct Opening {
+  const uint64_t* keys;  // sorted Morton keys (a node's first key names its cell)
+  const double* geometry;
+  double inv_theta, inv_theta2;
+  int criterion;         // NBSP_BH_OPENING_*
+};
+
+__device__ void finish_node(const Tree& t, int node, const Moments& mo, int first, int lvl,
+                            const Opening& o) {
   t.mom[node] = make_double4(mo.m, mo.cx, mo.cy, mo.cz);
   for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
   t.trace64[node] = mo.t2;
   t.com[node] = make_float4((float)mo.cx, (float)mo.cy, (float)mo.cz, (float)mo.m);
-  // cell side 2h = root side / 2^lvl ; accept when (2h)^2 < theta^2 d^2
-  const double side = ldexp(root_size, -min(lvl, 21));
-  const double r2 = side * side * inv_theta2;
+  // cell side 2h = root side / 2^lvl; the cell's centre from the first key's
+  // top 3 lvl bits, in the particles' frame (relative to the centre of mass)
+  const int l = min(lvl, 21);
+  const double half = o.geometry[3];
+  const double side = ldexp(2.0 * half, -l);
+  const uint64_t key = o.keys[first];
+  double shift2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double lo = o.geometry[a] - half - o.geometry[4 + a];
+    const double centre = lo + ((double)(compact3(key >> a) >> (21 - l)) + 0.5) * side;
+    const double d = (a == 0 ? mo.cx : a == 1 ? mo.cy : mo.cz) - centre;
+    shift2 += d * d;
+  }
+  const double shift = sqrt(shift2);
+  // reference: accept when (2h)^2 < theta^2 d^2; offset: when 2h / theta + shift < d
+  const double r2 = o.criterion == NBSP_BH_OPENING_OFFSET
+                        ? (side * o.inv_theta + shift) * (side * o.inv_theta + shift)
+                        : side * side * o.inv_theta2;
   t.ropen2[node] = (float)r2;
   t.side[node] = (float)side;
+  t.shift[node] = (float)shift;
   t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
   t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
   t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
@@ -787,10 +824,8 @@ __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
 // a fixed order and the result is deterministic, loads all of them at once and
 // writes the sorted list back for the interaction-list walk.
 __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
-                                                      const double* __restrict__ geometry,
-                                                      double inv_theta2, int* status) {
+                                                      Opening open, int* status) {
   const int total = (int)t.offset[t.n];
-  const double root_size = 2.0 * geometry[3];
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < total;
        node += gridDim.x * blockDim.x) {
     const int4 info = t.info[node];
@@ -831,7 +866,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
         mo.q[5] += w * (3.0 * dz * dz - r2);
       }
     }
-    finish_node(t, node, mo, root_size, inv_theta2, t.level[node]);
+    finish_node(t, node, mo, info.y, t.level[node], open);
     int parent = info.w;
     for (int climb = 0; parent >= 0; ++climb) {
       if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
@@ -922,7 +957,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
           make_int4(nc > 4 ? ch[4] : -1, nc > 5 ? ch[5] : -1, nc > 6 ? ch[6] : -1,
                     nc > 7 ? ch[7] : -1);
       t.height[parent] = hmax + 1;
-      finish_node(t, parent, pm, root_size, inv_theta2, __ldcg(&t.level[parent]));
+      finish_node(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open);
       parent = pinfo.w;
     }
   }
@@ -1382,11 +1417,11 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 constexpr float kCorrGroup = 0.3f;
 
 // Training pairs: sample k picks a random target and, walking the tree with the
-// reference criterion at theta_train, one of the cells that target accepts and
+// opening criterion at theta_train, one of the cells that target accepts and
 // its group would correct, uniformly (reservoir sampling).  Up to 8 targets
 // are tried per sample.
 __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, float theta,
-                                 unsigned long long seed, int samples, int* __restrict__ target,
+                                 int opening, unsigned long long seed, int samples, int* __restrict__ target,
                                  int* __restrict__ cell, int* status) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= samples) return;
@@ -1430,7 +1465,9 @@ __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, 
       const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float s = t.side[node];
-      if (d2 > 0.f && s * s < th2 * d2 && c.w > 0.f) {
+      const float ro = s / theta + t.shift[node];
+      const bool pass = opening == NBSP_BH_OPENING_OFFSET ? d2 > ro * ro : s * s < th2 * d2;
+      if (d2 > 0.f && pass && c.w > 0.f) {
         const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
         if (kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2) {
           ++count;
@@ -2064,16 +2101,20 @@ void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree
   NBSP_COUNT_LAUNCH(1), place_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
 }
 
-void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry, double theta, int order,
-                     void* tree, int* status, cudaStream_t stream) {
-  (void)order;
+void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const double* geometry,
+                     double theta, int opening, void* tree, int* status, cudaStream_t stream) {
   Tree t = tree_view(tree, n);
   const size_t nb = 2 * n - 1;
-  const double inv_theta2 = theta > 0.0 ? 1.0 / (theta * theta) : INFINITY;
+  Opening o;
+  o.keys = keys;
+  o.geometry = geometry;
+  o.inv_theta = theta > 0.0 ? 1.0 / theta : INFINITY;
+  o.inv_theta2 = theta > 0.0 ? 1.0 / (theta * theta) : INFINITY;
+  o.criterion = opening;
   size_t blocks = (nb + 255) / 256;  // grid-stride over the octree nodes (<= 2n - 1)
   if (blocks > 148 * 16) blocks = 148 * 16;
   NBSP_COUNT_LAUNCH(1), moments_kernel<<<(unsigned)blocks, 256, 0, stream>>>((const float4*)pos4, t,
-                                                                   geometry, inv_theta2, status);
+                                                                   o, status);
 }
 
 void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
@@ -2117,12 +2158,12 @@ void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* per
                                                        az);
 }
 
-void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta,
+void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta, int opening,
                        unsigned long long seed, int samples, int* target, int* cell, int* status,
                        cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   NBSP_COUNT_LAUNCH(1), mlp_pairs_kernel<<<(samples + 127) / 128, 128, 0, stream>>>(
-      (const float4*)pos4, (int)n, t, theta, seed, samples, target, cell, status);
+      (const float4*)pos4, (int)n, t, theta, opening, seed, samples, target, cell, status);
 }
 
 void nbsp_bh_mlp_labels(const void* pos4, size_t n, const void* tree, const int* target,

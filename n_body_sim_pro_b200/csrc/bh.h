@@ -37,6 +37,7 @@ typedef struct NbspBarnesHutParams {
     int multipole_order;
     int leaf_capacity;
     int walk_mode;
+    int opening;            /* NBSP_BH_OPENING_* */
     const void* correction; /* device network (mlp.cuh Net) or NULL */
 } NbspBarnesHutParams;
 
@@ -112,9 +113,13 @@ NBSP_HIDDEN void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity
                                int* status, cudaStream_t stream);
 
 /* Moments + walk-format node records.  order 1 or 2. */
-NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, size_t n, const double* geometry,
-                                 double theta, int order, void* tree, int* status,
-                                 cudaStream_t stream);
+/* Opening tests: the reference's (2h)^2 < theta^2 d^2 (barnes_hut.c:596-599), or
+ * with the cell's centre-of-mass offset added, 2h / theta + shift < d. */
+enum { NBSP_BH_OPENING_REFERENCE = 0, NBSP_BH_OPENING_OFFSET = 1 };
+
+NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n,
+                                 const double* geometry, double theta, int opening, void* tree,
+                                 int* status, cudaStream_t stream);
 
 enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
 
@@ -128,10 +133,10 @@ NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int 
                               cudaStream_t stream);
 
 /* Learned correction: training pairs (target, accepted cell) sampled with the
- * reference criterion at theta, their features and exact-sum labels, and the
- * column statistics written into the network's scaling tables (`net`). */
+ * opening criterion `opening` at theta, their features and exact-sum labels, and
+ * the column statistics written into the network's scaling tables (`net`). */
 NBSP_HIDDEN void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta,
-                                   unsigned long long seed, int samples, int* target, int* cell,
+                                   int opening, unsigned long long seed, int samples, int* target, int* cell,
                                    int* status, cudaStream_t stream);
 NBSP_HIDDEN void nbsp_bh_mlp_labels(const void* pos4, size_t n, const void* tree,
                                     const int* target, const int* cell, int samples,
@@ -147,6 +152,7 @@ typedef struct NbspTreeRef {
     size_t n;
     cudaStream_t stream;
     int* status;
+    int opening; /* the criterion the tree's opening radii were built with */
 } NbspTreeRef;
 
 /* Build the tree of the context's resident state (one Barnes-Hut evaluation,

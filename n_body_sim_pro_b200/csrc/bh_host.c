@@ -149,7 +149,8 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     nbsp_bh_gather(s->x, s->y, s->z, s->m, b->index, n, b->geometry, b->pos4, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
-    nbsp_bh_moments(b->pos4, n, b->geometry, p->theta, p->multipole_order, b->tree, status, stream);
+    nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening, b->tree, status,
+                    stream);
     cudaEventRecord(b->events[5], stream);
     nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode, p->correction,
                  (float)p->softening_squared, b->acc_hi,

@@ -42,6 +42,15 @@ typedef struct NbspAllPairsShape {
     int paired;       /* 1: targets processed in pairs with fma/add/mul.f32x2 */
 } NbspAllPairsShape;
 
+/* Sources of one chunk: ceil(n_padded / chunks) rounded up to a multiple of
+ * NBSP_ALLPAIRS_CHUNK_ALIGN (trailing chunks may be short or empty). */
+#define NBSP_ALLPAIRS_CHUNK_ALIGN 8
+static inline size_t nbsp_allpairs_chunk_len(size_t n_padded, int chunks) {
+    const size_t units = (n_padded + NBSP_ALLPAIRS_CHUNK_ALIGN - 1) / NBSP_ALLPAIRS_CHUNK_ALIGN;
+    const size_t c = chunks < 1 ? 1 : (size_t)chunks;
+    return (units + c - 1) / c * NBSP_ALLPAIRS_CHUNK_ALIGN;
+}
+
 /* Number of CTAs per SM the force kernel of this shape can keep resident. */
 NBSP_HIDDEN int nbsp_allpairs_resident_ctas(NbspAllPairsShape shape);
 NBSP_HIDDEN int nbsp_allpairs_shape_supported(NbspAllPairsShape shape);

@@ -237,7 +237,7 @@ NBodySimProStatus n_body_sim_pro_cuda_correction_generate(NBodySimProCudaCorrect
     MTRY(cudaMalloc((void**)&ok, samples * sizeof(int)));
     MTRY(cudaMalloc((void**)&feat, samples * IN * sizeof(float)));
     MTRY(cudaMalloc((void**)&lab, samples * OUT * sizeof(float)));
-    nbsp_bh_mlp_pairs(tr.pos4, tr.n, tr.tree, (float)theta, seed, ns, target, cell, tr.status,
+    nbsp_bh_mlp_pairs(tr.pos4, tr.n, tr.tree, (float)theta, tr.opening, seed, ns, target, cell, tr.status,
                       tr.stream);
     nbsp_bh_mlp_labels(tr.pos4, tr.n, tr.tree, target, cell, ns, (float)gravity->softening_squared,
                        feat, lab, ok, tr.stream);

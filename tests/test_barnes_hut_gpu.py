@@ -29,11 +29,12 @@ def walk(request):
     return request.param
 
 
-def bh(nb, p, eps, theta, ctx, order=1, leaf=16, walk=1):
+def bh(nb, p, eps, theta, ctx, order=1, leaf=16, walk=1, opening=0):
     ctx.theta = theta
     ctx.set_multipole_order(order)
     ctx.set_leaf_capacity(leaf)
     ctx.set_walk(walk)
+    ctx.set_opening(opening)
     s = to_system(nb, p)
     a = nb.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, nb.gravity_init(1.0, eps), ctx)
     return a, ctx.stats()
@@ -145,6 +146,34 @@ def test_collision_config_accuracy(cuda, ctx, walk):
     e2 = O.rms_relative_error(a2[targets], ref)
     print(f"collision200k mono={e1:.3e} quad={e2:.3e} stats={st}")
     assert e1 < 1e-2 and e2 < e1
+
+
+@pytest.mark.parametrize("theta", [0.5, 1.0])
+def test_offset_opening_is_more_accurate(cuda, ctx, theta, walk):
+    """The offset test (2h / theta + |com - cell centre| < d) accepts a subset of
+    the reference test's cells: at theta 1.0 no target inside a cell accepts it,
+    which removes most of the reference criterion's error there."""
+    p = O.preset("plummer_collision", 200000, 42)
+    targets = np.random.default_rng(2).choice(p.n, 1024, replace=False)
+    ref = O.gravity_subset(p, 1.0, 0.01, targets)
+    a0, s0 = bh(cuda, p, 0.01, theta, ctx, walk=walk, opening=0)
+    a1, s1 = bh(cuda, p, 0.01, theta, ctx, walk=walk, opening=1)
+    e0 = O.rms_relative_error(a0[targets], ref)
+    e1 = O.rms_relative_error(a1[targets], ref)
+    print(f"theta={theta} reference={e0:.3e} offset={e1:.3e} "
+          f"terms {s0['accepted_approximations'] + s0['exact_interactions']} -> "
+          f"{s1['accepted_approximations'] + s1['exact_interactions']}")
+    assert e1 < e0
+    if theta == 1.0:
+        assert e1 < 0.8 * e0
+    b1, _ = bh(cuda, p, 0.01, theta, ctx, walk=walk, opening=1)
+    assert np.array_equal(a1, b1)
+
+
+def test_opening_argument_checked(cuda, ctx):
+    with pytest.raises(cuda.CudaError):
+        ctx.set_opening(2)
+    ctx.set_opening(cuda.Opening.REFERENCE)
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 33, 4097, 10000])
