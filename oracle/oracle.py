@@ -110,6 +110,11 @@ def build(ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref and os.path.isdir("/root/reference/src/c"):
         subprocess.run(["make", "-s", "-C", HERE, "-j8", "ref"], check=True)
+        # the reference's force benchmark with the two CUDA algorithms (needs
+        # the B200 library, built first by the package's own build step)
+        if os.path.exists(os.path.join(HERE, "..", "n_body_sim_pro_b200", "lib",
+                                       "libn_body_sim_pro_cuda.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "integrated"], check=True)
 
 
 _lib = None
