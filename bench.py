@@ -10,7 +10,10 @@ Metric: particle-steps/s (N x steps / device time).
 
 Other workloads (parity configs, selectable): ``allpairs_plummer_16k``,
 ``allpairs_precision_262k``, ``ensemble_4096`` and ``bh_matched_10m`` (the
-same collision at N = 10M).
+same collision at N = 10M).  Multi-GPU sharding (strong scaling, `scaling`
+"strong"): ``allpairs_sharded_262k`` splits one all-pairs system by targets
+over the ranks with an NCCL all-gather of the packed sources every step;
+``ensemble_4096_sharded`` splits the 4096 systems over the ranks by cost.
 
 `matched_accuracy` (Barnes-Hut workloads, skipped with --no-matched): on the
 initial state, the rms relative force error against the FP64 direct sum on
@@ -25,9 +28,10 @@ cell-target pairs of the 1M collision).
 Timing: W untimed warm-up steps; then K steps, each a 1-step device-resident
 advance bracketed by CUDA events recorded by the library on its own stream;
 a 256 MiB buffer is written between timed steps to flush the 126 MB L2.
-Under torchrun (N > 1) every rank advances its own replica (no data-path
-collective: the path is single-GPU; "replicas only"), the step time is the
-max over ranks and `value` sums the ranks' particle-steps.
+Under torchrun (N > 1) every rank of the Barnes-Hut and all-pairs workloads
+advances its own replica (no data-path collective: "replicas only"), the step
+time is the max over ranks and `value` sums the ranks' particle-steps; the
+sharded workloads divide one job instead.
 
 `e2e`: the same metric through the reference-facing plugin call
 n_body_sim_pro_barnes_hut_compute_acceleration_cuda(view, ...) on pinned host
@@ -65,6 +69,12 @@ WORKLOADS = {
                           dt=1e-3, ic="ensemble", steps=1000),
     "bh_matched_10m": dict(n=10_000_000, algorithm="barnes_hut", theta=0.5, eps=0.01, dt=1e-3,
                            ic="collision", steps=3, order=1, matched=True, correction=True),
+    # one system split by targets over the ranks (strong scaling; NCCL all-gather per step)
+    "allpairs_sharded_262k": dict(n=262144, algorithm="all_pairs_sharded", eps=1e-3, dt=1e-4,
+                                  ic="uniform_log_mass", steps=3),
+    # the 4096 systems split over the ranks by cost (strong scaling; no collective)
+    "ensemble_4096_sharded": dict(n=None, algorithm="ensemble", systems=4096, lo=32, hi=4096,
+                                  eps=0.01, dt=1e-3, ic="ensemble", steps=1000, sharded=True),
 }
 
 # Matched-accuracy study: the largest opening angle of this grid whose rms
@@ -207,7 +217,9 @@ def fp32_peak_tflops(sm_count, mhz):
     return sm_count * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
 
 
-def dist_setup(gpus):
+def dist_setup(gpus, backend="nccl"):
+    """One process per GPU under torchrun (RANK / WORLD_SIZE / LOCAL_RANK from the
+    environment); `backend` "gloo" runs the same host logic on CPU processes."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -217,20 +229,26 @@ def dist_setup(gpus):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
-def barrier_sync(world):
+def _device_sync():
     import torch
 
-    torch.cuda.synchronize()
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.synchronize()
+
+
+def barrier_sync(world):
+    _device_sync()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-        torch.cuda.synchronize()
+        _device_sync()
 
 
 def max_over_ranks(value, world):
@@ -239,7 +257,8 @@ def max_over_ranks(value, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -543,14 +562,17 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
     return out
 
 
-def ensemble_ic(wl, seed=42):
+def ensemble_ic(wl, seed=42, systems=None):
     """Systems of round(exp(U(ln lo, ln hi))) Plummer particles (a = 1, M = 1), each
-    from its own seeded stream, concatenated."""
+    from its own seeded stream, concatenated (only `systems`, when given)."""
     sizes, blocks = [], []
+    keep = set(range(wl["systems"])) if systems is None else set(systems)
     for k in range(wl["systems"]):
         rng = np.random.default_rng([seed, k])
         n = int(np.clip(np.rint(np.exp(rng.uniform(np.log(wl["lo"]), np.log(wl["hi"])))),
                         wl["lo"], wl["hi"]))
+        if k not in keep:
+            continue
         blocks.append(plummer_block(rng, n, 1.0, 1.0, (0.0, 0.0, 0.0)))
         sizes.append(n)
     pos = np.vstack([b[0] for b in blocks])
@@ -560,12 +582,29 @@ def ensemble_ic(wl, seed=42):
     return pos, vel, mass, offsets
 
 
+def ensemble_sizes(wl, seed=42):
+    """The system sizes ensemble_ic draws, without generating the particles."""
+    out = []
+    for k in range(wl["systems"]):
+        rng = np.random.default_rng([seed, k])
+        out.append(int(np.clip(np.rint(np.exp(rng.uniform(np.log(wl["lo"]),
+                                                           np.log(wl["hi"])))),
+                               wl["lo"], wl["hi"])))
+    return out
+
+
 def run_ensemble(args, wl, world, rank, local):
     import torch
 
     import n_body_sim_pro_b200 as nb
 
-    pos, vel, mass, offsets = ensemble_ic(wl, seed=42 + rank)
+    if wl.get("sharded"):  # one ensemble, its systems split over the ranks by cost
+        from n_body_sim_pro_b200 import shard
+
+        mine = shard.assign_systems(ensemble_sizes(wl), world)[rank]
+        pos, vel, mass, offsets = ensemble_ic(wl, seed=42, systems=mine)
+    else:  # an independent replica per rank
+        pos, vel, mass, offsets = ensemble_ic(wl, seed=42 + rank)
     n = mass.shape[0]
     sizes = np.diff(offsets.astype(np.int64))
     g = nb.gravity_init(1.0, wl["eps"])
@@ -606,13 +645,113 @@ def run_ensemble(args, wl, world, rank, local):
                              f"({peak_kind})", "flops_per_launch": flops,
                 "launch_ms": round(total_ms, 3), "traffic": None}
     ens.close()
-    value = world * n * args.steps / (total_ms * 1e-3)
+    if wl.get("sharded"):
+        n_all = max_over_ranks(float(sum(ensemble_sizes(wl))), world)
+        value = n_all * args.steps / (total_ms * 1e-3)
+        interactions = float(sum(float(v) ** 2 for v in ensemble_sizes(wl))) / world
+    else:
+        value = world * n * args.steps / (total_ms * 1e-3)
     return dict(value=value, total_ms=total_ms, rms=None, max_rel=None, drift=None,
                 roofline=roofline, clocks=clk, launches=launches, e2e=None,
                 interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
                 stats={"systems": int(len(sizes)), "particles": int(n),
                        "ensemble": info, "one_launch_per_system": baseline},
                 timings={"advance_ms": round(ms, 3)})
+
+
+def run_sharded_allpairs(args, wl, world, rank, local):
+    """One all-pairs system split by targets over the ranks (strong scaling):
+    each step is shard_begin (kick-drift-pack), an NCCL all-gather of the
+    packed sources (16 bytes per particle) and shard_end (forces + kick)."""
+    import torch
+
+    import n_body_sim_pro_b200 as nb
+    from n_body_sim_pro_b200 import shard
+
+    n = wl["n"]
+    pos, vel, mass = initial_conditions(wl["ic"], n, seed=42)  # the same system on every rank
+    first, count = shard.split(n, world)[rank]
+    g = nb.gravity_init(1.0, wl["eps"])
+    ctx = nb.CudaContext()
+    part = nb.ParticleSystem.from_arrays(pos[first:first + count], vel[first:first + count],
+                                         mass[first:first + count])
+    device = torch.device("cuda", local)
+    sim = shard.ShardedAllPairs(part, g, shard.CudaShardBackend(ctx), device)
+    sim.compute_forces()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        sim.step(wl["dt"], 1)
+    barrier_sync(world)
+    launches0 = nb.kernel_launches()
+    step_ms, force_ms = [], []
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed_steps")
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ev0.record()
+            sim.step(wl["dt"], 1)
+            ev1.record()
+            ev1.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+            force_ms.append(ctx.timings()["walk_ms"])
+    torch.cuda.nvtx.range_pop()
+    launches = nb.kernel_launches() - launches0
+    barrier_sync(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+
+    # accuracy of the final state on rank 0: the full system gathered, FP64 oracle
+    sim.compute_forces()
+    mine = nb.ParticleSystem.zeros(count)
+    sim.download(mine)
+    rows = np.zeros((sim.capacity, 7))
+    rows[:count] = np.stack([mine.x, mine.y, mine.z, part.m, mine.ax, mine.ay, mine.az], 1)
+    local_rows = torch.from_numpy(rows).to(device)
+    if world > 1:
+        import torch.distributed as dist
+
+        every = torch.empty((world * sim.capacity, 7), dtype=torch.float64, device=device)
+        dist.all_gather_into_tensor(every, local_rows)
+        every = every.cpu().numpy()
+    else:
+        every = rows
+    rms = max_rel = None
+    if rank == 0:
+        full = np.concatenate([every[r * sim.capacity: r * sim.capacity + c]
+                               for r, c in enumerate(sim.counts)])
+        state = nb.ParticleSystem.from_arrays(full[:, :3], np.zeros((n, 3)), full[:, 3])
+        targets = np.random.default_rng(7).choice(n, min(4096, n), replace=False)
+        with nb.CudaContext() as oracle_ctx:
+            oracle_ctx.upload(state)
+            ref = oracle_ctx.reference_acceleration(g, targets)
+        acc = full[targets, 4:7]
+        rms = float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
+        max_rel = float(np.max(np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+
+    peaks, peak_kind = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
+    kernel_ms = float(np.mean(force_ms))
+    flops = FLOPS_PAIR * float(count) * float(n)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "allpairs_force_kernel (this rank's targets)",
+                "achieved": round(achieved, 3), "peak": round(peak_max, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak_max, 4),
+                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x "
+                             f"{peaks.get('sm_max_mhz', 1965.0)} MHz ({peak_kind})",
+                "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None,
+                "all_gather_bytes_per_step": 16 * world * sim.capacity}
+    ctx.close()
+    return dict(value=n * args.steps / (total_ms * 1e-3), total_ms=total_ms, rms=rms,
+                max_rel=max_rel, drift=None, roofline=roofline, clocks=clocks.summary(),
+                launches=launches, e2e=None,
+                interactions_per_s=float(n) * n * args.steps / (total_ms * 1e-3),
+                stats={"particles": n, "ranks": world, "slice": count,
+                       "slice_capacity": sim.capacity},
+                timings={"step_ms_mean": round(float(np.mean(step_ms)), 4),
+                         "force_ms_mean": round(kernel_ms, 4)})
 
 
 def ctx_timings_summary(step_ms, walk_ms, phases=()):
@@ -720,9 +859,15 @@ def main(argv=None):
         return 0
 
     world, rank, local = dist_setup(args.gpus)
+    sharded = wl["algorithm"] == "all_pairs_sharded" or wl.get("sharded", False)
+    if sharded:
+        config["parallelism"] = f"sharded x{world}"
     if wl["algorithm"] == "ensemble":
         r = run_ensemble(args, wl, world, rank, local)
-        config["particles"] = r["stats"]["particles"]
+        config["particles"] = (sum(ensemble_sizes(wl)) if wl.get("sharded")
+                               else r["stats"]["particles"])
+    elif wl["algorithm"] == "all_pairs_sharded":
+        r = run_sharded_allpairs(args, wl, world, rank, local)
     else:
         r = run_ours(args, wl, world, rank, local)
     cpu = None
@@ -741,7 +886,8 @@ def main(argv=None):
         line = {"metric": metric, "value": r["value"], "unit": metric, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32-force/f64-state",
+                "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+                "dtype": "f32-force/f64-state",
                 "data": "synthetic", "config": config,
                 "accuracy": {"rms_rel_force_err": r["rms"], "max_rel_force_err": r["max_rel"],
                              "energy_drift": r["drift"], "oracle": "FP64 device direct sum, "

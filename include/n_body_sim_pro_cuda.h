@@ -379,6 +379,33 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_advance(
     NBodySimProCudaAlgorithm algorithm, NBodySimProError* error);
 
 /*
+ * All-pairs sharded by targets, one process (and context) per GPU: the
+ * context's resident state is this rank's slice of the particles.  One
+ * leapfrog KDK step (integrator.c:47-85) is split around the all-gather of
+ * the packed sources, which the caller runs (NCCL):
+ *
+ *   shard_begin  opening kick + drift of the slice (skipped for timestep 0),
+ *                then the slice packed as float4 (x - c, y - c, z - c, m) into
+ *                `slice` (device memory, slice_capacity entries, a multiple of
+ *                8 and >= the resident count; the rest written massless).
+ *                `centre` c must be the same on every rank.
+ *   (caller)     all-gather every rank's slice, in rank order, into `sources`.
+ *   shard_end    accelerations of the slice from the source_count packed
+ *                sources (this rank's own slice at entry slice_offset, so the
+ *                pair of a particle with itself adds 0), then the closing kick.
+ *
+ * timestep 0 in both calls only sets the accelerations (the forces before the
+ * first step).  Both return when their work has finished.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_shard_begin(
+    NBodySimProCudaContext* context, double timestep, const double centre[3], void* slice,
+    size_t slice_capacity, NBodySimProError* error);
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_shard_end(
+    NBodySimProCudaContext* context, const NBodySimProGravity* gravity, double timestep,
+    const void* sources, size_t source_count, size_t slice_offset, NBodySimProError* error);
+
+/*
  * Conservation diagnostics of the resident state in FP64 on the device:
  * n_body_sim_pro_diagnostics_compute_global (src/c/diagnostics/numerics.c:5-81)
  * and, when `potential_energy` is non-NULL, the O(N^2) softened potential

@@ -176,6 +176,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
+    "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
 )
 
 # NBodySimProSimulationPreset (generation/presets.h:27-38)
@@ -235,6 +236,10 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_download": (st, [vp, pv, pe]),
         "n_body_sim_pro_cuda_compute_acceleration": (st, [vp, pg, C.c_int, pe]),
         "n_body_sim_pro_cuda_advance": (st, [vp, pg, C.c_int, C.c_double, C.c_int, C.c_int, pe]),
+        "n_body_sim_pro_cuda_shard_begin": (st, [vp, C.c_double, C.POINTER(C.c_double), vp,
+                                                 C.c_size_t, pe]),
+        "n_body_sim_pro_cuda_shard_end": (st, [vp, pg, C.c_double, vp, C.c_size_t, C.c_size_t,
+                                               pe]),
         "n_body_sim_pro_cuda_diagnostics": (st, [vp, pg, C.POINTER(DiagnosticsQuantities),
                                                  C.POINTER(C.c_double), pe]),
         "n_body_sim_pro_cuda_reference_acceleration": (st, [vp, pg, C.POINTER(C.c_int64),
@@ -520,6 +525,26 @@ class CudaContext:
         _check(library().n_body_sim_pro_cuda_advance(self.handle, C.byref(gravity),
                                                      int(integrator), float(timestep), int(steps),
                                                      int(algorithm), C.byref(err)), err)
+
+    def shard_begin(self, timestep: float, centre, slice_ptr: int, slice_capacity: int) -> None:
+        """Opening kick + drift of the resident slice, then its packed sources
+        into the device buffer at `slice_ptr` (slice_capacity float4 entries)."""
+        c3 = (C.c_double * 3)(*[float(v) for v in centre])
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_shard_begin(self.handle, float(timestep), c3,
+                                                         C.c_void_p(int(slice_ptr)),
+                                                         int(slice_capacity), C.byref(err)), err)
+
+    def shard_end(self, gravity: Gravity, timestep: float, sources_ptr: int, source_count: int,
+                  slice_offset: int) -> None:
+        """Forces of the resident slice from all gathered sources, then the
+        closing kick."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_shard_end(self.handle, C.byref(gravity),
+                                                       float(timestep),
+                                                       C.c_void_p(int(sources_ptr)),
+                                                       int(source_count), int(slice_offset),
+                                                       C.byref(err)), err)
 
     def diagnostics(self, gravity: Gravity | None = None, potential: bool = False):
         err = Error()

@@ -49,8 +49,8 @@ constexpr int kChunkAlign = NBSP_ALLPAIRS_CHUNK_ALIGN;
 
 template <int BLOCK, int K, bool ZERO_SOFTENING>
 __global__ void __launch_bounds__(BLOCK) allpairs_force_kernel(
-    const float4* __restrict__ packed, int n, int n_padded, int chunk_len, float eps2,
-    float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
+    const float4* __restrict__ packed, const float4* __restrict__ targets, int n, int n_padded,
+    int chunk_len, float eps2, float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
   __shared__ float4 tile[BLOCK];
   const int tid = threadIdx.x;
   const int first_target = blockIdx.x * (BLOCK * K) + tid;
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_kernel(
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int i = first_target + k * BLOCK;
-    const float4 q = i < n ? packed[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 q = i < n ? targets[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     xi[k] = q.x;
     yi[k] = q.y;
     zi[k] = q.z;
@@ -147,8 +147,8 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
 
 template <int BLOCK, int K, bool ZERO_SOFTENING>
 __global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
-    const float4* __restrict__ packed, int n, int n_padded, int chunk_len, float eps2,
-    float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
+    const float4* __restrict__ packed, const float4* __restrict__ targets, int n, int n_padded,
+    int chunk_len, float eps2, float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
   static_assert(K % 2 == 0, "targets are processed in pairs");
   constexpr int P = K / 2;
   __shared__ float4 tile[BLOCK];
@@ -160,8 +160,8 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     const int i0 = first_target + (2 * p) * BLOCK, i1 = first_target + (2 * p + 1) * BLOCK;
-    const float4 a = i0 < n ? packed[i0] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 b = i1 < n ? packed[i1] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 a = i0 < n ? targets[i0] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 b = i1 < n ? targets[i1] : make_float4(0.f, 0.f, 0.f, 0.f);
     X[p] = pack2(a.x, b.x);
     Y[p] = pack2(a.y, b.y);
     Z[p] = pack2(a.z, b.z);
@@ -234,7 +234,8 @@ __global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
   }
 }
 
-typedef void (*ForceKernel)(const float4*, int, int, int, float, float4*, float4*);
+typedef void (*ForceKernel)(const float4*, const float4*, int, int, int, float, float4*,
+                            float4*);
 
 template <int BLOCK, int K>
 ForceKernel pick(bool zero_softening) {
@@ -640,16 +641,24 @@ void nbsp_pack_relative(const double* x, const double* y, const double* z, const
                                                            (float4*)packed, status);
 }
 
+void nbsp_allpairs_force_targets(const void* sources, size_t n_sources_padded, const void* targets,
+                                 size_t n_targets, float softening_squared,
+                                 NbspAllPairsShape shape, void* partial_hi, void* partial_lo,
+                                 cudaStream_t stream) {
+  ForceKernel k = select_kernel(shape, softening_squared == 0.f);
+  const int targets_per_cta = shape.block * shape.per_thread;
+  const int chunk_len = (int)nbsp_allpairs_chunk_len(n_sources_padded, shape.chunks);
+  dim3 grid((unsigned)((n_targets + targets_per_cta - 1) / targets_per_cta), (unsigned)shape.chunks);
+  NBSP_COUNT_LAUNCH(1), k<<<grid, shape.block, 0, stream>>>(
+      (const float4*)sources, (const float4*)targets, (int)n_targets, (int)n_sources_padded,
+      chunk_len, softening_squared, (float4*)partial_hi, (float4*)partial_lo);
+}
+
 void nbsp_allpairs_force(const void* packed, size_t n, size_t n_padded, float softening_squared,
                          NbspAllPairsShape shape, void* partial_hi, void* partial_lo,
                          cudaStream_t stream) {
-  ForceKernel k = select_kernel(shape, softening_squared == 0.f);
-  const int targets_per_cta = shape.block * shape.per_thread;
-  const int chunk_len = (int)nbsp_allpairs_chunk_len(n_padded, shape.chunks);
-  dim3 grid((unsigned)((n + targets_per_cta - 1) / targets_per_cta), (unsigned)shape.chunks);
-  NBSP_COUNT_LAUNCH(1), k<<<grid, shape.block, 0, stream>>>((const float4*)packed, (int)n, (int)n_padded, chunk_len,
-                                      softening_squared, (float4*)partial_hi,
-                                      (float4*)partial_lo);
+  nbsp_allpairs_force_targets(packed, n_padded, packed, n, softening_squared, shape, partial_hi,
+                              partial_lo, stream);
 }
 
 void nbsp_allpairs_finalize(const void* partial_hi, const void* partial_lo, size_t n, int chunks,

@@ -18,6 +18,7 @@
 
 #include <cuda_runtime_api.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -70,7 +71,8 @@ static NBodySimProStatus cuda_fail(NBodySimProError* error, cudaError_t code, co
 enum { TUNE_SLOTS = 16, EVENT_COUNT = 10 };
 
 typedef struct TuneEntry {
-    size_t n;
+    size_t n;       /* targets */
+    size_t sources; /* padded sources */
     int zero_softening;
     NbspAllPairsShape shape;
 } TuneEntry;
@@ -367,21 +369,20 @@ static const NbspAllPairsShape kShapes[] = {
  * CTAs: the busiest CTA slot's sources (chunks end on 8-source boundaries) against
  * the average, less a small cost per chunk (one more partial per target). */
 static NbspAllPairsShape fit_chunks(const NBodySimProCudaContext* c, NbspAllPairsShape s,
-                                    size_t n) {
+                                    size_t n_targets, size_t n_sources_padded) {
     const size_t per_cta = (size_t)s.block * (size_t)s.per_thread;
-    const size_t target_blocks = (n + per_cta - 1) / per_cta;
+    const size_t target_blocks = (n_targets + per_cta - 1) / per_cta;
     int resident = nbsp_allpairs_resident_ctas(s);
     if (resident < 1) resident = 1;
     const size_t slots = (size_t)c->sm_count * (size_t)resident;
-    const size_t n_padded = round_up(n, 256);
     size_t best_chunks = 1;
     double best_eff = 0.0;
     for (size_t chunks = 1; chunks <= 64; ++chunks) {
-        const size_t len = nbsp_allpairs_chunk_len(n_padded, (int)chunks);
+        const size_t len = nbsp_allpairs_chunk_len(n_sources_padded, (int)chunks);
         if (chunks > 1 && len < 2 * (size_t)s.block) break;
         const size_t ctas = target_blocks * chunks;
         const size_t waves = (ctas + slots - 1) / slots;
-        const double work = (double)target_blocks * (double)n_padded;
+        const double work = (double)target_blocks * (double)n_sources_padded;
         const double span = (double)waves * (double)len * (double)slots;
         const double eff = work / span - 0.002 * (double)chunks;
         if (eff > best_eff + 1e-9) {
@@ -393,23 +394,30 @@ static NbspAllPairsShape fit_chunks(const NBodySimProCudaContext* c, NbspAllPair
     return s;
 }
 
-static NbspAllPairsShape choose_shape(NBodySimProCudaContext* c, size_t n, float eps2) {
+/* The fastest kernel shape for n_targets targets (`targets`) against
+ * n_sources_padded packed sources (`sources`), timed once per size pair on
+ * the live buffers and cached. */
+static NbspAllPairsShape choose_shape_for(NBodySimProCudaContext* c, const void* sources,
+                                          size_t n_sources_padded, const void* targets,
+                                          size_t n_targets, float eps2) {
     const int zero = eps2 == 0.f;
     for (int k = 0; k < c->tune_count; ++k)
-        if (c->tune[k].n == n && c->tune[k].zero_softening == zero) return c->tune[k].shape;
-    NbspAllPairsShape best = fit_chunks(c, kShapes[0], n);
-    if (c->autotune && n >= 2048) {
+        if (c->tune[k].n == n_targets && c->tune[k].sources == n_sources_padded &&
+            c->tune[k].zero_softening == zero)
+            return c->tune[k].shape;
+    NbspAllPairsShape best = fit_chunks(c, kShapes[0], n_targets, n_sources_padded);
+    if (c->autotune && n_targets >= 2048) {
         float best_ms = 1e30f;
         const int shapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
         for (int k = 0; k < shapes; ++k) {
             if (!nbsp_allpairs_shape_supported(kShapes[k])) continue;
-            NbspAllPairsShape s = fit_chunks(c, kShapes[k], n);
-            if ((size_t)s.chunks * n > c->partial_elems) continue;
+            NbspAllPairsShape s = fit_chunks(c, kShapes[k], n_targets, n_sources_padded);
+            if ((size_t)s.chunks * n_targets > c->partial_elems) continue;
             float total = 0.f;
             for (int rep = 0; rep < 3; ++rep) {
                 cudaEventRecord(c->events[8], c->stream);
-                nbsp_allpairs_force(c->packed, n, c->n_padded, eps2, s, c->partial_hi,
-                                    c->partial_lo, c->stream);
+                nbsp_allpairs_force_targets(sources, n_sources_padded, targets, n_targets, eps2,
+                                            s, c->partial_hi, c->partial_lo, c->stream);
                 cudaEventRecord(c->events[9], c->stream);
                 cudaEventSynchronize(c->events[9]);
                 float ms = 0.f;
@@ -422,11 +430,16 @@ static NbspAllPairsShape choose_shape(NBodySimProCudaContext* c, size_t n, float
             }
         }
     }
-    const int slot = c->tune_count < TUNE_SLOTS ? c->tune_count++ : (int)(n % TUNE_SLOTS);
-    c->tune[slot].n = n;
+    const int slot = c->tune_count < TUNE_SLOTS ? c->tune_count++ : (int)(n_targets % TUNE_SLOTS);
+    c->tune[slot].n = n_targets;
+    c->tune[slot].sources = n_sources_padded;
     c->tune[slot].zero_softening = zero;
     c->tune[slot].shape = best;
     return best;
+}
+
+static NbspAllPairsShape choose_shape(NBodySimProCudaContext* c, size_t n, float eps2) {
+    return choose_shape_for(c, c->packed, c->n_padded, c->packed, n, eps2);
 }
 
 /* Partial buffers big enough for any candidate shape at n (<= 64 chunks). */
@@ -812,6 +825,90 @@ NBodySimProStatus n_body_sim_pro_cuda_advance(NBodySimProCudaContext* c,
         c->timings.walk_ms = force_ms;
         c->timings.integrate_ms = ms - force_ms * steps;
     }
+    c->timings.total_ms = ms;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+/* ---- all-pairs sharded by targets (one process per GPU) ------------------ */
+
+NBodySimProStatus n_body_sim_pro_cuda_shard_begin(NBodySimProCudaContext* c, double timestep,
+                                                  const double centre[3], void* slice,
+                                                  size_t slice_capacity, NBodySimProError* error) {
+    if (c == NULL || centre == NULL || slice == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "context, centre and slice must not be null");
+    if (!(timestep >= 0.0) || !isfinite(timestep))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "timestep must be finite and >= 0");
+    if (!isfinite(centre[0]) || !isfinite(centre[1]) || !isfinite(centre[2]))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "centre must be finite");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    if (slice_capacity < c->n || slice_capacity % NBSP_ALLPAIRS_CHUNK_ALIGN != 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "slice capacity must hold the resident particles and be a multiple of 8");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaEventRecord(c->events[0], c->stream));
+    if (timestep > 0.0 && c->n > 0)
+        nbsp_kick_drift(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, c->n,
+                        0.5 * timestep, timestep, c->stream);
+    CUDA_TRY(cudaMemcpyAsync(c->centre, centre, 3 * sizeof(double), cudaMemcpyHostToDevice,
+                             c->stream));
+    if (slice_capacity > 0)
+        nbsp_pack_relative(c->x, c->y, c->z, c->m, c->n, slice_capacity, c->centre, slice,
+                           c->status, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
+    NBodySimProStatus st = check_device_status(c, error); /* synchronises */
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
+    memset(&c->timings, 0, sizeof(c->timings));
+    c->timings.integrate_ms = ms;
+    c->timings.total_ms = ms;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_shard_end(NBodySimProCudaContext* c,
+                                                const NBodySimProGravity* gravity,
+                                                double timestep, const void* sources,
+                                                size_t source_count, size_t slice_offset,
+                                                NBodySimProError* error) {
+    if (c == NULL || gravity == NULL || sources == NULL)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "context, gravity and sources must not be null");
+    if (!(timestep >= 0.0) || !isfinite(timestep))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "timestep must be finite and >= 0");
+    if (!c->resident) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "no resident state");
+    if (source_count % NBSP_ALLPAIRS_CHUNK_ALIGN != 0 || slice_offset > source_count ||
+        c->n > source_count - slice_offset || source_count > (size_t)INT32_MAX)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "sources must be a multiple of 8 entries holding this rank's slice at "
+                    "slice_offset");
+    NBodySimProStatus st = check_gravity(gravity, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    const size_t n = c->n;
+    if (n == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if ((st = prepare_allpairs(c, n, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    const float eps2 = (float)gravity->softening_squared;
+    const void* targets = (const char*)sources + slice_offset * 16;
+    NbspAllPairsShape s = choose_shape_for(c, sources, source_count, targets, n, eps2);
+    if ((size_t)s.chunks * n > c->partial_elems) s.chunks = (int)(c->partial_elems / n);
+    CUDA_TRY(cudaEventRecord(c->events[2], c->stream));
+    nbsp_allpairs_force_targets(sources, source_count, targets, n, eps2, s, c->partial_hi,
+                                c->partial_lo, c->stream);
+    CUDA_TRY(cudaEventRecord(c->events[3], c->stream));
+    nbsp_allpairs_finalize_kick(c->partial_hi, c->partial_lo, n, s.chunks,
+                                gravity->gravitational_constant, c->ax, c->ay, c->az, c->vx,
+                                c->vy, c->vz, 0.5 * timestep, c->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
+    if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    float ms = 0.f, force_ms = 0.f;
+    cudaEventElapsedTime(&ms, c->events[2], c->events[1]);
+    cudaEventElapsedTime(&force_ms, c->events[2], c->events[3]);
+    memset(&c->timings, 0, sizeof(c->timings));
+    c->timings.walk_ms = force_ms;
+    c->timings.integrate_ms = ms - force_ms;
     c->timings.total_ms = ms;
     return N_BODY_SIM_PRO_STATUS_OK;
 }

@@ -67,6 +67,15 @@ NBSP_HIDDEN void nbsp_allpairs_force(const void* packed, size_t n, size_t n_padd
                                      float softening_squared, NbspAllPairsShape shape,
                                      void* partial_hi, void* partial_lo, cudaStream_t stream);
 
+/* The same for n_targets targets (float4, same frame) against the first
+ * n_sources_padded packed sources (a multiple of NBSP_ALLPAIRS_CHUNK_ALIGN;
+ * trailing entries massless): hi[s*n_targets + i], lo[...]. */
+NBSP_HIDDEN void nbsp_allpairs_force_targets(const void* sources, size_t n_sources_padded,
+                                             const void* targets, size_t n_targets,
+                                             float softening_squared, NbspAllPairsShape shape,
+                                             void* partial_hi, void* partial_lo,
+                                             cudaStream_t stream);
+
 /* Accelerations a = G * sum_s (hi_s + lo_s) in FP64 into ax, ay, az. */
 NBSP_HIDDEN void nbsp_allpairs_finalize(const void* partial_hi, const void* partial_lo, size_t n,
                                         int chunks, double gravitational_constant, double* ax,
