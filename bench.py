@@ -88,9 +88,9 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 
 # capture of exactly this configuration (the file under profiles/ gives the command).
 PROFILED_TRAFFIC = {
     ("bh_collision_1m", 0.7, 1, "lists", 16): (
-        29_787_392, "profiles/walk_lists_kernel_bh_collision_1m.md"),
+        30_559_232, "profiles/walk_lists_kernel_bh_collision_1m.md"),
     ("allpairs_plummer_16k", None, 1, "lists", 16): (
-        273_152, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
+        296_960, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
 }
 
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM

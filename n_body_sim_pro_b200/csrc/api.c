@@ -413,8 +413,8 @@ static NbspAllPairsShape choose_shape_for(NBodySimProCudaContext* c, const void*
             if (!nbsp_allpairs_shape_supported(kShapes[k])) continue;
             NbspAllPairsShape s = fit_chunks(c, kShapes[k], n_targets, n_sources_padded);
             if ((size_t)s.chunks * n_targets > c->partial_elems) continue;
-            float total = 0.f;
-            for (int rep = 0; rep < 3; ++rep) {
+            float fastest = 1e30f; /* best of 4 timed launches after one warm-up */
+            for (int rep = 0; rep < 5; ++rep) {
                 cudaEventRecord(c->events[8], c->stream);
                 nbsp_allpairs_force_targets(sources, n_sources_padded, targets, n_targets, eps2,
                                             s, c->partial_hi, c->partial_lo, c->stream);
@@ -422,10 +422,10 @@ static NbspAllPairsShape choose_shape_for(NBodySimProCudaContext* c, const void*
                 cudaEventSynchronize(c->events[9]);
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, c->events[8], c->events[9]);
-                if (rep > 0) total += ms;
+                if (rep > 0 && ms < fastest) fastest = ms;
             }
-            if (total < best_ms) {
-                best_ms = total;
+            if (fastest < best_ms) {
+                best_ms = fastest;
                 best = s;
             }
         }
