@@ -145,8 +145,8 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
   return r;
 }
 
-template <int BLOCK, int K, bool ZERO_SOFTENING>
-__global__ void __launch_bounds__(BLOCK) allpairs_force_paired_kernel(
+template <int BLOCK, int K, bool ZERO_SOFTENING, int MIN_BLOCKS = 1>
+__global__ void __launch_bounds__(BLOCK, MIN_BLOCKS) allpairs_force_paired_kernel(
     const float4* __restrict__ packed, const float4* __restrict__ targets, int n, int n_padded,
     int chunk_len, float eps2, float4* __restrict__ hi_out, float4* __restrict__ lo_out) {
   static_assert(K % 2 == 0, "targets are processed in pairs");
@@ -243,13 +243,20 @@ ForceKernel pick(bool zero_softening) {
                         : allpairs_force_kernel<BLOCK, K, false>;
 }
 
-template <int BLOCK, int K>
+template <int BLOCK, int K, int MIN_BLOCKS = 1>
 ForceKernel pick_paired(bool zero_softening) {
-  return zero_softening ? allpairs_force_paired_kernel<BLOCK, K, true>
-                        : allpairs_force_paired_kernel<BLOCK, K, false>;
+  return zero_softening ? allpairs_force_paired_kernel<BLOCK, K, true, MIN_BLOCKS>
+                        : allpairs_force_paired_kernel<BLOCK, K, false, MIN_BLOCKS>;
 }
 
 ForceKernel select_kernel(NbspAllPairsShape s, bool zero_softening) {
+  if (s.paired && s.min_blocks > 0) {  // register caps for more resident warps
+    if (s.block == 256 && s.per_thread == 2 && s.min_blocks == 4)
+      return pick_paired<256, 2, 4>(zero_softening);
+    if (s.block == 128 && s.per_thread == 4 && s.min_blocks == 6)
+      return pick_paired<128, 4, 6>(zero_softening);
+    return nullptr;
+  }
   if (s.paired) {
     if (s.block == 64 && s.per_thread == 4) return pick_paired<64, 4>(zero_softening);
     if (s.block == 64 && s.per_thread == 8) return pick_paired<64, 8>(zero_softening);

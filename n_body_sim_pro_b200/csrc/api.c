@@ -360,9 +360,10 @@ static NBodySimProStatus check_gravity(const NBodySimProGravity* g, NBodySimProE
 /* ------------------------------------------------------------------------- */
 
 static const NbspAllPairsShape kShapes[] = {
-    {128, 4, 1, 0}, {128, 2, 1, 0}, {256, 2, 1, 0}, {64, 8, 1, 0}, {128, 8, 1, 0},
-    {64, 4, 1, 0},  {256, 4, 1, 0}, {64, 8, 1, 1},  {128, 4, 1, 1}, {128, 8, 1, 1},
-    {256, 4, 1, 1}, {64, 4, 1, 1},  {128, 2, 1, 1}, {256, 2, 1, 1},
+    {128, 4, 1, 0, 0}, {128, 2, 1, 0, 0}, {256, 2, 1, 0, 0}, {64, 8, 1, 0, 0},
+    {128, 8, 1, 0, 0}, {64, 4, 1, 0, 0},  {256, 4, 1, 0, 0}, {64, 8, 1, 1, 0},
+    {128, 4, 1, 1, 0}, {128, 8, 1, 1, 0}, {256, 4, 1, 1, 0}, {64, 4, 1, 1, 0},
+    {128, 2, 1, 1, 0}, {256, 2, 1, 1, 0}, {256, 2, 1, 1, 4}, {128, 4, 1, 1, 6},
 };
 
 /* Source chunks so that (target blocks x chunks) fills whole waves of resident

@@ -428,7 +428,7 @@ static void enqueue_persistent(NBodySimProCudaEnsemble* e, double g, float eps2,
 /* One launch per system per phase (the baseline the persistent launch replaces). */
 static void enqueue_per_system(NBodySimProCudaEnsemble* e, double g, float eps2, double dt,
                                int steps) {
-    const NbspAllPairsShape shape = {128, 4, 1, 0};
+    const NbspAllPairsShape shape = {128, 4, 1, 0, 0};
     const double h = 0.5 * dt;
     for (int step = 0; step < steps; ++step) {
         for (size_t s = 0; s < e->systems; ++s) {

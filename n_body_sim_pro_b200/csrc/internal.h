@@ -40,6 +40,7 @@ typedef struct NbspAllPairsShape {
     int per_thread;   /* targets per thread (1, 2, 4 or 8) */
     int chunks;       /* source chunks S (grid.y); partials reduced in FP64 */
     int paired;       /* 1: targets processed in pairs with fma/add/mul.f32x2 */
+    int min_blocks;   /* paired only: CTAs per SM the registers are capped for (0: none) */
 } NbspAllPairsShape;
 
 /* Sources of one chunk: ceil(n_padded / chunks) rounded up to a multiple of

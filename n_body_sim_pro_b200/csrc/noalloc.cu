@@ -154,6 +154,7 @@ n_body_sim_pro_cuda_allpairs_acceleration_noalloc(
   shape.block = kNoAllocBlock;
   shape.per_thread = kNoAllocPerThread;
   shape.paired = 0;
+  shape.min_blocks = 0;
   const size_t target_blocks = (n + kNoAllocBlock * kNoAllocPerThread - 1) /
                                (kNoAllocBlock * kNoAllocPerThread);
   size_t chunks = (148 * 8 + target_blocks - 1) / target_blocks;
