@@ -6,8 +6,9 @@
 // (src/c/physics/integrator.c:47-85, FP64 state).
 //
 // Scheduling: the host bundles systems of the same size class into work items
-// (a CTA of BLOCK threads split into subgroups of G = BLOCK / systems-per-item
-// threads, each subgroup owning one system of at most G * K particles) and
+// (a CTA of BLOCK threads split into subgroups of G threads — whole warps, or a
+// power of two below one warp — each subgroup owning one system of at most
+// G * K particles; threads past the last subgroup idle through the item) and
 // orders the items by cost (sum of n^2), largest first.  The grid is one
 // resident wave (SMs x CTAs-per-SM); each CTA takes the next item from an
 // atomic counter and runs ALL the requested steps of its systems before it

@@ -195,10 +195,16 @@ static int by_cost_desc(const void* a, const void* b) {
 
 /* Threads of the subgroup that owns a system of n particles: the kernel pads
  * each system to whole tiles of ENS_TILE sources (ensemble.cu kTile), and the
- * subgroup's G * k shared-memory slots must hold the padded system. */
+ * subgroup's G * k shared-memory slots must hold the padded system.  G is the
+ * smallest whole number of warps that does (a power of two below one warp, so
+ * subgroups never straddle a warp boundary): every thread slot beyond the
+ * system's particles still runs the force loop, so a power-of-two G would
+ * waste up to half of the work of the largest systems. */
 static int group_threads(long long n, int k) {
     const long long padded = (n + ENS_TILE - 1) / ENS_TILE * ENS_TILE;
-    return (int)next_pow2((unsigned)((padded + k - 1) / k));
+    const long long need = (padded + k - 1) / k;
+    if (need < 32) return (int)next_pow2((unsigned)need);
+    return (int)((need + 31) / 32 * 32);
 }
 
 /* Bundle systems into work items for threads-per-CTA `block` and `k` targets
