@@ -187,12 +187,14 @@ inline size_t sort_scratch_words(size_t n) {
 
 __global__ void __launch_bounds__(256) keys_kernel(
     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
-    size_t n, const double* __restrict__ geometry, uint64_t* __restrict__ keys,
-    uint32_t* __restrict__ index, uint32_t* __restrict__ hist) {
+    const double* __restrict__ m, size_t n, const double* __restrict__ geometry,
+    uint64_t* __restrict__ keys, uint32_t* __restrict__ index, float4* __restrict__ unsorted,
+    uint32_t* __restrict__ hist) {
   __shared__ uint32_t h[kSortPasses][kRadix];
   for (int k = threadIdx.x; k < kSortPasses * kRadix; k += blockDim.x) (&h[0][0])[k] = 0;
   __syncthreads();
   const double cx = geometry[0], cy = geometry[1], cz = geometry[2], hs = geometry[3];
+  const double mx = geometry[4], my = geometry[5], mz = geometry[6];  // centre of mass
   const unsigned lane = threadIdx.x & 31;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const size_t first = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -203,10 +205,15 @@ __global__ void __launch_bounds__(256) keys_kernel(
     const bool valid = i < n;
     uint64_t key = 0;
     if (valid) {
-      key = spread3(axis_code(x[i], cx, hs)) | (spread3(axis_code(y[i], cy, hs)) << 1) |
-            (spread3(axis_code(z[i], cz, hs)) << 2);
+      const double xi = x[i], yi = y[i], zi = z[i];
+      key = spread3(axis_code(xi, cx, hs)) | (spread3(axis_code(yi, cy, hs)) << 1) |
+            (spread3(axis_code(zi, cz, hs)) << 2);
       keys[i] = key;
       index[i] = (uint32_t)i;
+      // the walk's float4 (relative to the centre of mass), still in input
+      // order: the gather then moves one 16-byte record per particle
+      unsorted[i] = make_float4((float)__dsub_rn(xi, mx), (float)__dsub_rn(yi, my),
+                                (float)__dsub_rn(zi, mz), (float)m[i]);
     }
 #pragma unroll
     // digit counts: the low six bytes of the keys of one warp are spread over
@@ -408,12 +415,11 @@ __global__ void duplicates_kernel(const uint64_t* __restrict__ keys,
 // gather / scatter
 // ---------------------------------------------------------------------------
 
-__global__ void gather_kernel(const double* __restrict__ x, const double* __restrict__ y,
-                              const double* __restrict__ z, const double* __restrict__ m,
+// pos[s] = unsorted[perm[s]]; inverse[perm[s]] = s (for the unsort).
+__global__ void gather_kernel(const float4* __restrict__ unsorted,
                               const uint32_t* __restrict__ perm, size_t n,
-                              const double* __restrict__ geometry, float4* __restrict__ pos,
+                              float4* __restrict__ pos, uint32_t* __restrict__ inverse,
                               int* status) {
-  const double cx = geometry[4], cy = geometry[5], cz = geometry[6];
   for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
        s += (size_t)gridDim.x * blockDim.x) {
     const uint32_t i = perm[s];
@@ -422,23 +428,23 @@ __global__ void gather_kernel(const double* __restrict__ x, const double* __rest
       pos[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       continue;
     }
-    pos[s] = make_float4((float)__dsub_rn(x[i], cx), (float)__dsub_rn(y[i], cy),
-                         (float)__dsub_rn(z[i], cz), (float)m[i]);
+    pos[s] = unsorted[i];
+    inverse[i] = (uint32_t)s;
   }
 }
 
-__global__ void scatter_kernel(const float4* __restrict__ hi, const float4* __restrict__ lo,
-                               const uint32_t* __restrict__ perm, size_t n, double g,
-                               double* __restrict__ ax, double* __restrict__ ay,
-                               double* __restrict__ az) {
-  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
-       s += (size_t)gridDim.x * blockDim.x) {
-    const float4 h = hi[s], l = lo[s];
-    const uint32_t i = perm[s];
-    if (i >= n) continue;  // the gather already flagged a bad permutation
-    ax[i] = g * ((double)h.x + (double)l.x);
-    ay[i] = g * ((double)h.y + (double)l.y);
-    az[i] = g * ((double)h.z + (double)l.z);
+// a[i] = G * acc[inverse[i]]: random 32-byte reads, coalesced FP64 writes.
+__global__ void unsort_kernel(const double4* __restrict__ acc, const uint32_t* __restrict__ inverse,
+                              size_t n, double g, double* __restrict__ ax,
+                              double* __restrict__ ay, double* __restrict__ az) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t s = inverse[i];
+    if (s >= n) continue;  // only after the gather flagged a bad permutation
+    const double4 a = acc[s];
+    ax[i] = g * a.x;
+    ay[i] = g * a.y;
+    az[i] = g * a.z;
   }
 }
 
@@ -1095,14 +1101,13 @@ __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, i
   out.exact = exact;
 }
 
+// The compensated (hi, lo) sums combined in FP64, in Morton order.
 __device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active, int lane,
-                                           float4* __restrict__ acc_hi,
-                                           float4* __restrict__ acc_lo,
+                                           double4* __restrict__ acc,
                                            unsigned long long* __restrict__ counters) {
-  if (active) {
-    acc_hi[s] = make_float4(a.hx, a.hy, a.hz, 0.f);
-    acc_lo[s] = make_float4(a.lx, a.ly, a.lz, 0.f);
-  }
+  if (active)
+    acc[s] = make_double4((double)a.hx + (double)a.lx, (double)a.hy + (double)a.ly,
+                          (double)a.hz + (double)a.lz, 0.0);
   unsigned long long ap = a.approx, ex = a.exact;
   for (int off = 16; off > 0; off >>= 1) {
     ap += __shfl_down_sync(kFull, ap, off);
@@ -1116,8 +1121,8 @@ __device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active,
 
 template <int ORDER>
 __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
-    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
-    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status) {
+    const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
+    unsigned long long* __restrict__ counters, int* status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
@@ -1126,7 +1131,7 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
   const float4 p = pos[active ? s : n - 1];
   WalkAcc a;
   stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
-  store_walk(a, s, active, lane, acc_hi, acc_lo, counters);
+  store_walk(a, s, active, lane, acc, counters);
 }
 
 // Point sources (bucket particles and monopole cells) gathered per warp in
@@ -1663,8 +1668,8 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
 template <int ORDER, int STACK, bool CORR>
 __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
-    const float4* __restrict__ pos, int n, Tree t, float eps2, float4* __restrict__ acc_hi,
-    float4* __restrict__ acc_lo, unsigned long long* __restrict__ counters, int* status,
+    const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
+    unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ int s_cells[kListThreads / 32][CORR ? kListCap : 1];
@@ -1998,7 +2003,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
     a.approx = approx;
     a.exact = exact;
   }
-  store_walk(a, s, active, lane, acc_hi, acc_lo, counters);
+  store_walk(a, s, active, lane, acc, counters);
 }
 
 __global__ void tree_counts_kernel(Tree t, unsigned long long* counters) {
@@ -2030,16 +2035,16 @@ void nbsp_bh_bounds(const double* x, const double* y, const double* z, const dou
 
 size_t nbsp_bh_sort_scratch_words(size_t n) { return sort_scratch_words(n); }
 
-void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
-                  const double* geometry, uint64_t* keys, uint32_t* index, uint32_t* scratch,
-                  cudaStream_t stream) {
+void nbsp_bh_keys(const double* x, const double* y, const double* z, const double* m, size_t n,
+                  const double* geometry, uint64_t* keys, uint32_t* index, void* unsorted,
+                  uint32_t* scratch, cudaStream_t stream) {
   cudaMemsetAsync(scratch, 0, sort_scratch_words(n) * sizeof(uint32_t), stream);
   const SortScratch sc = sort_scratch(scratch, n);
   size_t blocks = (n + 255) / 256;
   if (blocks < 1) blocks = 1;
   if (blocks > (size_t)kKeysBlocks) blocks = kKeysBlocks;
-  NBSP_COUNT_LAUNCH(1), keys_kernel<<<(unsigned)blocks, 256, 0, stream>>>(x, y, z, n, geometry, keys,
-                                                                          index, sc.hist);
+  NBSP_COUNT_LAUNCH(1), keys_kernel<<<(unsigned)blocks, 256, 0, stream>>>(
+      x, y, z, m, n, geometry, keys, index, (float4*)unsorted, sc.hist);
 }
 
 void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt, uint32_t* index_alt,
@@ -2073,11 +2078,10 @@ void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double
   NBSP_COUNT_LAUNCH(1), duplicates_kernel<<<grid_for(n, 256), 256, 0, stream>>>(keys, perm, x, y, z, n, status);
 }
 
-void nbsp_bh_gather(const double* x, const double* y, const double* z, const double* m,
-                    const uint32_t* perm, size_t n, const double* geometry, void* pos4,
-                    int* status, cudaStream_t stream) {
-  NBSP_COUNT_LAUNCH(1), gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, y, z, m, perm, n, geometry,
-                                                      (float4*)pos4, status);
+void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
+                    uint32_t* inverse, int* status, cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
+      (const float4*)unsorted, perm, n, (float4*)pos4, inverse, status);
 }
 
 size_t nbsp_bh_tree_bytes(size_t n) { return tree_bytes(n); }
@@ -2118,44 +2122,40 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
 }
 
 void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
-                  const void* correction, float eps2, void* acc_hi, void* acc_lo,
+                  const void* correction, float eps2, void* acc,
                   unsigned long long* counters, int* status, cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
+  const float4* p = (const float4*)pos4;
+  double4* out = (double4*)acc;
   if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
-    const float4* p = (const float4*)pos4;
-    float4* hi = (float4*)acc_hi;
-    float4* lo = (float4*)acc_lo;
     if (net != nullptr) {  // the network corrects the monopole term
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, hi, lo, counters, status, net);
+          p, (int)n, t, eps2, out, counters, status, net);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, hi, lo, counters, status, nullptr);
+          p, (int)n, t, eps2, out, counters, status, nullptr);
     } else {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, hi, lo, counters, status, nullptr);
+          p, (int)n, t, eps2, out, counters, status, nullptr);
     }
     return;
   }
   const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
   if (order == 2) {
-    NBSP_COUNT_LAUNCH(1), walk_kernel<2><<<blocks, kWalkThreads, 0, stream>>>((const float4*)pos4, (int)n, t, eps2,
-                                                        (float4*)acc_hi, (float4*)acc_lo, counters,
-                                                        status);
+    NBSP_COUNT_LAUNCH(1), walk_kernel<2><<<blocks, kWalkThreads, 0, stream>>>(p, (int)n, t, eps2,
+                                                                            out, counters, status);
   } else {
-    NBSP_COUNT_LAUNCH(1), walk_kernel<1><<<blocks, kWalkThreads, 0, stream>>>((const float4*)pos4, (int)n, t, eps2,
-                                                        (float4*)acc_hi, (float4*)acc_lo, counters,
-                                                        status);
+    NBSP_COUNT_LAUNCH(1), walk_kernel<1><<<blocks, kWalkThreads, 0, stream>>>(p, (int)n, t, eps2,
+                                                                            out, counters, status);
   }
 }
 
-void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* perm, size_t n,
-                     double g, double* ax, double* ay, double* az, cudaStream_t stream) {
-  NBSP_COUNT_LAUNCH(1), scatter_kernel<<<grid_for(n, 256), 256, 0, stream>>>((const float4*)acc_hi,
-                                                       (const float4*)acc_lo, perm, n, g, ax, ay,
-                                                       az);
+void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n, double g, double* ax,
+                    double* ay, double* az, cudaStream_t stream) {
+  NBSP_COUNT_LAUNCH(1), unsort_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
+      (const double4*)acc, inverse, n, g, ax, ay, az);
 }
 
 void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta, int opening,

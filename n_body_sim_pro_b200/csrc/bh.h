@@ -79,9 +79,12 @@ NBSP_HIDDEN void nbsp_bh_bounds(const double* x, const double* y, const double* 
                                 const double* m, size_t n, double* partial, double* geometry,
                                 int* status, cudaStream_t stream);
 
-NBSP_HIDDEN void nbsp_bh_keys(const double* x, const double* y, const double* z, size_t n,
-                              const double* geometry, uint64_t* keys, uint32_t* index,
-                              uint32_t* sort_scratch, cudaStream_t stream);
+/* Morton keys, the identity index, the 8 digit histograms (into sort_scratch)
+ * and the walk's float4 (x - c, y - c, z - c, m) with c the centre of mass, in
+ * input order (`unsorted`, n entries). */
+NBSP_HIDDEN void nbsp_bh_keys(const double* x, const double* y, const double* z, const double* m,
+                              size_t n, const double* geometry, uint64_t* keys, uint32_t* index,
+                              void* unsorted, uint32_t* sort_scratch, cudaStream_t stream);
 
 /* 32-bit words of sort scratch for n keys (digit histograms, pass bases, tile
  * tickets and look-back status words). */
@@ -100,10 +103,9 @@ NBSP_HIDDEN void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, 
                                     const double* y, const double* z, size_t n, int* status,
                                     cudaStream_t stream);
 
-NBSP_HIDDEN void nbsp_bh_gather(const double* x, const double* y, const double* z,
-                                const double* m, const uint32_t* perm, size_t n,
-                                const double* geometry, void* pos4, int* status,
-                                cudaStream_t stream);
+/* pos4[s] = unsorted[perm[s]] (Morton order); inverse[perm[s]] = s. */
+NBSP_HIDDEN void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
+                                uint32_t* inverse, int* status, cudaStream_t stream);
 
 /* Device-side layout of the tree build scratch; sized by nbsp_bh_tree_bytes. */
 NBSP_HIDDEN size_t nbsp_bh_tree_bytes(size_t n);
@@ -123,14 +125,14 @@ NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t 
 
 enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
 
-/* Walk: a_sorted (float4 hi, lo per target) and interaction counters.
+/* Walk: a_sorted / G (double4 per target: the compensated sums combined in
+ * FP64) and interaction counters.
  * mode NBSP_BH_WALK_STACKLESS: warp-coherent skip-link walk, per-target test;
  * mode NBSP_BH_WALK_LISTS: lane-parallel node tests against the warp's group
  * box, dense evaluation of gathered interaction lists. */
 NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
-                              const void* correction, float softening_squared, void* acc_hi,
-                              void* acc_lo, unsigned long long* counters, int* status,
-                              cudaStream_t stream);
+                              const void* correction, float softening_squared, void* acc,
+                              unsigned long long* counters, int* status, cudaStream_t stream);
 
 /* Learned correction: training pairs (target, accepted cell) sampled with the
  * opening criterion `opening` at theta, their features and exact-sum labels, and
@@ -168,10 +170,10 @@ NBSP_HIDDEN const void* nbsp_correction_net(const NBodySimProCudaCorrection* cor
 NBSP_HIDDEN const void* nbsp_bh_positions(const NbspBarnesHut* bh);
 NBSP_HIDDEN const void* nbsp_bh_tree(const NbspBarnesHut* bh);
 
-/* a[perm[s]] = G * (hi + lo)[s] */
-NBSP_HIDDEN void nbsp_bh_scatter(const void* acc_hi, const void* acc_lo, const uint32_t* perm,
-                                 size_t n, double gravitational_constant, double* ax, double* ay,
-                                 double* az, cudaStream_t stream);
+/* a[i] = G * acc[inverse[i]] (acc: double4 per target in Morton order) */
+NBSP_HIDDEN void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n,
+                                double gravitational_constant, double* ax, double* ay,
+                                double* az, cudaStream_t stream);
 
 /* Copy node_count, leaf_count and depth of the tree to counters[2..4]. */
 NBSP_HIDDEN void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,

@@ -24,8 +24,9 @@ struct NbspBarnesHut {
     uint32_t* hist;
     void* pos4;
     void* tree;
-    void* acc_hi;
-    void* acc_lo;
+    void* acc;          /* double4 per target, Morton order */
+    void* unsorted;     /* float4 positions in input order */
+    uint32_t* inverse;  /* Morton slot of each input particle */
     unsigned long long* counters;       /* device */
     unsigned long long* host_counters;  /* pinned */
     cudaEvent_t events[BH_EVENTS];
@@ -62,13 +63,14 @@ static NBodySimProStatus bh_cuda(NBodySimProError* error, cudaError_t code, cons
 
 static void release_buffers(NbspBarnesHut* b) {
     void* buffers[] = {b->partial, b->geometry, b->keys, b->keys_alt, b->index, b->index_alt,
-                       b->hist, b->pos4, b->tree, b->acc_hi, b->acc_lo};
+                       b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->inverse};
     for (size_t k = 0; k < sizeof(buffers) / sizeof(buffers[0]); ++k) cudaFree(buffers[k]);
     b->partial = b->geometry = NULL;
     b->keys = b->keys_alt = NULL;
     b->index = b->index_alt = NULL;
     b->hist = NULL;
-    b->pos4 = b->tree = b->acc_hi = b->acc_lo = NULL;
+    b->pos4 = b->tree = b->acc = b->unsorted = NULL;
+    b->inverse = NULL;
     b->capacity = 0;
 }
 
@@ -107,8 +109,9 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
     BH_TRY(cudaMalloc((void**)&b->hist, nbsp_bh_sort_scratch_words(cap) * sizeof(uint32_t)));
     BH_TRY(cudaMalloc(&b->pos4, cap * 16));
     BH_TRY(cudaMalloc(&b->tree, nbsp_bh_tree_bytes(cap)));
-    BH_TRY(cudaMalloc(&b->acc_hi, cap * 16));
-    BH_TRY(cudaMalloc(&b->acc_lo, cap * 16));
+    BH_TRY(cudaMalloc(&b->acc, cap * 32));
+    BH_TRY(cudaMalloc(&b->unsorted, cap * 16));
+    BH_TRY(cudaMalloc((void**)&b->inverse, cap * sizeof(uint32_t)));
     b->capacity = cap;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
@@ -117,7 +120,8 @@ static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, i
                                 cudaStream_t stream) {
     nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status, stream);
     cudaEventRecord(b->events[1], stream);
-    nbsp_bh_keys(s->x, s->y, s->z, s->n, b->geometry, b->keys, b->index, b->hist, stream);
+    nbsp_bh_keys(s->x, s->y, s->z, s->m, s->n, b->geometry, b->keys, b->index, b->unsorted,
+                 b->hist, stream);
     cudaEventRecord(b->events[2], stream);
     nbsp_bh_sort(b->keys, b->index, b->keys_alt, b->index_alt, s->n, b->hist, status, stream);
     cudaEventRecord(b->events[3], stream);
@@ -146,18 +150,17 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     cudaEventRecord(b->events[0], stream);
     morton(b, s, status, stream);
     nbsp_bh_duplicates(b->keys, b->index, s->x, s->y, s->z, n, status, stream);
-    nbsp_bh_gather(s->x, s->y, s->z, s->m, b->index, n, b->geometry, b->pos4, status, stream);
+    nbsp_bh_gather(b->unsorted, b->index, n, b->pos4, b->inverse, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
     nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening, b->tree, status,
                     stream);
     cudaEventRecord(b->events[5], stream);
     nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode, p->correction,
-                 (float)p->softening_squared, b->acc_hi,
-                 b->acc_lo, b->counters, status, stream);
+                 (float)p->softening_squared, b->acc, b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
-    nbsp_bh_scatter(b->acc_hi, b->acc_lo, b->index, n, p->gravitational_constant, s->ax, s->ay,
-                    s->az, stream);
+    nbsp_bh_unsort(b->acc, b->inverse, n, p->gravitational_constant, s->ax, s->ay, s->az,
+                   stream);
     nbsp_bh_tree_counts(b->tree, n, b->counters, stream);
     cudaEventRecord(b->events[7], stream);
     BH_TRY(cudaGetLastError());
