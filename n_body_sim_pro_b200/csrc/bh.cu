@@ -1667,7 +1667,7 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
 // walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
 template <int ORDER, int STACK, bool CORR>
-__global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, CORR ? 2 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
     unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
@@ -1857,12 +1857,16 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
     const bool drain = top == 0;
     const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
     if (CORR && flush_cells) {
+      int nok = 0;  // cells the network corrects
       {
+        // Features of the listed cells; the cells the network may correct (in
+        // its training range, far enough from the group) are compacted into
+        // consecutive rows, so only those rows go through the network.
         uint32_t* xs = s_x[wib];
         float* ys = s_y[wib];
-        int* oks = s_ok[wib];
-        const int padded = (ncell + 15) & ~15;
-        for (int r = lane; r < padded; r += 32) {
+        int* oks = s_ok[wib];  // the cell's row, or -1 (plain monopole)
+        for (int r0 = 0; r0 < ncell; r0 += 32) {  // ncell < kListCap
+          const int r = r0 + lane;
           float f[nbsp_mlp::kIn];
           bool ok = false;
           if (r < ncell) {
@@ -1877,15 +1881,24 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
             for (int q = 0; q < nbsp_mlp::kIn; ++q)
               ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
           }
+          const unsigned okm = __ballot_sync(kFull, ok);
+          const int row = nok + __popc(okm & lt);
+          if (ok) {
 #pragma unroll
-          for (int w = 0; w < 8; ++w) {
-            const int q0 = 2 * w, q1 = 2 * w + 1;
-            const float v0 = ok && q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
-            const float v1 = ok && q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
-            xs[r * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
+            for (int w = 0; w < 8; ++w) {
+              const int q0 = 2 * w, q1 = 2 * w + 1;
+              const float v0 = q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
+              const float v1 = q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
+              xs[row * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
+            }
           }
-          oks[r] = ok ? 1 : 0;
+          if (r < ncell) oks[r] = ok ? row : -1;
+          nok += __popc(okm);
         }
+        const int padded = (nok + 15) & ~15;
+        for (int r = nok + lane; r < padded; r += 32)
+#pragma unroll
+          for (int w = 0; w < 8; ++w) xs[r * 8 + w] = 0u;
         __syncwarp();
         const int gq = lane >> 2, tq = lane & 3;
         for (int mt = 0; mt < padded / 16; ++mt) {
@@ -1905,29 +1918,32 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 3 : ORDER == 1 ? 8 : 5) w
         __syncwarp();
       }
       // Each cell becomes a correction source (centre of mass, Y = M y, or
-      // Y = 0 out of range) in a CorrTile, padded with far zero sources;
-      // every lane adds Y / |d|^2 for its own target, two cells per
-      // instruction.
-      CorrTile& ct = s_corr[CORR ? wib : 0];
-      const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
-      const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
-      for (int r = lane; r < kStage; r += 32) {
-        float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
-        float yx = 0.f, yy = 0.f, yz = 0.f;
-        if (r < ncell) {
-          c = t.com[cells[r]];
-          if (s_ok[wib][r]) {
-            const float* ye = &s_y[wib][r * 4];
-            yx = c.w * fmaf(ye[0], ys0, ym0);
-            yy = c.w * fmaf(ye[1], ys1, ym1);
-            yz = c.w * fmaf(ye[2], ys2, ym2);
+      // Y = 0 when the network does not correct it) in a CorrTile, padded
+      // with far zero sources; every lane adds Y / |d|^2 for its own target,
+      // two cells per instruction.
+      if (nok > 0) {
+        CorrTile& ct = s_corr[CORR ? wib : 0];
+        const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
+        const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
+        for (int r = lane; r < kStage; r += 32) {
+          float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
+          float yx = 0.f, yy = 0.f, yz = 0.f;
+          if (r < ncell) {
+            c = t.com[cells[r]];
+            const int row = s_ok[wib][r];
+            if (row >= 0) {
+              const float* ye = &s_y[wib][row * 4];
+              yx = c.w * fmaf(ye[0], ys0, ym0);
+              yy = c.w * fmaf(ye[1], ys1, ym1);
+              yz = c.w * fmaf(ye[2], ys2, ym2);
+            }
           }
+          stage_correction(ct, r, c, yx, yy, yz);
         }
-        stage_correction(ct, r, c, yx, yy, yz);
+        __syncwarp();
+        corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
+        __syncwarp();
       }
-      __syncwarp();
-      corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
-      __syncwarp();
     }
     if (CORR && flush_cells) ncell = 0;  // monopoles already staged, corrections applied
     if (nleaf >= 32 || (drain && nleaf > 0)) {
