@@ -1420,6 +1420,13 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 // the group centre, for cells whose distance from that centre exceeds the
 // group radius / kCorrGroup.
 constexpr float kCorrGroup = 0.3f;
+// Training pairs are the accepted cells with side / distance >= kCorrNear x
+// theta: the near cells, where the monopole's residual is largest.  The
+// trained feature range then excludes the far cells, so the walk leaves them
+// to the plain monopole (the fallback outside the training range); measured on
+// the 1M collision at theta 1.0 this both cuts the network evaluations and
+// lowers the rms error (7.7e-3 -> 5.6e-3 against 8.6e-3 uncorrected).
+constexpr float kCorrNear = 0.7f;
 
 // Training pairs: sample k picks a random target and, walking the tree with the
 // opening criterion at theta_train, one of the cells that target accepts and
@@ -1474,7 +1481,9 @@ __global__ void mlp_pairs_kernel(const float4* __restrict__ pos, int n, Tree t, 
       const bool pass = opening == NBSP_BH_OPENING_OFFSET ? d2 > ro * ro : s * s < th2 * d2;
       if (d2 > 0.f && pass && c.w > 0.f) {
         const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
-        if (kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2) {
+        const float near = kCorrNear * theta;
+        if (kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2 &&
+            s * s >= near * near * d2) {
           ++count;
           state = mix64(state + 0x9E3779B97F4A7C15ull);
           if (state % count == 0) chosen = node;
