@@ -157,31 +157,29 @@ __device__ __forceinline__ void forward_tile(const uint32_t* x, const uint2* w1,
       h1[4 * ks + 3] = bot;
     }
   }
-  uint32_t h2[16];
+  // layer 2 two n-tiles at a time: their GELU outputs are exactly the A
+  // fragment of one k-step of layer 3, consumed at once (4 registers live
+  // instead of the 16 of the whole hidden layer)
+  float o[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int ks3 = 0; ks3 < 4; ++ks3) {
+    uint32_t a3[4];
 #pragma unroll
-    for (int ks = 0; ks < 4; ++ks) mma_bf16(c, &h1[4 * ks], w2[(ks * 8 + nt) * 32 + lane]);
-    const float bb0 = b2[8 * nt + 2 * t], bb1 = b2[8 * nt + 2 * t + 1];
-    const uint32_t top = gelu2_bf16(c[0], c[1], bb0, bb1);
-    const uint32_t bot = gelu2_bf16(c[2], c[3], bb0, bb1);
-    const int ks = nt >> 1;
-    if ((nt & 1) == 0) {
-      h2[4 * ks + 0] = top;
-      h2[4 * ks + 1] = bot;
-    } else {
-      h2[4 * ks + 2] = top;
-      h2[4 * ks + 3] = bot;
+    for (int half = 0; half < 2; ++half) {
+      const int nt = 2 * ks3 + half;
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) mma_bf16(c, &h1[4 * ks], w2[(ks * 8 + nt) * 32 + lane]);
+      const float bb0 = b2[8 * nt + 2 * t], bb1 = b2[8 * nt + 2 * t + 1];
+      a3[2 * half] = gelu2_bf16(c[0], c[1], bb0, bb1);
+      a3[2 * half + 1] = gelu2_bf16(c[2], c[3], bb0, bb1);
     }
+    mma_bf16(o, a3, w3[ks3 * 32 + lane]);
   }
-  float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int ks = 0; ks < 4; ++ks) mma_bf16(c, &h2[4 * ks], w3[ks * 32 + lane]);
-  out[0] = c[0] + b3[2 * t];
-  out[1] = c[1] + b3[2 * t + 1];
-  out[2] = c[2] + b3[2 * t];
-  out[3] = c[3] + b3[2 * t + 1];
+  out[0] = o[0] + b3[2 * t];
+  out[1] = o[1] + b3[2 * t + 1];
+  out[2] = o[2] + b3[2 * t];
+  out[3] = o[3] + b3[2 * t + 1];
 }
 
 }  // namespace nbsp_mlp
