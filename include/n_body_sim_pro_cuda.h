@@ -247,6 +247,11 @@ typedef enum NBodySimProCudaWalk {
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(
     NBodySimProCudaContext* context, int walk, NBodySimProError* error);
 
+/* Largest particle count of one context: the radix sort's look-back counts
+ * are 30-bit and the kernels index particles with 32-bit integers.  (Device
+ * memory binds first: ~0.6 KB per particle for Barnes-Hut.) */
+#define N_BODY_SIM_PRO_CUDA_MAX_PARTICLES ((size_t)1073676288) /* 2^30 - 2^16 */
+
 /* Opening test of the Barnes-Hut walk (a target-cell pair at distance d from the
  * cell's centre of mass, cell side 2h):
  *   REFERENCE  accept when (2h)^2 < theta^2 d^2 (barnes_hut.c:596-599; default);

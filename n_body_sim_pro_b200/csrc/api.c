@@ -285,6 +285,9 @@ static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
 static NBodySimProStatus ensure_capacity(NBodySimProCudaContext* c, size_t n,
                                          NBodySimProError* error) {
+    if (n > N_BODY_SIM_PRO_CUDA_MAX_PARTICLES)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "more particles than N_BODY_SIM_PRO_CUDA_MAX_PARTICLES");
     if (n <= c->capacity && c->packed != NULL) return N_BODY_SIM_PRO_STATUS_OK;
     release_state(c);
     const size_t cap = n < 256 ? 256 : n;

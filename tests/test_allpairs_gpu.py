@@ -146,3 +146,17 @@ def test_precision_study_small(cuda, ctx):
     rms, mx = O.rms_relative_error(a, ref), vec_max_rel(a, ref)
     print(f"precision rms={rms:.3e} max={mx:.3e}")
     assert rms < 1e-5 and mx < 5e-4
+
+
+def test_particle_limit_is_checked_before_allocation(cuda, ctx):
+    """More than N_BODY_SIM_PRO_CUDA_MAX_PARTICLES (2^30 - 2^16: 30-bit sort
+    counts, 32-bit indices) is INVALID_ARGUMENT, not a failed allocation."""
+    import ctypes as C
+
+    null = C.POINTER(C.c_double)()
+    v = cuda.View((1 << 30) - (1 << 16) + 1, null, null, null, null, null, null, null, null,
+                  null, null)
+    err = cuda.Error()
+    rc = cuda.library().n_body_sim_pro_cuda_upload(ctx.handle, C.byref(v), C.byref(err))
+    assert rc == cuda.Status.INVALID_ARGUMENT
+    assert b"MAX_PARTICLES" in err.message
