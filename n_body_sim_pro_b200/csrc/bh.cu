@@ -1676,7 +1676,7 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
 // walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
 template <int ORDER, int STACK, bool CORR>
-__global__ void __launch_bounds__(kListThreads, CORR ? 2 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
     unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {

@@ -161,8 +161,8 @@ __device__ __forceinline__ void forward_tile(const uint32_t* x, const uint2* w1,
   // fragment of one k-step of layer 3, consumed at once (4 registers live
   // instead of the 16 of the whole hidden layer)
   float o[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int ks3 = 0; ks3 < 4; ++ks3) {
+#pragma unroll 1
+  for (int ks3 = 0; ks3 < 4; ++ks3) {  // not unrolled: 8 weight fragments in flight, not 32
     uint32_t a3[4];
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
