@@ -282,6 +282,13 @@ N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_timings(
 N_BODY_SIM_PRO_CUDA_API size_t n_body_sim_pro_cuda_context_walk_restarts(
     const NBodySimProCudaContext* context);
 
+/* No reference counterpart: in the last Barnes-Hut evaluation with a learned
+ * correction set, the number of (accepted cell, 32-target group) pairs the
+ * network evaluated (each one forward pass of 9,856 flop on the tensor cores).
+ * 0 for NULL or without a correction. */
+N_BODY_SIM_PRO_CUDA_API size_t n_body_sim_pro_cuda_context_corrected_cells(
+    const NBodySimProCudaContext* context);
+
 /* ---- force functions (NBodySimProForceFunction) -------------------------------- */
 
 /*

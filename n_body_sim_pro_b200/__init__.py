@@ -174,6 +174,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_reference_acceleration", "n_body_sim_pro_cuda_morton_order",
     "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
     "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
+    "n_body_sim_pro_cuda_context_corrected_cells",
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
     "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
@@ -224,6 +225,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
+        "n_body_sim_pro_cuda_context_corrected_cells": (C.c_size_t, [vp]),
         "n_body_sim_pro_cuda_preset_generate_parallel": (C.c_int, [vp, C.c_int,
                                                                    C.POINTER(C.c_size_t * 2), pe]),
         "n_body_sim_pro_cuda_checkpoint_write": (C.c_int, [vp, C.c_char_p,
@@ -490,6 +492,11 @@ class CudaContext:
         """Groups of the last Barnes-Hut evaluation that the interaction-list
         walk handed to the stackless walk (stack overflow)."""
         return int(library().n_body_sim_pro_cuda_context_walk_restarts(self.handle))
+
+    def corrected_cells(self) -> int:
+        """(cell, 32-target group) pairs the correction network evaluated in the
+        last Barnes-Hut evaluation."""
+        return int(library().n_body_sim_pro_cuda_context_corrected_cells(self.handle))
 
     def upload(self, system: ParticleSystem) -> None:
         err = Error()

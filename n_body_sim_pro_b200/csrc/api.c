@@ -113,6 +113,7 @@ struct NBodySimProCudaContext {
     NBodySimProBarnesHutStats stats;
     NBodySimProCudaTimings timings;
     size_t walk_restarts; /* groups the interaction-list walk handed to the stackless walk */
+    size_t corrected_cells; /* (cell, group) pairs the correction network evaluated */
 
     TuneEntry tune[TUNE_SLOTS];
     int tune_count;
@@ -273,6 +274,10 @@ size_t n_body_sim_pro_cuda_context_walk_restarts(const NBodySimProCudaContext* c
     return c == NULL ? 0 : c->walk_restarts;
 }
 
+size_t n_body_sim_pro_cuda_context_corrected_cells(const NBodySimProCudaContext* c) {
+    return c == NULL ? 0 : c->corrected_cells;
+}
+
 const char* n_body_sim_pro_cuda_architecture(void) { return "sm_100a"; }
 
 unsigned long long nbsp_kernel_launch_count = 0;
@@ -331,7 +336,7 @@ static NBodySimProStatus check_device_status(NBodySimProCudaContext* c, NBodySim
     CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (c->bh_pending) {
-        nbsp_bh_collect(c->bh, &c->stats, &c->timings, &c->walk_restarts);
+        nbsp_bh_collect(c->bh, &c->stats, &c->timings, &c->walk_restarts, &c->corrected_cells);
         c->bh_pending = 0;
     }
     const int bits = *c->host_status;

@@ -1645,7 +1645,9 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
+constexpr int kCorrRows = 96;      // corrected walk: network rows (< 32 waiting + < kListCap new)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
+constexpr int kCorrStack = 768;    // the corrected walk's (its network rows share the 48 KiB)
 
 // Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
 // traversal.  Each step the lanes pop up to 32 nodes from the warp's
@@ -1685,9 +1687,11 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
   __shared__ int s_pref[kListThreads / 32][kListCap];     // exclusive prefix of the counts
-  __shared__ uint32_t s_x[kListThreads / 32][CORR ? kListCap * 8 : 1];
-  __shared__ float s_y[kListThreads / 32][CORR ? kListCap * 4 : 1];
-  __shared__ int s_ok[kListThreads / 32][CORR ? kListCap : 1];
+  // corrected walk: network input rows waiting for a full tile, their cells,
+  // and the outputs of one run of the network
+  __shared__ uint32_t s_x[kListThreads / 32][CORR ? kCorrRows * 8 : 1];
+  __shared__ int s_row[kListThreads / 32][CORR ? kCorrRows : 1];
+  __shared__ float s_y[kListThreads / 32][CORR ? kStage * 4 : 1];
   // ORDER 1: accepted cells are point masses in the source tile (CORR: their
   // corrections come from a separate list); ORDER 2: cells fill a QuadTile
   static_assert(!(CORR && ORDER == 2), "the network corrects the monopole");
@@ -1697,6 +1701,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   SourceTile& src = s_src[wib];
   int staged = 0;   // sources waiting in src (warp-uniform)
+  int pending = 0;  // corrected walk: network rows waiting in s_x (warp-uniform)
   int qstaged = 0;  // cells waiting in the QuadTile (ORDER 2)
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
@@ -1866,93 +1871,102 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
     const bool drain = top == 0;
     const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
     if (CORR && flush_cells) {
-      int nok = 0;  // cells the network corrects
-      {
-        // Features of the listed cells; the cells the network may correct (in
-        // its training range, far enough from the group) are compacted into
-        // consecutive rows, so only those rows go through the network.
-        uint32_t* xs = s_x[wib];
-        float* ys = s_y[wib];
-        int* oks = s_ok[wib];  // the cell's row, or -1 (plain monopole)
-        for (int r0 = 0; r0 < ncell; r0 += 32) {  // ncell < kListCap
-          const int r = r0 + lane;
-          float f[nbsp_mlp::kIn];
-          bool ok = false;
-          if (r < ncell) {
-            const int node = cells[r];
-            const float4 c = t.com[node];
-            ok = cell_features(t, node, c, gx, gy, gz, f);
-            // the group centre must stand for every target: group radius
-            // below kCorrGroup of the distance, else the plain monopole
-            const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
-            ok = ok && kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2;
+      // Features of the listed cells; the cells the network may correct (in
+      // its training range, far enough from the group) are appended as rows
+      // to the warp's pending rows, so the network runs on full tiles.
+      uint32_t* xs = s_x[wib];
+      int* rows = s_row[wib];
+      int added = 0;
+      for (int r0 = 0; r0 < ncell; r0 += 32) {  // ncell < kListCap
+        const int r = r0 + lane;
+        float f[nbsp_mlp::kIn];
+        bool ok = false;
+        int node = 0;
+        if (r < ncell) {
+          node = cells[r];
+          const float4 c = t.com[node];
+          ok = cell_features(t, node, c, gx, gy, gz, f);
+          // the group centre must stand for every target: group radius
+          // below kCorrGroup of the distance, else the plain monopole
+          const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
+          ok = ok && kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2;
 #pragma unroll
-            for (int q = 0; q < nbsp_mlp::kIn; ++q)
-              ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
-          }
-          const unsigned okm = __ballot_sync(kFull, ok);
-          const int row = nok + __popc(okm & lt);
-          if (ok) {
-#pragma unroll
-            for (int w = 0; w < 8; ++w) {
-              const int q0 = 2 * w, q1 = 2 * w + 1;
-              const float v0 = q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
-              const float v1 = q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
-              xs[row * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
-            }
-          }
-          if (r < ncell) oks[r] = ok ? row : -1;
-          nok += __popc(okm);
+          for (int q = 0; q < nbsp_mlp::kIn; ++q)
+            ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
         }
-        const int padded = (nok + 15) & ~15;
-        for (int r = nok + lane; r < padded; r += 32)
+        const unsigned okm = __ballot_sync(kFull, ok);
+        const int row = pending + added + __popc(okm & lt);  // < kCorrRows
+        if (ok) {
 #pragma unroll
-          for (int w = 0; w < 8; ++w) xs[r * 8 + w] = 0u;
-        __syncwarp();
-        const int gq = lane >> 2, tq = lane & 3;
-        for (int mt = 0; mt < padded / 16; ++mt) {
-          const int ra = mt * 16 + gq, rb = ra + 8;
-          const uint32_t xa[4] = {xs[ra * 8 + tq], xs[rb * 8 + tq], xs[ra * 8 + tq + 4],
-                                  xs[rb * 8 + tq + 4]};
-          float out[4];
-          nbsp_mlp::forward_tile(xa, net->w1, net->b1, net->w2, net->b2, net->w3, net->b3, lane,
-                                 out);
-          if (tq < 2) {
-            ys[ra * 4 + 2 * tq] = out[0];
-            ys[ra * 4 + 2 * tq + 1] = out[1];
-            ys[rb * 4 + 2 * tq] = out[2];
-            ys[rb * 4 + 2 * tq + 1] = out[3];
+          for (int w = 0; w < 8; ++w) {
+            const int q0 = 2 * w, q1 = 2 * w + 1;
+            const float v0 = q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
+            const float v1 = q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
+            xs[row * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
           }
+          rows[row] = node;
         }
-        __syncwarp();
+        added += __popc(okm);
       }
-      // Each cell becomes a correction source (centre of mass, Y = M y, or
-      // Y = 0 when the network does not correct it) in a CorrTile, padded
-      // with far zero sources; every lane adds Y / |d|^2 for its own target,
-      // two cells per instruction.
-      if (nok > 0) {
-        CorrTile& ct = s_corr[CORR ? wib : 0];
-        const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
-        const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
-        for (int r = lane; r < kStage; r += 32) {
-          float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
-          float yx = 0.f, yy = 0.f, yz = 0.f;
-          if (r < ncell) {
-            c = t.com[cells[r]];
-            const int row = s_ok[wib][r];
-            if (row >= 0) {
-              const float* ye = &s_y[wib][row * 4];
-              yx = c.w * fmaf(ye[0], ys0, ym0);
-              yy = c.w * fmaf(ye[1], ys1, ym1);
-              yz = c.w * fmaf(ye[2], ys2, ym2);
-            }
-          }
-          stage_correction(ct, r, c, yx, yy, yz);
+      if (lane == 0 && added > 0) atomicAdd(&counters[6], (unsigned long long)added);
+      pending += added;
+      __syncwarp();
+    }
+    // Run the network on whole 16-row tiles of the pending rows (up to kStage
+    // at a time) once 32 are waiting, and on all of them when the walk ends;
+    // each corrected cell becomes a correction source (centre of mass, Y = M y)
+    // in a CorrTile padded with far zero sources, and every lane adds
+    // Y / |d|^2 for its own target, two cells per instruction.
+    while (CORR && (pending >= 32 || (drain && pending > 0))) {
+      uint32_t* xs = s_x[wib];
+      int* rows = s_row[wib];
+      float* ys = s_y[wib];
+      const int nrun = drain ? min(pending, kStage) : min(pending & ~15, kStage);
+      const int padded = (nrun + 15) & ~15;  // rows past nrun are free only when nrun = pending
+      for (int r = nrun + lane; r < padded; r += 32)
+#pragma unroll
+        for (int w = 0; w < 8; ++w) xs[r * 8 + w] = 0u;
+      __syncwarp();
+      const int gq = lane >> 2, tq = lane & 3;
+      for (int mt = 0; mt < padded / 16; ++mt) {
+        const int ra = mt * 16 + gq, rb = ra + 8;
+        const uint32_t xa[4] = {xs[ra * 8 + tq], xs[rb * 8 + tq], xs[ra * 8 + tq + 4],
+                                xs[rb * 8 + tq + 4]};
+        float out[4];
+        nbsp_mlp::forward_tile(xa, net->w1, net->b1, net->w2, net->b2, net->w3, net->b3, lane,
+                               out);
+        if (tq < 2) {
+          ys[ra * 4 + 2 * tq] = out[0];
+          ys[ra * 4 + 2 * tq + 1] = out[1];
+          ys[rb * 4 + 2 * tq] = out[2];
+          ys[rb * 4 + 2 * tq + 1] = out[3];
         }
-        __syncwarp();
-        corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
-        __syncwarp();
       }
+      __syncwarp();
+      CorrTile& ct = s_corr[CORR ? wib : 0];
+      const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
+      const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
+      for (int r = lane; r < kStage; r += 32) {
+        float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
+        float yx = 0.f, yy = 0.f, yz = 0.f;
+        if (r < nrun) {
+          c = t.com[rows[r]];
+          const float* ye = &ys[r * 4];
+          yx = c.w * fmaf(ye[0], ys0, ym0);
+          yy = c.w * fmaf(ye[1], ys1, ym1);
+          yz = c.w * fmaf(ye[2], ys2, ym2);
+        }
+        stage_correction(ct, r, c, yx, yy, yz);
+      }
+      __syncwarp();
+      corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
+      // the rows not run move to the front (destinations lie >= 16 rows below
+      // their sources, so no word is overwritten before it is read)
+      const int left = pending - nrun;
+      for (int k = lane; k < left * 8; k += 32) xs[k] = xs[k + nrun * 8];
+      for (int k = lane; k < left; k += 32) rows[k] = rows[k + nrun];
+      pending = left;
+      __syncwarp();
     }
     if (CORR && flush_cells) ncell = 0;  // monopoles already staged, corrections applied
     if (nleaf >= 32 || (drain && nleaf > 0)) {
@@ -2156,7 +2170,7 @@ void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int m
   if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
     if (net != nullptr) {  // the network corrects the monopole term
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true><<<blocks, kListThreads, 0, stream>>>(
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kCorrStack, true><<<blocks, kListThreads, 0, stream>>>(
           p, (int)n, t, eps2, out, counters, status, net);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(

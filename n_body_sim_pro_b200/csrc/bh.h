@@ -61,7 +61,8 @@ NBSP_HIDDEN NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** bh,
 /* After a stream synchronisation: fill stats / timings of the last evaluation
  * and the number of 32-target groups the interaction-list walk restarted. */
 NBSP_HIDDEN void nbsp_bh_collect(NbspBarnesHut* bh, NBodySimProBarnesHutStats* stats,
-                                 NBodySimProCudaTimings* timings, size_t* walk_restarts);
+                                 NBodySimProCudaTimings* timings, size_t* walk_restarts,
+                                 size_t* corrected_cells);
 
 /* Keys + sort only; copies the sorted keys / permutation / root to the host (synchronises). */
 NBSP_HIDDEN NBodySimProStatus nbsp_bh_morton(NbspBarnesHut** bh, const NbspBarnesHutState* s,

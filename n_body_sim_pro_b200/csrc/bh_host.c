@@ -183,7 +183,8 @@ static double elapsed(const NbspBarnesHut* b, int from, int to) {
 }
 
 void nbsp_bh_collect(NbspBarnesHut* b, NBodySimProBarnesHutStats* stats,
-                     NBodySimProCudaTimings* timings, size_t* walk_restarts) {
+                     NBodySimProCudaTimings* timings, size_t* walk_restarts,
+                     size_t* corrected_cells) {
     if (b == NULL || !b->timed) return;
     const unsigned long long* c = b->host_counters;
     stats->accepted_approximations = (size_t)c[0];
@@ -193,6 +194,7 @@ void nbsp_bh_collect(NbspBarnesHut* b, NBodySimProBarnesHutStats* stats,
     stats->internal_node_count = (size_t)(c[2] - c[3]);
     stats->maximum_depth = (size_t)c[4];
     *walk_restarts = (size_t)c[5];
+    *corrected_cells = (size_t)c[6];
     timings->bounds_ms = elapsed(b, 0, 1);
     timings->keys_ms = elapsed(b, 1, 2);
     timings->sort_ms = elapsed(b, 2, 3);

@@ -91,9 +91,15 @@ def test_correction_beats_plain_barnes_hut(cuda, trained):
     ctx.set_multipole_order(1)
     ctx.set_correction(None)
     plain = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)[targets].copy()
+    assert ctx.corrected_cells() == 0
     ctx.set_correction(corr)
     fixed = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)[targets].copy()
+    corrected = ctx.corrected_cells()
+    accepted = ctx.stats()["accepted_approximations"]
     ctx.set_correction(None)
+    # one network evaluation per corrected (cell, 32-target group) pair: never
+    # more than the accepted cells summed over all targets
+    assert 0 < corrected <= accepted
     e_plain = O.rms_relative_error(plain, ref)
     e_fixed = O.rms_relative_error(fixed, ref)
     print(f"theta=1.0 plain monopole rms={e_plain:.3e} corrected rms={e_fixed:.3e}")
@@ -117,5 +123,6 @@ def test_out_of_range_features_fall_back_to_plain(cuda, trained):
         empty.set_parameters(params, bad)
         ctx.set_correction(empty)
         guarded = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx).copy()
+        assert ctx.corrected_cells() == 0
         ctx.set_correction(None)
     assert np.array_equal(guarded, plain)
