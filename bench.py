@@ -96,6 +96,7 @@ PROFILED_TRAFFIC = {
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
 FLOPS_PAIR = 20          # standard convention per softened pair interaction
 FLOPS_QUAD = 58          # monopole + trace-free quadrupole per accepted cell
+MLP_FLOPS = 2 * (10 * 64 + 64 * 64 + 64 * 3)  # 9,856: one forward pass of the 10-64-64-3 network
 
 
 # ---------------------------------------------------------------------------
@@ -548,6 +549,8 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
                 cctx.set_correction(corr)
                 cctx.upload(system)
                 rms_c = rms_at_targets(nb, cctx, g, n, targets, ref)
+                evals = cctx.corrected_cells()  # network evaluations of that walk
+                walk_ms = cctx.timings()["walk_ms"]
                 cctx.close()
                 v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush,
                                     correction=corr, opening=opening)
@@ -555,6 +558,10 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
                 "theta": 1.0, "opening": oname, "rms": rms_c, "value": v,
                 "ms_per_step": round(ms, 4),
                 "uncorrected_rms_at_theta_1.0": dict(table[(1, oname)])[1.0],
+                "network": {"evaluations_per_walk": evals, "flop_per_evaluation": MLP_FLOPS,
+                            "walk_ms": round(walk_ms, 4),
+                            "tensor_tflops_in_walk": round(evals * MLP_FLOPS / (walk_ms * 1e-3)
+                                                           / 1e12, 3) if walk_ms > 0 else None},
                 "training": {"pairs": 1 << 22, "from": "collision N=1M", "epochs": 8,
                              "final_validation_loss": float(vl[-1]),
                              "seconds": round(train_s, 2)}}
