@@ -19,9 +19,11 @@ over the ranks with an NCCL all-gather of the packed sources every step;
 initial state, the rms relative force error against the FP64 direct sum on
 4096 seeded targets is measured over a theta grid for the monopole and the
 quadrupole walk under the reference's opening test and under the offset test;
-each method is then timed at the largest theta whose error is at most 1e-3.
-"plain" is the monopole walk with the reference's test, "chosen" the fastest
-method.  ``bh_matched_10m`` adds the plain walk at theta 0.5 and the learned
+each method is then timed at the largest theta whose error is at most 1e-3;
+the relative opening test (G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)
+with the reference's test at theta 1.0 as the safety bound) is swept over
+alpha the same way.  "plain" is the monopole walk with the reference's test,
+"chosen" the fastest method.  ``bh_matched_10m`` adds the plain walk at theta 0.5 and the learned
 correction at theta 1.0 under both opening tests (network trained on 2^22
 cell-target pairs of the 1M collision).
 
@@ -467,10 +469,12 @@ def rms_at_targets(nb, ctx, g, n, targets, ref):
 
 
 def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None,
-                opening=0):
-    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order, opening)."""
+                opening=0, alpha=0.0):
+    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order, opening,
+    relative tolerance alpha)."""
     ctx = nb.CudaContext(theta=theta, multipole_order=order, opening=opening)
     ctx.set_correction(correction)
+    ctx.set_relative_opening(alpha)
     ctx.upload(system)
     for _ in range(warmup):
         ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
@@ -485,6 +489,9 @@ def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, co
 
 
 OPENINGS = {"reference": 0, "offset": 1}
+# relative opening test (G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)) over the
+# reference test at theta 1.0: the alphas of its sweep
+ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.005, 0.007, 0.01)
 
 
 def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
@@ -509,11 +516,24 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
                 ctx.theta = th
                 rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
             table[(order, oname)] = rows
+    # relative test: each alpha evaluated twice, the second walk reading the
+    # first one's accelerations as a_old (as in a run, where a_old is the
+    # previous step's)
+    ctx.set_opening(0)
+    ctx.set_multipole_order(1)
+    ctx.theta = 1.0
+    rel_rows = []
+    for alpha in ALPHA_GRID:
+        ctx.set_relative_opening(alpha)
+        ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+        rel_rows.append((alpha, rms_at_targets(nb, ctx, g, n, targets, ref)))
+    ctx.set_relative_opening(0.0)
     ctx.close()
     out = {"rms_target": RMS_TARGET, "oracle": "FP64 device direct sum, 4096 seeded targets, "
            "initial state",
            "sweep": {f"order{o}_{on}": [[t, round(r, 6)] for t, r in rows]
                      for (o, on), rows in table.items()}}
+    out["sweep"]["order1_relative_alpha_theta1.0"] = [[a, round(r, 6)] for a, r in rel_rows]
     methods = {}
     for (order, oname), rows in table.items():
         ok = [t for t, r in rows if r <= RMS_TARGET]
@@ -525,6 +545,13 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
         methods[(order, oname)] = {"theta": th, "multipole_order": order, "opening": oname,
                                    "rms": dict(rows)[th], "value": v,
                                    "ms_per_step": round(ms, 4)}
+    ok = [a for a, r in rel_rows if r <= RMS_TARGET]
+    if ok:
+        alpha = max(ok)
+        v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush, alpha=alpha)
+        methods[(1, "relative")] = {"theta": 1.0, "multipole_order": 1, "opening": "reference",
+                                    "relative_alpha": alpha, "rms": dict(rel_rows)[alpha],
+                                    "value": v, "ms_per_step": round(ms, 4)}
     out["methods"] = list(methods.values())
     out["plain"] = methods.get((1, "reference"))
     out["chosen"] = max(methods.values(), key=lambda m: m["value"]) if methods else None

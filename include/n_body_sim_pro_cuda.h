@@ -267,6 +267,17 @@ typedef enum NBodySimProCudaOpening {
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_opening(
     NBodySimProCudaContext* context, int opening, NBodySimProError* error);
 
+/* No reference counterpart: the relative opening test (Springel 2001) on top of
+ * the geometric one.  With alpha > 0 a cell of mass M and side 2h is accepted
+ * for a target only when also  G M (2h)^2 / d^4 <= alpha |a_old|,  a_old the
+ * target's acceleration in the state (the previous evaluation's, or what was
+ * uploaded / passed in the view); targets with a_old = 0 use the geometric
+ * test alone.  theta (with OFFSET, 1.0 keeps every target outside the cells it
+ * accepts) becomes the safety bound.  0 (default) turns it off.  Not combined
+ * with a learned correction, which keeps the geometric test it was trained on. */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_opening(
+    NBodySimProCudaContext* context, double alpha, NBodySimProError* error);
+
 /* Replaces n_body_sim_pro_barnes_hut_tree_stats (barnes_hut/barnes_hut.h:116-117):
  * 0 on success, non-zero when an argument is NULL. */
 N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_stats(

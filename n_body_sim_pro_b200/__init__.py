@@ -174,7 +174,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_reference_acceleration", "n_body_sim_pro_cuda_morton_order",
     "n_body_sim_pro_cuda_synchronize", "n_body_sim_pro_cuda_architecture",
     "n_body_sim_pro_cuda_kernel_launches", "n_body_sim_pro_cuda_context_walk_restarts",
-    "n_body_sim_pro_cuda_context_corrected_cells",
+    "n_body_sim_pro_cuda_context_corrected_cells", "n_body_sim_pro_cuda_context_set_relative_opening",
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
     "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
@@ -222,6 +222,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_set_leaf_capacity": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_walk": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_opening": (st, [vp, C.c_int, pe]),
+        "n_body_sim_pro_cuda_context_set_relative_opening": (st, [vp, C.c_double, pe]),
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
@@ -440,6 +441,13 @@ class CudaContext:
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_opening(self.handle, int(opening),
                                                                  C.byref(err)), err)
+
+    def set_relative_opening(self, alpha: float) -> None:
+        """Relative opening test G M (2h)^2 / d^4 <= alpha |a_old| on top of the
+        geometric one (alpha 0: off)."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_relative_opening(
+            self.handle, float(alpha), C.byref(err)), err)
 
     def set_correction(self, correction: "CudaCorrection | None") -> None:
         err = Error()

@@ -106,6 +106,7 @@ struct NBodySimProCudaContext {
     int leaf_capacity;
     int walk_mode;
     int opening;
+    double tolerance; /* alpha of the relative opening test; 0: off */
     const void* correction; /* device network of the learned correction, or NULL */
     NbspBarnesHut* bh;
     int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
@@ -245,6 +246,16 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_opening(NBodySimProCudaContext
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown opening criterion");
     c->opening = opening == N_BODY_SIM_PRO_CUDA_OPENING_OFFSET ? NBSP_BH_OPENING_OFFSET
                                                               : NBSP_BH_OPENING_REFERENCE;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_opening(NBodySimProCudaContext* c,
+                                                                  double alpha,
+                                                                  NBodySimProError* error) {
+    if (c == NULL || !(alpha >= 0.0) || !isfinite(alpha))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "relative opening tolerance must be finite and >= 0");
+    c->tolerance = alpha;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
@@ -504,6 +515,7 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.leaf_capacity = c->leaf_capacity;
         p.walk_mode = c->walk_mode;
         p.opening = c->opening;
+        p.tolerance = c->tolerance;
         p.correction = c->correction;
         NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
         c->bh_pending = 1;
@@ -590,6 +602,20 @@ static NBodySimProStatus view_force(const NBodySimProParticleSystemView* view,
     c->n_padded = round_up(n, 256);
     c->resident = 0; /* the plugin path only stages positions and masses */
     if ((st = copy_in(c, view, 0, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && c->tolerance > 0.0) {
+        /* the relative opening test reads the view's previous accelerations */
+        const size_t bytes = n * sizeof(double);
+        double* dst[3] = {c->ax, c->ay, c->az};
+        const double* src[3] = {view->accelerations_x, view->accelerations_y,
+                                view->accelerations_z};
+        for (int k = 0; k < 3; ++k) {
+            if (src[k] != NULL)
+                CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyHostToDevice,
+                                         c->stream));
+            else
+                CUDA_TRY(cudaMemsetAsync(dst[k], 0, bytes, c->stream));
+        }
+    }
     CUDA_TRY(cudaEventRecord(c->events[0], c->stream));
     if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
         return st;

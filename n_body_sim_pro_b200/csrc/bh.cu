@@ -37,14 +37,16 @@ constexpr unsigned kFull = 0xffffffffu;
 
 constexpr int kBoundsThreads = 256;
 constexpr int kBoundsBlocks = 1024;
-constexpr int kBoundsVals = 10;  // min xyz, max xyz, m, mx, my, mz
+constexpr int kBoundsVals = 11;  // min xyz, max xyz, m, mx, my, mz, |a|^2
 
 __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
-    const double* __restrict__ m, size_t n, double* __restrict__ partial, int* status) {
+    const double* __restrict__ m, size_t n, double* __restrict__ partial, int* status,
+    const double* __restrict__ ax, const double* __restrict__ ay,
+    const double* __restrict__ az) {
   __shared__ double sh[kBoundsVals][kBoundsThreads];
   double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
-                           0.0,      0.0,      0.0,      0.0};
+                           0.0,      0.0,      0.0,      0.0,       0.0};
   bool bad = false;
   for (size_t i = blockIdx.x * (size_t)kBoundsThreads + threadIdx.x; i < n;
        i += (size_t)gridDim.x * kBoundsThreads) {
@@ -60,6 +62,7 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
     v[7] += pm * px;
     v[8] += pm * py;
     v[9] += pm * pz;
+    if (ax != nullptr) v[10] += ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i];
   }
   if (bad) atomicOr(status, NBSP_DEVICE_ERROR_NONFINITE_POSITION);
   const int t = threadIdx.x;
@@ -78,10 +81,10 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
 
 // Root cube with the exact FP64 operation sequence of barnes_hut.c:471-483.
 __global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
-    const double* __restrict__ partial, int blocks, double* __restrict__ geometry) {
+    const double* __restrict__ partial, int blocks, size_t n, double* __restrict__ geometry) {
   __shared__ double sh[kBoundsVals][kBoundsThreads];
   double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
-                           0.0,      0.0,      0.0,      0.0};
+                           0.0,      0.0,      0.0,      0.0,       0.0};
   for (int b = threadIdx.x; b < blocks; b += kBoundsThreads) {
     for (int q = 0; q < 3; ++q) v[q] = fmin(v[q], partial[b * kBoundsVals + q]);
     for (int q = 3; q < 6; ++q) v[q] = fmax(v[q], partial[b * kBoundsVals + q]);
@@ -112,6 +115,7 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
     geometry[3] = half;
     const double mt = sh[6][0];
     for (int k = 0; k < 3; ++k) geometry[4 + k] = mt != 0.0 ? sh[7 + k][0] / mt : 0.0;
+    geometry[7] = n > 0 ? sqrt(sh[10][0] / (double)n) : 0.0;  // rms |a| (when given)
   }
 }
 
@@ -189,12 +193,14 @@ __global__ void __launch_bounds__(256) keys_kernel(
     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
     const double* __restrict__ m, size_t n, const double* __restrict__ geometry,
     uint64_t* __restrict__ keys, uint32_t* __restrict__ index, float4* __restrict__ unsorted,
-    uint32_t* __restrict__ hist) {
+    uint32_t* __restrict__ hist, const double* __restrict__ ax, const double* __restrict__ ay,
+    const double* __restrict__ az, double tol_scale, float* __restrict__ unsorted_tol) {
   __shared__ uint32_t h[kSortPasses][kRadix];
   for (int k = threadIdx.x; k < kSortPasses * kRadix; k += blockDim.x) (&h[0][0])[k] = 0;
   __syncthreads();
   const double cx = geometry[0], cy = geometry[1], cz = geometry[2], hs = geometry[3];
   const double mx = geometry[4], my = geometry[5], mz = geometry[6];  // centre of mass
+  const double a_floor = geometry[7];  // rms |a_old|: the relative test's floor
   const unsigned lane = threadIdx.x & 31;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const size_t first = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -214,6 +220,10 @@ __global__ void __launch_bounds__(256) keys_kernel(
       // order: the gather then moves one 16-byte record per particle
       unsorted[i] = make_float4((float)__dsub_rn(xi, mx), (float)__dsub_rn(yi, my),
                                 (float)__dsub_rn(zi, mz), (float)m[i]);
+      if (unsorted_tol != nullptr) {  // relative opening test: alpha max(|a_old|, rms) / G
+        const double a = fmax(sqrt(ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i]), a_floor);
+        unsorted_tol[i] = a > 0.0 && isfinite(a) ? (float)(tol_scale * a) : INFINITY;
+      }
     }
 #pragma unroll
     // digit counts: the low six bytes of the keys of one warp are spread over
@@ -415,10 +425,12 @@ __global__ void duplicates_kernel(const uint64_t* __restrict__ keys,
 // gather / scatter
 // ---------------------------------------------------------------------------
 
-// pos[s] = unsorted[perm[s]]; inverse[perm[s]] = s (for the unsort).
+// pos[s] = unsorted[perm[s]]; inverse[perm[s]] = s (for the unsort); the
+// relative opening test's tolerances the same way when present.
 __global__ void gather_kernel(const float4* __restrict__ unsorted,
                               const uint32_t* __restrict__ perm, size_t n,
                               float4* __restrict__ pos, uint32_t* __restrict__ inverse,
+                              const float* __restrict__ unsorted_tol, float* __restrict__ tol,
                               int* status) {
   for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
        s += (size_t)gridDim.x * blockDim.x) {
@@ -430,6 +442,7 @@ __global__ void gather_kernel(const float4* __restrict__ unsorted,
     }
     pos[s] = unsorted[i];
     inverse[i] = (uint32_t)s;
+    if (tol != nullptr) tol[s] = unsorted_tol[i];
   }
 }
 
@@ -481,6 +494,7 @@ struct Tree {
   float* side;        // cell side 2h = root side / 2^level
   float* spread;      // sum m |x - com|^2 / (M side^2): the correction MLP's 10th feature
   float* shift;       // distance from the cell's geometric centre to its centre of mass
+  float* kmass;       // M side^2: the relative opening test's cell term
   unsigned long long* leaves;  // [1]
 };
 
@@ -524,6 +538,7 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.side = carve<float>(p, nb);
   t.spread = carve<float>(p, nb);
   t.shift = carve<float>(p, nb);
+  t.kmass = carve<float>(p, nb);
   t.leaves = carve<unsigned long long>(p, 1);
   if (end != nullptr) *end = p;
   return t;
@@ -806,6 +821,7 @@ __device__ void finish_node(const Tree& t, int node, const Moments& mo, int firs
   t.ropen2[node] = (float)r2;
   t.side[node] = (float)side;
   t.shift[node] = (float)shift;
+  t.kmass[node] = (float)(mo.m * side * side);
   t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
   t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
   t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
@@ -991,15 +1007,26 @@ constexpr int kWalkThreads = 256;
 // accepts), otherwise all lanes apply its multipole and skip its subtree.
 // Buckets (leaves of up to leaf_capacity particles) take the same test and are
 // summed particle by particle when it fails; single particles are always exact.
+// Opening test of a (node, target) pair at squared distance d2 from the node's
+// centre of mass: the geometric test (d2 > ro, ro = the node's opening radius
+// squared) and, with REL, the relative test G M side^2 / d^4 <= alpha |a_old|,
+// i.e. M side^2 <= tol d^4 with tol = alpha |a_old| / G per target (Springel
+// 2001); tol = +inf (no previous acceleration) leaves the geometric test.
+template <bool REL>
+__device__ __forceinline__ bool opening_passes(float d2, float ro, float km, float tol) {
+  return d2 > ro && (!REL || d2 * d2 * tol >= km);
+}
+
 struct WalkAcc {
   float hx, hy, hz, lx, ly, lz;  // compensated acceleration / G
   unsigned approx, exact;        // accepted cells, particle-particle terms
 };
 
-template <int ORDER>
+template <int ORDER, bool REL>
 __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, int n,
                                                const Tree& t, float eps2, int s, bool active,
-                                               float4 p, int lane, int* status, WalkAcc& out) {
+                                               float4 p, float tol, int lane, int* status,
+                                               WalkAcc& out) {
   const int total = (int)t.offset[n];
   const int limit = 2 * total + 64;
 
@@ -1025,7 +1052,8 @@ __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, i
       const float4 c = t.com[node];
       const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      direct = __any_sync(kFull, active && !(d2 > t.ropen2[node]));
+      direct = __any_sync(kFull, active && !opening_passes<REL>(d2, t.ropen2[node],
+                                                               REL ? t.kmass[node] : 0.f, tol));
     }
     if (direct) {
       const int j1 = info.y + info.z;
@@ -1046,7 +1074,8 @@ __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, i
       const float4 c = t.com[node];
       const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const bool open = active && !(d2 > t.ropen2[node]);
+      const bool open =
+          active && !opening_passes<REL>(d2, t.ropen2[node], REL ? t.kmass[node] : 0.f, tol);
       if (__any_sync(kFull, open)) {
         node = node + 1;
         continue;
@@ -1119,18 +1148,19 @@ __device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active,
   }
 }
 
-template <int ORDER>
+template <int ORDER, bool REL>
 __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
-    const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
-    unsigned long long* __restrict__ counters, int* status) {
+    const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
+    double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
   const int s = warp * 32 + lane;
   const bool active = s < n;
   const float4 p = pos[active ? s : n - 1];
+  const float tl = REL ? tol[active ? s : n - 1] : 0.f;
   WalkAcc a;
-  stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
+  stackless_walk<ORDER, REL>(pos, n, t, eps2, s, active, p, tl, lane, status, a);
   store_walk(a, s, active, lane, acc, counters);
 }
 
@@ -1677,12 +1707,14 @@ constexpr int kCorrStack = 768;    // the corrected walk's (its network rows sha
 // stand for all 32 targets), keep the plain monopole.
 // Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
 // walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
-template <int ORDER, int STACK, bool CORR>
+template <int ORDER, int STACK, bool CORR, bool REL>
 __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
-    const float4* __restrict__ pos, int n, Tree t, float eps2, double4* __restrict__ acc,
-    unsigned long long* __restrict__ counters, int* status,
+    const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
+    double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net) {
+  static_assert(!(CORR && REL), "the network corrects cells the geometric test accepts");
   __shared__ int s_stack[kListThreads / 32][STACK];
+  __shared__ float s_probe_k[kListThreads / 32][REL ? 32 : 1];  // their M side^2
   __shared__ int s_cells[kListThreads / 32][CORR ? kListCap : 1];
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
@@ -1713,6 +1745,11 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
   const float4 p = pos[active ? s : n - 1];
   const unsigned lt = (1u << lane) - 1u;
   const bool guard = !__all_sync(kFull, !active || self_term_is_finite(p.w, eps2));
+  // relative test: this lane's tolerance and the group's smallest (the box
+  // test stands for every target only with the least tolerant one)
+  float tl = REL && active ? tol[s] : INFINITY, tmin = tl;
+  if (REL)
+    for (int off = 16; off > 0; off >>= 1) tmin = fminf(tmin, __shfl_xor_sync(kFull, tmin, off));
 
   // group bounding box
   float bx0 = p.x, bx1 = p.x, by0 = p.y, by1 = p.y, bz0 = p.z, bz1 = p.z;
@@ -1749,7 +1786,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
       int kids = 0;
       int4 info = make_int4(0, 0, 0, 0);
       float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
-      float ro = 0.f;
+      float ro = 0.f, km = 0.f;
       int4 ca = make_int4(-1, -1, -1, -1), cb = make_int4(-1, -1, -1, -1);
       if (node >= total) {
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
@@ -1761,6 +1798,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
         info = t.info[at];
         c = t.com[at];
         ro = t.ropen2[at];
+        if (REL) km = t.kmass[at];
         const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
         if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         const bool ok = valid && !bad;
@@ -1770,24 +1808,26 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
         const float qz = fmaxf(fabsf(c.z - gz) - ez, 0.f);
         const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
         const bool cellish = ok && info.z != 1;
-        accept = cellish && dmin2 > ro;
-        test = cellish && !(dmin2 > ro);
+        const bool box = opening_passes<REL>(dmin2, ro, km, tmin);
+        accept = cellish && box;
+        test = cellish && !box;
       }
       // Nodes the box could not accept: a node that fails this lane's own
       // target is opened at once; for the rest every target's own test
       // decides, one node at a time with the 32 targets tested in parallel.
-      const bool opened = test && active && !(fmaf(c.x - p.x, c.x - p.x,
-                                                   fmaf(c.y - p.y, c.y - p.y,
-                                                        (c.z - p.z) * (c.z - p.z))) > ro);
+      const float d2own = fmaf(c.x - p.x, c.x - p.x, fmaf(c.y - p.y, c.y - p.y, (c.z - p.z) * (c.z - p.z)));
+      const bool opened = test && active && !opening_passes<REL>(d2own, ro, km, tl);
       test = test && !opened;
       float4* probe = s_probe[wib];
       if (test) probe[lane] = make_float4(c.x, c.y, c.z, ro);
+      if (REL && test) s_probe_k[wib][lane] = km;
       __syncwarp();
       for (unsigned pend = __ballot_sync(kFull, test); pend != 0u; pend &= pend - 1u) {
         const int from = __ffs(pend) - 1;
         const float4 q = probe[from];
         const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-        const bool fail = active && !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > q.w);
+        const bool fail = active && !opening_passes<REL>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), q.w,
+                                                         REL ? s_probe_k[wib][from] : 0.f, tl);
         const bool any = __any_sync(kFull, fail);
         if (lane == from) accept = !any;
       }
@@ -2031,7 +2071,7 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
   WalkAcc a;
   if (overflow) {
     if (lane == 0) atomicAdd(&counters[5], 1ull);  // groups walked again
-    stackless_walk<ORDER>(pos, n, t, eps2, s, active, p, lane, status, a);
+    stackless_walk<ORDER, REL>(pos, n, t, eps2, s, active, p, tl, lane, status, a);
   } else {
     a.hx = hx;
     a.hy = hy;
@@ -2059,31 +2099,64 @@ int grid_for(size_t n, int threads) {
   return (int)b;
 }
 
+template <bool REL>
+void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order, int mode,
+                 const nbsp_mlp::Net* net, float eps2, double4* out, unsigned long long* counters,
+                 int* status, cudaStream_t stream) {
+  if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
+    const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
+    if (!REL && net != nullptr) {  // the network corrects the monopole term
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kCorrStack, true, false><<<blocks, kListThreads, 0, stream>>>(
+          p, tol, (int)n, t, eps2, out, counters, status, net);
+    } else if (order == 2) {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
+          p, tol, (int)n, t, eps2, out, counters, status, nullptr);
+    } else {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
+          p, tol, (int)n, t, eps2, out, counters, status, nullptr);
+    }
+    return;
+  }
+  const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
+  if (order == 2) {
+    NBSP_COUNT_LAUNCH(1), walk_kernel<2, REL><<<blocks, kWalkThreads, 0, stream>>>(
+        p, tol, (int)n, t, eps2, out, counters, status);
+  } else {
+    NBSP_COUNT_LAUNCH(1), walk_kernel<1, REL><<<blocks, kWalkThreads, 0, stream>>>(
+        p, tol, (int)n, t, eps2, out, counters, status);
+  }
+}
+
 }  // namespace
 
 extern "C" {
 
 void nbsp_bh_bounds(const double* x, const double* y, const double* z, const double* m, size_t n,
-                    double* partial, double* geometry, int* status, cudaStream_t stream) {
+                    double* partial, double* geometry, int* status, const double* ax,
+                    const double* ay, const double* az, cudaStream_t stream) {
   size_t blocks = (n + kBoundsThreads - 1) / kBoundsThreads;
   if (blocks < 1) blocks = 1;
   if (blocks > (size_t)kBoundsBlocks) blocks = kBoundsBlocks;
-  NBSP_COUNT_LAUNCH(1), bounds_kernel<<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(x, y, z, m, n, partial, status);
-  NBSP_COUNT_LAUNCH(1), bounds_final_kernel<<<1, kBoundsThreads, 0, stream>>>(partial, (int)blocks, geometry);
+  NBSP_COUNT_LAUNCH(1), bounds_kernel<<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(x, y, z, m, n, partial, status,
+                                                                   ax, ay, az);
+  NBSP_COUNT_LAUNCH(1), bounds_final_kernel<<<1, kBoundsThreads, 0, stream>>>(partial, (int)blocks,
+                                                                            n, geometry);
 }
 
 size_t nbsp_bh_sort_scratch_words(size_t n) { return sort_scratch_words(n); }
 
 void nbsp_bh_keys(const double* x, const double* y, const double* z, const double* m, size_t n,
                   const double* geometry, uint64_t* keys, uint32_t* index, void* unsorted,
-                  uint32_t* scratch, cudaStream_t stream) {
+                  uint32_t* scratch, const double* ax, const double* ay, const double* az,
+                  double tol_scale, float* unsorted_tol, cudaStream_t stream) {
   cudaMemsetAsync(scratch, 0, sort_scratch_words(n) * sizeof(uint32_t), stream);
   const SortScratch sc = sort_scratch(scratch, n);
   size_t blocks = (n + 255) / 256;
   if (blocks < 1) blocks = 1;
   if (blocks > (size_t)kKeysBlocks) blocks = kKeysBlocks;
   NBSP_COUNT_LAUNCH(1), keys_kernel<<<(unsigned)blocks, 256, 0, stream>>>(
-      x, y, z, m, n, geometry, keys, index, (float4*)unsorted, sc.hist);
+      x, y, z, m, n, geometry, keys, index, (float4*)unsorted, sc.hist, ax, ay, az, tol_scale,
+      unsorted_tol);
 }
 
 void nbsp_bh_sort(uint64_t* keys, uint32_t* index, uint64_t* keys_alt, uint32_t* index_alt,
@@ -2118,9 +2191,10 @@ void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double
 }
 
 void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
-                    uint32_t* inverse, int* status, cudaStream_t stream) {
+                    uint32_t* inverse, const float* unsorted_tol, float* tol, int* status,
+                    cudaStream_t stream) {
   NBSP_COUNT_LAUNCH(1), gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
-      (const float4*)unsorted, perm, n, (float4*)pos4, inverse, status);
+      (const float4*)unsorted, perm, n, (float4*)pos4, inverse, unsorted_tol, tol, status);
 }
 
 size_t nbsp_bh_tree_bytes(size_t n) { return tree_bytes(n); }
@@ -2160,35 +2234,17 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
                                                                    o, status);
 }
 
-void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
-                  const void* correction, float eps2, void* acc,
+void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree, int order,
+                  int mode, const void* correction, float eps2, void* acc,
                   unsigned long long* counters, int* status, cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
   const float4* p = (const float4*)pos4;
   double4* out = (double4*)acc;
-  if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
-    const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
-    if (net != nullptr) {  // the network corrects the monopole term
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kCorrStack, true><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, out, counters, status, net);
-    } else if (order == 2) {
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, out, counters, status, nullptr);
-    } else {
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false><<<blocks, kListThreads, 0, stream>>>(
-          p, (int)n, t, eps2, out, counters, status, nullptr);
-    }
-    return;
-  }
-  const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
-  if (order == 2) {
-    NBSP_COUNT_LAUNCH(1), walk_kernel<2><<<blocks, kWalkThreads, 0, stream>>>(p, (int)n, t, eps2,
-                                                                            out, counters, status);
-  } else {
-    NBSP_COUNT_LAUNCH(1), walk_kernel<1><<<blocks, kWalkThreads, 0, stream>>>(p, (int)n, t, eps2,
-                                                                            out, counters, status);
-  }
+  if (tol != nullptr && net == nullptr)
+    launch_walk<true>(p, tol, n, t, order, mode, net, eps2, out, counters, status, stream);
+  else
+    launch_walk<false>(p, nullptr, n, t, order, mode, net, eps2, out, counters, status, stream);
 }
 
 void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n, double g, double* ax,

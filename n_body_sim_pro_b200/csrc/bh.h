@@ -38,6 +38,7 @@ typedef struct NbspBarnesHutParams {
     int leaf_capacity;
     int walk_mode;
     int opening;            /* NBSP_BH_OPENING_* */
+    double tolerance;       /* alpha of the relative opening test; 0: geometric test alone */
     const void* correction; /* device network (mlp.cuh Net) or NULL */
 } NbspBarnesHutParams;
 
@@ -78,14 +79,21 @@ NBSP_HIDDEN void nbsp_bh_destroy(NbspBarnesHut* bh);
  * with the reference), geometry[4..6] = centre of mass.  partial >= 1024*10 doubles. */
 NBSP_HIDDEN void nbsp_bh_bounds(const double* x, const double* y, const double* z,
                                 const double* m, size_t n, double* partial, double* geometry,
-                                int* status, cudaStream_t stream);
+                                int* status, const double* ax, const double* ay, const double* az,
+                                cudaStream_t stream);
+/* geometry: root centre [0..2], half side [3], centre of mass [4..6], and rms
+ * |a| [7] of (ax, ay, az) when they are given (the relative test's floor) */
 
 /* Morton keys, the identity index, the 8 digit histograms (into sort_scratch)
  * and the walk's float4 (x - c, y - c, z - c, m) with c the centre of mass, in
  * input order (`unsorted`, n entries). */
 NBSP_HIDDEN void nbsp_bh_keys(const double* x, const double* y, const double* z, const double* m,
                               size_t n, const double* geometry, uint64_t* keys, uint32_t* index,
-                              void* unsorted, uint32_t* sort_scratch, cudaStream_t stream);
+                              void* unsorted, uint32_t* sort_scratch, const double* ax,
+                              const double* ay, const double* az, double tol_scale,
+                              float* unsorted_tol, cudaStream_t stream);
+/* (with unsorted_tol != NULL also the relative opening test's tolerance of each
+ * particle, tol_scale |a| from the previous accelerations, +inf where |a| = 0) */
 
 /* 32-bit words of sort scratch for n keys (digit histograms, pass bases, tile
  * tickets and look-back status words). */
@@ -106,7 +114,8 @@ NBSP_HIDDEN void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, 
 
 /* pos4[s] = unsorted[perm[s]] (Morton order); inverse[perm[s]] = s. */
 NBSP_HIDDEN void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
-                                uint32_t* inverse, int* status, cudaStream_t stream);
+                                uint32_t* inverse, const float* unsorted_tol, float* tol,
+                                int* status, cudaStream_t stream);
 
 /* Device-side layout of the tree build scratch; sized by nbsp_bh_tree_bytes. */
 NBSP_HIDDEN size_t nbsp_bh_tree_bytes(size_t n);
@@ -131,9 +140,12 @@ enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
  * mode NBSP_BH_WALK_STACKLESS: warp-coherent skip-link walk, per-target test;
  * mode NBSP_BH_WALK_LISTS: lane-parallel node tests against the warp's group
  * box, dense evaluation of gathered interaction lists. */
-NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, size_t n, const void* tree, int order, int mode,
-                              const void* correction, float softening_squared, void* acc,
-                              unsigned long long* counters, int* status, cudaStream_t stream);
+NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree,
+                              int order, int mode, const void* correction,
+                              float softening_squared, void* acc, unsigned long long* counters,
+                              int* status, cudaStream_t stream);
+/* (tol != NULL and no correction: every opening test also takes the relative
+ * test with the per-target tolerances tol, Morton order) */
 
 /* Learned correction: training pairs (target, accepted cell) sampled with the
  * opening criterion `opening` at theta, their features and exact-sum labels, and

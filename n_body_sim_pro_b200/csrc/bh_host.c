@@ -7,6 +7,7 @@
 #include "bh.h"
 
 #include <cuda_runtime_api.h>
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -15,7 +16,7 @@ enum { BH_EVENTS = 8, BH_COUNTERS = 8 };
 
 struct NbspBarnesHut {
     size_t capacity;
-    double* partial;    /* 1024 * 10 */
+    double* partial;    /* 1024 * 12 */
     double* geometry;   /* 8 */
     uint64_t* keys;
     uint64_t* keys_alt;
@@ -27,6 +28,8 @@ struct NbspBarnesHut {
     void* acc;          /* double4 per target, Morton order */
     void* unsorted;     /* float4 positions in input order */
     uint32_t* inverse;  /* Morton slot of each input particle */
+    float* tol_unsorted; /* relative opening test: tolerance per particle, input order */
+    float* tol;          /* the same in Morton order */
     unsigned long long* counters;       /* device */
     unsigned long long* host_counters;  /* pinned */
     cudaEvent_t events[BH_EVENTS];
@@ -63,7 +66,8 @@ static NBodySimProStatus bh_cuda(NBodySimProError* error, cudaError_t code, cons
 
 static void release_buffers(NbspBarnesHut* b) {
     void* buffers[] = {b->partial, b->geometry, b->keys, b->keys_alt, b->index, b->index_alt,
-                       b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->inverse};
+                       b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->inverse,
+                       b->tol_unsorted, b->tol};
     for (size_t k = 0; k < sizeof(buffers) / sizeof(buffers[0]); ++k) cudaFree(buffers[k]);
     b->partial = b->geometry = NULL;
     b->keys = b->keys_alt = NULL;
@@ -71,6 +75,7 @@ static void release_buffers(NbspBarnesHut* b) {
     b->hist = NULL;
     b->pos4 = b->tree = b->acc = b->unsorted = NULL;
     b->inverse = NULL;
+    b->tol_unsorted = b->tol = NULL;
     b->capacity = 0;
 }
 
@@ -100,7 +105,7 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
     if (n <= b->capacity) return N_BODY_SIM_PRO_STATUS_OK;
     release_buffers(b);
     const size_t cap = n < 1024 ? 1024 : n;
-    BH_TRY(cudaMalloc((void**)&b->partial, 1024 * 10 * sizeof(double)));
+    BH_TRY(cudaMalloc((void**)&b->partial, 1024 * 12 * sizeof(double)));
     BH_TRY(cudaMalloc((void**)&b->geometry, 8 * sizeof(double)));
     BH_TRY(cudaMalloc((void**)&b->keys, cap * sizeof(uint64_t)));
     BH_TRY(cudaMalloc((void**)&b->keys_alt, cap * sizeof(uint64_t)));
@@ -112,16 +117,21 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
     BH_TRY(cudaMalloc(&b->acc, cap * 32));
     BH_TRY(cudaMalloc(&b->unsorted, cap * 16));
     BH_TRY(cudaMalloc((void**)&b->inverse, cap * sizeof(uint32_t)));
+    BH_TRY(cudaMalloc((void**)&b->tol_unsorted, cap * sizeof(float)));
+    BH_TRY(cudaMalloc((void**)&b->tol, cap * sizeof(float)));
     b->capacity = cap;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
-static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, int* status,
-                                cudaStream_t stream) {
-    nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status, stream);
+/* tol_scale > 0: also the relative opening test's tolerances (alpha / G). */
+static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, double tol_scale,
+                                int* status, cudaStream_t stream) {
+    const int rel = tol_scale > 0.0;
+    nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status,
+                   rel ? s->ax : NULL, rel ? s->ay : NULL, rel ? s->az : NULL, stream);
     cudaEventRecord(b->events[1], stream);
     nbsp_bh_keys(s->x, s->y, s->z, s->m, s->n, b->geometry, b->keys, b->index, b->unsorted,
-                 b->hist, stream);
+                 b->hist, s->ax, s->ay, s->az, tol_scale, rel ? b->tol_unsorted : NULL, stream);
     cudaEventRecord(b->events[2], stream);
     nbsp_bh_sort(b->keys, b->index, b->keys_alt, b->index_alt, s->n, b->hist, status, stream);
     cudaEventRecord(b->events[3], stream);
@@ -148,15 +158,24 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     }
     BH_TRY(cudaMemsetAsync(b->counters, 0, BH_COUNTERS * sizeof(unsigned long long), stream));
     cudaEventRecord(b->events[0], stream);
-    morton(b, s, status, stream);
+    /* relative opening test: tolerance alpha |a_old| / G (the correction uses
+     * the geometric test its network was trained with) */
+    const double g = fabs(p->gravitational_constant);
+    const double tol_scale = p->tolerance > 0.0 && p->correction == NULL
+                                 ? (g > 0.0 ? p->tolerance / g : INFINITY)
+                                 : 0.0;
+    const int rel = tol_scale > 0.0;
+    morton(b, s, tol_scale, status, stream);
     nbsp_bh_duplicates(b->keys, b->index, s->x, s->y, s->z, n, status, stream);
-    nbsp_bh_gather(b->unsorted, b->index, n, b->pos4, b->inverse, status, stream);
+    nbsp_bh_gather(b->unsorted, b->index, n, b->pos4, b->inverse, rel ? b->tol_unsorted : NULL,
+                   rel ? b->tol : NULL, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
     nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening, b->tree, status,
                     stream);
     cudaEventRecord(b->events[5], stream);
-    nbsp_bh_walk(b->pos4, n, b->tree, p->multipole_order, p->walk_mode, p->correction,
+    nbsp_bh_walk(b->pos4, rel ? b->tol : NULL, n, b->tree, p->multipole_order, p->walk_mode,
+                 p->correction,
                  (float)p->softening_squared, b->acc, b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
     nbsp_bh_unsort(b->acc, b->inverse, n, p->gravitational_constant, s->ax, s->ay, s->az,
@@ -215,7 +234,7 @@ NBodySimProStatus nbsp_bh_morton(NbspBarnesHut** handle, const NbspBarnesHutStat
     NbspBarnesHut* b = *handle;
     const size_t n = s->n;
     cudaEventRecord(b->events[0], stream);
-    morton(b, s, status, stream);
+    morton(b, s, 0.0, status, stream);
     BH_TRY(cudaGetLastError());
     uint32_t* perm32 = NULL;
     if (permutation != NULL) {

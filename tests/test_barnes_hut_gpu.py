@@ -170,10 +170,90 @@ def test_offset_opening_is_more_accurate(cuda, ctx, theta, walk):
     assert np.array_equal(a1, b1)
 
 
+def _resident(cuda, p, theta, opening=0, alpha=0.0, eps=0.01):
+    ctx = cuda.CudaContext(theta=theta, opening=opening)
+    ctx.set_relative_opening(alpha)
+    ctx.upload(to_system(cuda, p))
+    return ctx
+
+
+def test_relative_opening_limits_are_the_geometric_walk(cuda):
+    """alpha -> infinity, or no previous accelerations at all (a_old = 0 and rms
+    |a_old| = 0): every relative test passes, the geometric test alone decides."""
+    p = O.preset("plummer_collision", 100000, 42)
+    g = cuda.gravity_init(1.0, 0.01)
+    with _resident(cuda, p, 1.0, opening=1) as ctx:
+        ctx.set_relative_opening(1e30)
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old = 0 here
+        first = ctx.download_accelerations()
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old = first
+        huge = ctx.download_accelerations()
+        ctx.set_relative_opening(0.0)
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+        geometric = ctx.download_accelerations()
+    assert np.array_equal(first, geometric) and np.array_equal(huge, geometric)
+    with _resident(cuda, p, 1.0, opening=1, alpha=1e-3) as ctx:  # uploaded a = 0
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+        assert np.array_equal(ctx.download_accelerations(), geometric)
+
+
+def test_relative_opening_trades_accuracy_for_work(cuda):
+    """G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|): smaller alpha, more
+    terms and a smaller error; at alpha 0.0025 the error is below the geometric
+    theta 0.6 walk's with fewer terms."""
+    p = O.preset("plummer_collision", 200000, 42)
+    g = cuda.gravity_init(1.0, 0.01)
+    targets = np.random.default_rng(2).choice(p.n, 1024, replace=False)
+    ref = O.gravity_subset(p, 1.0, 0.01, targets)
+    rows = []
+    with _resident(cuda, p, 0.6) as ctx:
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+        st = ctx.stats()
+        geo = (O.rms_relative_error(ctx.download_accelerations()[targets], ref),
+               st["accepted_approximations"] + st["exact_interactions"])
+        ctx.theta = 1.0
+        for alpha in (0.01, 0.0025, 0.001):
+            ctx.set_relative_opening(alpha)
+            ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old: the last walk's
+            st = ctx.stats()
+            rows.append((alpha, O.rms_relative_error(ctx.download_accelerations()[targets], ref),
+                         st["accepted_approximations"] + st["exact_interactions"]))
+    print("geometric theta 0.6", geo, "relative", rows)
+    assert rows[0][1] > rows[1][1] > rows[2][1]
+    assert rows[0][2] < rows[1][2] < rows[2][2]
+    assert rows[1][1] < geo[0] and rows[1][2] < geo[1]
+
+
+def test_relative_opening_reads_the_views_accelerations(cuda):
+    """Through the plugin function the previous accelerations come from the view."""
+    p = O.preset("plummer_collision", 100000, 42)
+    g = cuda.gravity_init(1.0, 0.01)
+    targets = np.random.default_rng(2).choice(p.n, 512, replace=False)
+    ref = O.gravity_subset(p, 1.0, 0.01, targets)
+    s = to_system(cuda, p)
+    with cuda.CudaContext(theta=0.5) as ctx:
+        cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)  # a_old in the view
+        ctx.theta = 1.0
+        ctx.set_relative_opening(0.0025)
+        a = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)
+        rel = O.rms_relative_error(a[targets], ref)
+        s.ax[:] = 0.0
+        s.ay[:] = 0.0
+        s.az[:] = 0.0
+        b = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, ctx)  # no a_old
+        fallback = O.rms_relative_error(b[targets], ref)
+    print(f"relative {rel:.3e} without previous accelerations (geometric theta 1.0) {fallback:.3e}")
+    assert rel < 2e-3 and rel < 0.5 * fallback
+
+
 def test_opening_argument_checked(cuda, ctx):
     with pytest.raises(cuda.CudaError):
         ctx.set_opening(2)
     ctx.set_opening(cuda.Opening.REFERENCE)
+    for bad in (-1.0, float("nan"), float("inf")):
+        with pytest.raises(cuda.CudaError):
+            ctx.set_relative_opening(bad)
+    ctx.set_relative_opening(0.0)
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 33, 4097, 10000])
