@@ -469,10 +469,11 @@ def rms_at_targets(nb, ctx, g, n, targets, ref):
 
 
 def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None,
-                opening=0, alpha=0.0):
+                opening=0, alpha=0.0, leaf=16):
     """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order, opening,
-    relative tolerance alpha)."""
-    ctx = nb.CudaContext(theta=theta, multipole_order=order, opening=opening)
+    relative tolerance alpha, bucket capacity)."""
+    ctx = nb.CudaContext(theta=theta, multipole_order=order, opening=opening,
+                         leaf_capacity=leaf)
     ctx.set_correction(correction)
     ctx.set_relative_opening(alpha)
     ctx.upload(system)
@@ -495,12 +496,14 @@ ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.005, 0.007, 
 
 
 def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
-    """Plain Barnes-Hut (monopole, the reference's opening test) vs the chosen
-    method — the fastest of {monopole, quadrupole} x {reference, offset opening
-    test} — each at the largest theta of THETA_GRID meeting RMS_TARGET, all
-    timed; optionally the learned correction at theta 1.0 (trained on 2^22
-    pairs of the 1M collision) under either opening test and the plain walk at
-    theta 0.5."""
+    """Plain Barnes-Hut (monopole, the reference's opening test, 16-particle
+    buckets) vs the chosen method — the fastest of {monopole, quadrupole} x
+    {reference, offset opening test}, the monopole walk with 32-particle buckets,
+    and the relative test over the reference test at theta 1.0 with 16- and
+    32-particle buckets — each at the largest theta (alpha) of its grid meeting
+    RMS_TARGET, all timed; optionally the learned correction at theta 1.0
+    (trained on 2^22 pairs of the 1M collision) under either opening test and
+    the plain walk at theta 0.5."""
     n = wl["n"]
     targets = np.random.default_rng(11).choice(n, min(4096, n), replace=False)
     ctx = nb.CudaContext(theta=0.5)
@@ -516,24 +519,39 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
                 ctx.theta = th
                 rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
             table[(order, oname)] = rows
+    ctx.set_opening(0)
+    ctx.set_multipole_order(1)
+    ctx.set_leaf_capacity(32)
+    table_leaf32 = []
+    for th in THETA_GRID:
+        ctx.theta = th
+        table_leaf32.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
+    ctx.set_leaf_capacity(16)
     # relative test: each alpha evaluated twice, the second walk reading the
     # first one's accelerations as a_old (as in a run, where a_old is the
     # previous step's)
     ctx.set_opening(0)
     ctx.set_multipole_order(1)
     ctx.theta = 1.0
-    rel_rows = []
-    for alpha in ALPHA_GRID:
-        ctx.set_relative_opening(alpha)
-        ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
-        rel_rows.append((alpha, rms_at_targets(nb, ctx, g, n, targets, ref)))
+    rel_rows = {}
+    for leaf in (16, 32):
+        ctx.set_leaf_capacity(leaf)
+        rows = []
+        for alpha in ALPHA_GRID:
+            ctx.set_relative_opening(alpha)
+            ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+            rows.append((alpha, rms_at_targets(nb, ctx, g, n, targets, ref)))
+        rel_rows[leaf] = rows
     ctx.set_relative_opening(0.0)
     ctx.close()
     out = {"rms_target": RMS_TARGET, "oracle": "FP64 device direct sum, 4096 seeded targets, "
            "initial state",
            "sweep": {f"order{o}_{on}": [[t, round(r, 6)] for t, r in rows]
                      for (o, on), rows in table.items()}}
-    out["sweep"]["order1_relative_alpha_theta1.0"] = [[a, round(r, 6)] for a, r in rel_rows]
+    out["sweep"]["order1_reference_leaf32"] = [[t, round(r, 6)] for t, r in table_leaf32]
+    for leaf, rows in rel_rows.items():
+        out["sweep"][f"order1_relative_alpha_theta1.0_leaf{leaf}"] = [[a, round(r, 6)]
+                                                                      for a, r in rows]
     methods = {}
     for (order, oname), rows in table.items():
         ok = [t for t, r in rows if r <= RMS_TARGET]
@@ -543,15 +561,27 @@ def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correctio
         v, ms = timed_steps(nb, torch, system, g, wl, th, order, steps, warmup, flush,
                             opening=OPENINGS[oname])
         methods[(order, oname)] = {"theta": th, "multipole_order": order, "opening": oname,
-                                   "rms": dict(rows)[th], "value": v,
+                                   "leaf_capacity": 16, "rms": dict(rows)[th], "value": v,
                                    "ms_per_step": round(ms, 4)}
-    ok = [a for a, r in rel_rows if r <= RMS_TARGET]
+    ok = [t for t, r in table_leaf32 if r <= RMS_TARGET]
     if ok:
+        th = max(ok)
+        v, ms = timed_steps(nb, torch, system, g, wl, th, 1, steps, warmup, flush, leaf=32)
+        methods[(1, "reference", 32)] = {"theta": th, "multipole_order": 1,
+                                         "opening": "reference", "leaf_capacity": 32,
+                                         "rms": dict(table_leaf32)[th], "value": v,
+                                         "ms_per_step": round(ms, 4)}
+    for leaf, rows in rel_rows.items():
+        ok = [a for a, r in rows if r <= RMS_TARGET]
+        if not ok:
+            continue
         alpha = max(ok)
-        v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush, alpha=alpha)
-        methods[(1, "relative")] = {"theta": 1.0, "multipole_order": 1, "opening": "reference",
-                                    "relative_alpha": alpha, "rms": dict(rel_rows)[alpha],
-                                    "value": v, "ms_per_step": round(ms, 4)}
+        v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush, alpha=alpha,
+                            leaf=leaf)
+        methods[(1, "relative", leaf)] = {"theta": 1.0, "multipole_order": 1,
+                                          "opening": "reference", "relative_alpha": alpha,
+                                          "leaf_capacity": leaf, "rms": dict(rows)[alpha],
+                                          "value": v, "ms_per_step": round(ms, 4)}
     out["methods"] = list(methods.values())
     out["plain"] = methods.get((1, "reference"))
     out["chosen"] = max(methods.values(), key=lambda m: m["value"]) if methods else None
@@ -951,7 +981,8 @@ def main(argv=None):
                     "value_is": "the configuration's throughput (plain walk at its theta)",
                     "chosen_at_rms_1e-3": m["chosen"]["value"],
                     "chosen_method": {k: m["chosen"].get(k) for k in
-                                      ("theta", "multipole_order", "opening", "relative_alpha")},
+                                      ("theta", "multipole_order", "opening", "relative_alpha",
+                                       "leaf_capacity")},
                     "plain_at_rms_1e-3": m["plain"]["value"],
                     "chosen_over_plain": m.get("chosen_over_plain"),
                     "fp32_peak_frac": r["roofline"].get("frac")}
