@@ -492,7 +492,8 @@ def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, co
 OPENINGS = {"reference": 0, "offset": 1}
 # relative opening test (G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)) over the
 # reference test at theta 1.0: the alphas of its sweep
-ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.005, 0.007, 0.01)
+ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
+              0.007, 0.01)
 
 
 def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
