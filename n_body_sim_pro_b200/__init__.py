@@ -381,7 +381,8 @@ class CudaContext:
     """NBodySimProCudaContext: device-resident state, stepping and diagnostics."""
 
     def __init__(self, theta: float | None = None, multipole_order: int | None = None,
-                 leaf_capacity: int | None = None, opening: int | None = None):
+                 leaf_capacity: int | None = None, opening: int | None = None,
+                 relative_opening: float | None = None):
         L = library()
         err = Error()
         h = L.n_body_sim_pro_cuda_context_create(C.byref(err))
@@ -398,6 +399,8 @@ class CudaContext:
             self.set_leaf_capacity(leaf_capacity)
         if opening is not None:
             self.set_opening(opening)
+        if relative_opening is not None:
+            self.set_relative_opening(relative_opening)
 
     def close(self) -> None:
         if getattr(self, "handle", None):
