@@ -108,6 +108,7 @@ struct NBodySimProCudaContext {
     int opening;
     double tolerance; /* alpha of the relative opening test; 0: off */
     const void* correction; /* device network of the learned correction, or NULL */
+    int tree_quadrupoles; /* the next build keeps every cell's quadrupole (training reads them) */
     NbspBarnesHut* bh;
     int bh_pending; /* a Barnes-Hut evaluation's stats await collection */
 
@@ -517,6 +518,7 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.opening = c->opening;
         p.tolerance = c->tolerance;
         p.correction = c->correction;
+        p.quadrupoles = c->tree_quadrupoles;
         NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
         c->bh_pending = 1;
         return nbsp_bh_accelerations(&c->bh, &s, &p, c->status, c->stream, &c->stats,
@@ -1059,9 +1061,11 @@ NBodySimProStatus nbsp_context_tree(NBodySimProCudaContext* c, const NBodySimPro
     if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
     CUDA_TRY(cudaSetDevice(c->device));
     const void* saved = c->correction;
-    c->correction = NULL; /* the plain tree and walk */
+    c->correction = NULL; /* the plain tree and walk, with the features' moments */
+    c->tree_quadrupoles = 1;
     st = resident_accelerations(c, gravity, N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT, error);
     c->correction = saved;
+    c->tree_quadrupoles = 0;
     if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
     if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
     out->pos4 = nbsp_bh_positions(c->bh);

@@ -794,11 +794,14 @@ struct Opening {
   int criterion;         // NBSP_BH_OPENING_*
 };
 
+template <bool QUAD>
 __device__ void finish_node(const Tree& t, int node, const Moments& mo, int first, int lvl,
                             const Opening& o) {
   t.mom[node] = make_double4(mo.m, mo.cx, mo.cy, mo.cz);
-  for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
-  t.trace64[node] = mo.t2;
+  if (QUAD) {
+    for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
+    t.trace64[node] = mo.t2;
+  }
   t.com[node] = make_float4((float)mo.cx, (float)mo.cy, (float)mo.cz, (float)mo.m);
   // cell side 2h = root side / 2^lvl; the cell's centre from the first key's
   // top 3 lvl bits, in the particles' frame (relative to the centre of mass)
@@ -822,9 +825,11 @@ __device__ void finish_node(const Tree& t, int node, const Moments& mo, int firs
   t.side[node] = (float)side;
   t.shift[node] = (float)shift;
   t.kmass[node] = (float)(mo.m * side * side);
-  t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
-  t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
-  t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
+  if (QUAD) {
+    t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
+    t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
+    t.quad[2 * node + 1] = make_float4((float)mo.q[4], 0.f, 0.f, 0.f);
+  }
 }
 
 // L2-coherent load of a double4 written by another thread of this grid.
@@ -845,6 +850,9 @@ __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
 // the combine sorts them into depth-first (= octant) order, so the sums run in
 // a fixed order and the result is deterministic, loads all of them at once and
 // writes the sorted list back for the interaction-list walk.
+// QUAD: also the trace-free quadrupoles and the spread (the quadrupole walk,
+// the correction's features); the monopole walk reads neither.
+template <bool QUAD>
 __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
                                                       Opening open, int* status) {
   const int total = (int)t.offset[t.n];
@@ -874,7 +882,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
       for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
       mo.t2 = 0.0;
 #pragma unroll 4
-      for (int j = info.y; j < info.y + info.z; ++j) {
+      for (int j = info.y; QUAD && j < info.y + info.z; ++j) {
         const float4 p = pos[j];
         const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
         const double r2 = dx * dx + dy * dy + dz * dz;
@@ -888,7 +896,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
         mo.q[5] += w * (3.0 * dz * dz - r2);
       }
     }
-    finish_node(t, node, mo, info.y, t.level[node], open);
+    finish_node<QUAD>(t, node, mo, info.y, t.level[node], open);
     int parent = info.w;
     for (int climb = 0; parent >= 0; ++climb) {
       if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
@@ -958,7 +966,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
       pm.t2 = 0.0;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        if (k < nc) {
+        if (QUAD && k < nc) {
           const int c = ch[k];
           const double dx = cm[k].y - pm.cx, dy = cm[k].z - pm.cy, dz = cm[k].w - pm.cz;
           const double r2 = dx * dx + dy * dy + dz * dz;
@@ -979,7 +987,7 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
           make_int4(nc > 4 ? ch[4] : -1, nc > 5 ? ch[5] : -1, nc > 6 ? ch[6] : -1,
                     nc > 7 ? ch[7] : -1);
       t.height[parent] = hmax + 1;
-      finish_node(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open);
+      finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open);
       parent = pinfo.w;
     }
   }
@@ -2219,7 +2227,8 @@ void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree
 }
 
 void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const double* geometry,
-                     double theta, int opening, void* tree, int* status, cudaStream_t stream) {
+                     double theta, int opening, int quadrupoles, void* tree, int* status,
+                     cudaStream_t stream) {
   Tree t = tree_view(tree, n);
   const size_t nb = 2 * n - 1;
   Opening o;
@@ -2230,8 +2239,12 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
   o.criterion = opening;
   size_t blocks = (nb + 255) / 256;  // grid-stride over the octree nodes (<= 2n - 1)
   if (blocks > 148 * 16) blocks = 148 * 16;
-  NBSP_COUNT_LAUNCH(1), moments_kernel<<<(unsigned)blocks, 256, 0, stream>>>((const float4*)pos4, t,
-                                                                   o, status);
+  if (quadrupoles)
+    NBSP_COUNT_LAUNCH(1), moments_kernel<true><<<(unsigned)blocks, 256, 0, stream>>>(
+                              (const float4*)pos4, t, o, status);
+  else
+    NBSP_COUNT_LAUNCH(1), moments_kernel<false><<<(unsigned)blocks, 256, 0, stream>>>(
+                              (const float4*)pos4, t, o, status);
 }
 
 void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree, int order,

@@ -40,6 +40,8 @@ typedef struct NbspBarnesHutParams {
     int opening;            /* NBSP_BH_OPENING_* */
     double tolerance;       /* alpha of the relative opening test; 0: geometric test alone */
     const void* correction; /* device network (mlp.cuh Net) or NULL */
+    int quadrupoles;        /* the cells' quadrupoles and spread even for the monopole walk
+                               (the correction's training reads them) */
 } NbspBarnesHutParams;
 
 typedef struct NbspBarnesHutState {
@@ -130,8 +132,8 @@ NBSP_HIDDEN void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity
 enum { NBSP_BH_OPENING_REFERENCE = 0, NBSP_BH_OPENING_OFFSET = 1 };
 
 NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n,
-                                 const double* geometry, double theta, int opening, void* tree,
-                                 int* status, cudaStream_t stream);
+                                 const double* geometry, double theta, int opening,
+                                 int quadrupoles, void* tree, int* status, cudaStream_t stream);
 
 enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
 

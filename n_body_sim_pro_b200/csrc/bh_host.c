@@ -171,8 +171,9 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
                    rel ? b->tol : NULL, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
-    nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening, b->tree, status,
-                    stream);
+    nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening,
+                    p->multipole_order == 2 || p->correction != NULL || p->quadrupoles, b->tree,
+                    status, stream);
     cudaEventRecord(b->events[5], stream);
     nbsp_bh_walk(b->pos4, rel ? b->tol : NULL, n, b->tree, p->multipole_order, p->walk_mode,
                  p->correction,
