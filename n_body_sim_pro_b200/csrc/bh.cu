@@ -839,6 +839,15 @@ __device__ __forceinline__ double4 ldcg_d4(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// Arrival at a parent: a release (this thread's node records are visible
+// before the increment) and an acquire (the last child to arrive sees every
+// sibling's records) in one atomic, instead of two full fences around it.
+__device__ __forceinline__ int arrive_acq_rel(int* p) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
   const int lo = min(a, b), hi = max(a, b);
   a = lo;
@@ -903,11 +912,9 @@ __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         break;
       }
-      __threadfence();
       const int nc = __ldcg(&t.nchild[parent]);
-      const int arrived = atomicAdd(&t.arrive[parent], 1);
+      const int arrived = arrive_acq_rel(&t.arrive[parent]);
       if (arrived != nc - 1) break;
-      __threadfence();
       if (nc < 1 || nc > 8) {
         atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         break;
