@@ -422,12 +422,18 @@ def run_ours(args, wl, world, rank, local):
     if wl["algorithm"] == "barnes_hut" and phases:
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         nodes = float(stats_acc[-1]["node_count"])
+        # the moments pass: the monopole walk's reads each particle once and
+        # writes 64 B per node (FP64 moments, the walk's float4, opening
+        # terms), reading 52 (record, level, children's moments); the
+        # quadrupole pass reads the particles twice, writes 156 and reads 108
+        quad = wl.get("order", 1) == 2
+        mom_bytes = (32.0 * n + 264.0 * nodes) if quad else (16.0 * n + 116.0 * nodes)
         stages = {}
         for name, key, nbytes in (
                 ("bounds", "bounds_ms", 32.0 * n),
                 ("keys", "keys_ms", 36.0 * n),
                 ("sort", "sort_ms", 8 * 24.0 * n),
-                ("moments", "moments_ms", 32.0 * n + 120.0 * nodes),
+                ("moments", "moments_ms", mom_bytes),
                 ("integrate", "integrate_ms", 36.0 * n + 24.0 * n + 120.0 * n)):
             ms = float(np.mean([ph[key] for ph in phases]))
             gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
@@ -436,8 +442,9 @@ def run_ours(args, wl, world, rank, local):
                             "frac_of_hbm": round(gbs / hbm, 4) if gbs else None}
         stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes: "
                            "bounds 32/particle, keys 24+12, sort 8 passes x (12+12), moments "
-                           "2 x 16 per particle + 120 per node, integrate scatter 36 + kick-drift "
-                           "24 + 120 per particle")
+                           + ("2 x 16 per particle + 264 per node" if quad else
+                              "16 per particle + 116 per node")
+                           + ", integrate scatter 36 + kick-drift 24 + 120 per particle")
 
     # e2e through the plugin call on pinned host arrays
     e2e = None
