@@ -134,6 +134,22 @@ def test_quadrupole_is_more_accurate(cuda, ctx, walk):
     assert e2 < 0.5 * e1
 
 
+def test_quadrupoles_follow_the_walk_order(cuda, walk):
+    """The monopole walk's build skips the quadrupoles; a context switched to the
+    quadrupole walk (or back) must give, bit for bit, what a fresh context of
+    that order gives."""
+    p = O.preset("plummer_collision", 50000, 7)
+    fresh = {}
+    for order in (1, 2):
+        with cuda.CudaContext() as c:
+            fresh[order], _ = bh(cuda, p, 0.01, 0.7, c, order=order, walk=walk)
+    with cuda.CudaContext() as c:
+        for order in (1, 2, 1, 2):
+            a, _ = bh(cuda, p, 0.01, 0.7, c, order=order, walk=walk)
+            assert np.array_equal(a, fresh[order]), order
+    assert not np.array_equal(fresh[1], fresh[2])
+
+
 def test_collision_config_accuracy(cuda, ctx, walk):
     """Config-2 shape at N=200k: two Plummer spheres 10 apart, eps 0.01, theta 0.7,
     vs the FP64 oracle on 1024 seeded targets."""
