@@ -39,15 +39,48 @@ constexpr int kBoundsThreads = 256;
 constexpr int kBoundsBlocks = 1024;
 constexpr int kBoundsVals = 11;  // min xyz, max xyz, m, mx, my, mz, |a|^2
 
+// The block's combined values in thread 0: each warp by shuffles, then the
+// warps' results by the first warp.
+__device__ __forceinline__ void bounds_block_reduce(double (&v)[kBoundsVals],
+                                                    double (*sh)[kBoundsThreads / 32]) {
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int q = 0; q < kBoundsVals; ++q) {
+      const double o = __shfl_xor_sync(0xffffffffu, v[q], off);
+      v[q] = q < 3 ? fmin(v[q], o) : q < 6 ? fmax(v[q], o) : v[q] + o;
+    }
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < kBoundsVals; ++q) sh[q][w] = v[q];
+  __syncthreads();
+  if (w != 0) return;
+#pragma unroll
+  for (int q = 0; q < kBoundsVals; ++q)
+    v[q] = lane < kBoundsThreads / 32 ? sh[q][lane]
+           : q < 3                    ? INFINITY
+           : q < 6                    ? -INFINITY
+                                      : 0.0;
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int q = 0; q < kBoundsVals; ++q) {
+      const double o = __shfl_xor_sync(0xffffffffu, v[q], off);
+      v[q] = q < 3 ? fmin(v[q], o) : q < 6 ? fmax(v[q], o) : v[q] + o;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
     const double* __restrict__ m, size_t n, double* __restrict__ partial, int* status,
     const double* __restrict__ ax, const double* __restrict__ ay,
     const double* __restrict__ az) {
-  __shared__ double sh[kBoundsVals][kBoundsThreads];
+  __shared__ double sh[kBoundsVals][kBoundsThreads / 32];
   double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
                            0.0,      0.0,      0.0,      0.0,       0.0};
   bool bad = false;
+#pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)kBoundsThreads + threadIdx.x; i < n;
        i += (size_t)gridDim.x * kBoundsThreads) {
     const double px = x[i], py = y[i], pz = z[i], pm = m[i];
@@ -65,24 +98,16 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
     if (ax != nullptr) v[10] += ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i];
   }
   if (bad) atomicOr(status, NBSP_DEVICE_ERROR_NONFINITE_POSITION);
-  const int t = threadIdx.x;
-  for (int q = 0; q < kBoundsVals; ++q) sh[q][t] = v[q];
-  __syncthreads();
-  for (int stride = kBoundsThreads / 2; stride > 0; stride >>= 1) {
-    if (t < stride) {
-      for (int q = 0; q < 3; ++q) sh[q][t] = fmin(sh[q][t], sh[q][t + stride]);
-      for (int q = 3; q < 6; ++q) sh[q][t] = fmax(sh[q][t], sh[q][t + stride]);
-      for (int q = 6; q < kBoundsVals; ++q) sh[q][t] += sh[q][t + stride];
-    }
-    __syncthreads();
-  }
-  if (t < kBoundsVals) partial[blockIdx.x * kBoundsVals + t] = sh[t][0];
+  bounds_block_reduce(v, sh);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < kBoundsVals; ++q) partial[blockIdx.x * kBoundsVals + q] = v[q];
 }
 
 // Root cube with the exact FP64 operation sequence of barnes_hut.c:471-483.
 __global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
     const double* __restrict__ partial, int blocks, size_t n, double* __restrict__ geometry) {
-  __shared__ double sh[kBoundsVals][kBoundsThreads];
+  __shared__ double sh[kBoundsVals][kBoundsThreads / 32];
   double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
                            0.0,      0.0,      0.0,      0.0,       0.0};
   for (int b = threadIdx.x; b < blocks; b += kBoundsThreads) {
@@ -90,20 +115,10 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
     for (int q = 3; q < 6; ++q) v[q] = fmax(v[q], partial[b * kBoundsVals + q]);
     for (int q = 6; q < kBoundsVals; ++q) v[q] += partial[b * kBoundsVals + q];
   }
-  const int t = threadIdx.x;
-  for (int q = 0; q < kBoundsVals; ++q) sh[q][t] = v[q];
-  __syncthreads();
-  for (int stride = kBoundsThreads / 2; stride > 0; stride >>= 1) {
-    if (t < stride) {
-      for (int q = 0; q < 3; ++q) sh[q][t] = fmin(sh[q][t], sh[q][t + stride]);
-      for (int q = 3; q < 6; ++q) sh[q][t] = fmax(sh[q][t], sh[q][t + stride]);
-      for (int q = 6; q < kBoundsVals; ++q) sh[q][t] += sh[q][t + stride];
-    }
-    __syncthreads();
-  }
-  if (t == 0) {
-    const double lo[3] = {sh[0][0], sh[1][0], sh[2][0]};
-    const double hi[3] = {sh[3][0], sh[4][0], sh[5][0]};
+  bounds_block_reduce(v, sh);
+  if (threadIdx.x == 0) {
+    const double lo[3] = {v[0], v[1], v[2]};
+    const double hi[3] = {v[3], v[4], v[5]};
     double half = __dmul_rn(0.5, __dsub_rn(hi[0], lo[0]));
     for (int k = 1; k < 3; ++k) {
       const double e = __dmul_rn(0.5, __dsub_rn(hi[k], lo[k]));
@@ -113,9 +128,9 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_final_kernel(
     half = __dmul_rn(half, 1.0 + 1.0e-9);
     for (int k = 0; k < 3; ++k) geometry[k] = __dmul_rn(0.5, __dadd_rn(lo[k], hi[k]));
     geometry[3] = half;
-    const double mt = sh[6][0];
-    for (int k = 0; k < 3; ++k) geometry[4 + k] = mt != 0.0 ? sh[7 + k][0] / mt : 0.0;
-    geometry[7] = n > 0 ? sqrt(sh[10][0] / (double)n) : 0.0;  // rms |a| (when given)
+    const double mt = v[6];
+    for (int k = 0; k < 3; ++k) geometry[4 + k] = mt != 0.0 ? v[7 + k] / mt : 0.0;
+    geometry[7] = n > 0 ? sqrt(v[10] / (double)n) : 0.0;  // rms |a| (when given)
   }
 }
 
