@@ -306,7 +306,9 @@ N_BODY_SIM_PRO_CUDA_API size_t n_body_sim_pro_cuda_context_corrected_cells(
  * `cuda` algorithm: exact softened all-pairs sum (j == i excluded) on the GPU,
  * semantics of n_body_sim_pro_gravity_compute_acceleration_reference
  * (physics/gravity.h:46-59, src/c/physics/gravity.c:15-70).  `context` is an
- * NBodySimProCudaContext*, or NULL for a lazily created process-wide context.
+ * NBodySimProCudaContext*, or NULL for a lazily created process-wide context
+ * (one host thread at a time, like the reference's integrator loop; threads
+ * that compute concurrently pass contexts of their own).
  * Copies positions/masses to the device and accelerations back every call.
  */
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_gravity_compute_acceleration_cuda(

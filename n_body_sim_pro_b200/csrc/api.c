@@ -18,6 +18,7 @@
 
 #include <cuda_runtime_api.h>
 #include <math.h>
+#include <stdatomic.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -533,12 +534,21 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
 /* plugin force functions                                                     */
 /* ------------------------------------------------------------------------- */
 
-static NBodySimProCudaContext* g_default_context = NULL;
+static _Atomic(NBodySimProCudaContext*) g_default_context = NULL;
 
+/* The context of a NULL `context` argument, created by the first such call;
+ * when two threads make that call at once, one creation wins and the other
+ * is destroyed. */
 static NBodySimProCudaContext* context_or_default(void* context, NBodySimProError* error) {
     if (context != NULL) return (NBodySimProCudaContext*)context;
-    if (g_default_context == NULL) g_default_context = n_body_sim_pro_cuda_context_create(error);
-    return g_default_context;
+    NBodySimProCudaContext* c = atomic_load(&g_default_context);
+    if (c != NULL) return c;
+    NBodySimProCudaContext* made = n_body_sim_pro_cuda_context_create(error);
+    if (made == NULL) return NULL;
+    NBodySimProCudaContext* expected = NULL;
+    if (atomic_compare_exchange_strong(&g_default_context, &expected, made)) return made;
+    n_body_sim_pro_cuda_context_destroy(made);
+    return expected;
 }
 
 static NBodySimProStatus copy_in(NBodySimProCudaContext* c, const NBodySimProParticleSystemView* v,
