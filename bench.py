@@ -2,30 +2,38 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-Default workload (``bh_collision_1m``): plain Barnes-Hut on two Plummer
-spheres of 500k particles (a = 1, M = 1/2 each, centres 10 apart on x,
-relative velocity 0.3 on y), eps = 0.01, theta = 0.7, leapfrog KDK at
-dt = 1e-3 — one step = one kick-drift-force-kick of all N particles.
-Metric: particle-steps/s (N x steps / device time).
+Default workload (``bh_matched_10m``): the two-Plummer collision at N = 10M
+(two spheres of 5M equal-mass particles, a = 1, M = 1/2 each, centres 10 apart
+on x, relative velocity 0.3 on y), eps = 0.01, leapfrog KDK at dt = 1e-3, at a
+matched rms relative force error of at most 1e-3 against the FP64 direct sum.
+The initial conditions come from the device generator of the reference's
+parallel presets (per-particle xoshiro256** streams, block b seeded
+mix_seed(42, b)); the reference arm builds the same state with the CPU
+restatement of that generator.
 
-Other workloads (parity configs, selectable): ``allpairs_plummer_16k``,
-``allpairs_precision_262k``, ``ensemble_4096`` and ``bh_matched_10m`` (the
-same collision at N = 10M).  Multi-GPU sharding (strong scaling, `scaling`
-"strong"): ``allpairs_sharded_262k`` splits one all-pairs system by targets
-over the ranks with an NCCL all-gather of the packed sources every step;
-``ensemble_4096_sharded`` splits the 4096 systems over the ranks by cost.
+One step = one kick-drift-force-kick of all N particles; metric: particle-steps/s
+(N x steps / device time).  The matched-accuracy study runs first on the
+initial state: for each Barnes-Hut method — the monopole and quadrupole walks
+under the reference's opening test and under the offset test, 16- and
+32-particle buckets, the relative opening test (G M (2h)^2 / d^4 <=
+alpha max(|a_old|, rms |a_old|)) over the reference test at theta 1.0, and the
+learned correction at theta 1.0 — the largest theta (alpha) of its grid whose
+rms error on 4096 seeded targets is at most 1e-3 is timed.  "plain" is the
+monopole walk with the reference's test; `value` is the fastest method meeting
+the bar ("chosen"), timed over the K steps of the timed region; the line also
+carries plain at theta 0.5, plain at its matched theta, the relative test and the
+corrected walk, each with its rms and max error and its energy drift.
 
-`matched_accuracy` (Barnes-Hut workloads, skipped with --no-matched): on the
-initial state, the rms relative force error against the FP64 direct sum on
-4096 seeded targets is measured over a theta grid for the monopole and the
-quadrupole walk under the reference's opening test and under the offset test;
-each method is then timed at the largest theta whose error is at most 1e-3;
-the relative opening test (G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)
-with the reference's test at theta 1.0 as the safety bound) is swept over
-alpha the same way.  "plain" is the monopole walk with the reference's test,
-"chosen" the fastest method.  ``bh_matched_10m`` adds the plain walk at theta 0.5 and the learned
-correction at theta 1.0 under both opening tests (network trained on 2^22
-cell-target pairs of the 1M collision).
+Other workloads (each one configuration; the default run also reports them as
+compact sub-records): ``bh_collision_1m`` (the same collision at 1M, theta
+0.7, 10 steps), ``allpairs_plummer_16k`` (16384-particle Plummer sphere from
+the reference's globular-cluster preset, 3 steps), ``allpairs_precision_262k``
+(uniform positions, log-uniform masses, eps 1e-3, 100 steps at dt 1e-4),
+``ensemble_4096`` (4096 Plummer systems of 32..4096 particles, 1000 steps).
+Multi-GPU sharding (strong scaling): ``allpairs_sharded_262k`` splits one
+all-pairs system by targets over the ranks with an NCCL all-gather of the
+packed sources every step; ``ensemble_4096_sharded`` splits the 4096 systems
+over the ranks by cost.
 
 Timing: W untimed warm-up steps; then K steps, each a 1-step device-resident
 advance bracketed by CUDA events recorded by the library on its own stream;
@@ -37,12 +45,13 @@ sharded workloads divide one job instead.
 
 `e2e`: the same metric through the reference-facing plugin call
 n_body_sim_pro_barnes_hut_compute_acceleration_cuda(view, ...) on pinned host
-arrays inside a host leapfrog loop: every step copies positions + masses to
-the device and accelerations back.
+arrays inside a host leapfrog loop: every step copies positions, masses and
+the previous accelerations to the device and the new accelerations back.
 
 `cpu_baseline` / `--impl reference`: the reference engine compiled from its
 own sources (oracle/_ref) timed on this host's cores on the same initial
-conditions (a bounded sample of steps).
+conditions, over a bounded sample of steps (stated in the line), with its own
+rms force error on the same 4096 targets.
 """
 from __future__ import annotations
 
@@ -60,17 +69,21 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+DEFAULT_WORKLOAD = "bh_matched_10m"
 WORKLOADS = {
+    # the headline: chosen vs plain Barnes-Hut at rms <= 1e-3 on the 10M collision
+    "bh_matched_10m": dict(n=10_000_000, algorithm="barnes_hut", theta=0.5, eps=0.01, dt=1e-3,
+                           ic="collision", steps=10, order=1, matched=True, correction=True,
+                           reference_theta=0.5, reference_steps=1),
     "bh_collision_1m": dict(n=1_000_000, algorithm="barnes_hut", theta=0.7, eps=0.01, dt=1e-3,
-                            ic="collision", steps=10, order=1),
+                            ic="collision", steps=10, order=1, reference_theta=0.7,
+                            reference_steps=3),
     "allpairs_plummer_16k": dict(n=16384, algorithm="all_pairs", eps=0.01, dt=1e-3,
-                                 ic="plummer", steps=3),
+                                 ic="plummer", steps=3, reference_steps=3),
     "allpairs_precision_262k": dict(n=262144, algorithm="all_pairs", eps=1e-3, dt=1e-4,
-                                    ic="uniform_log_mass", steps=3),
+                                    ic="uniform_log_mass", steps=100, reference_steps=1),
     "ensemble_4096": dict(n=None, algorithm="ensemble", systems=4096, lo=32, hi=4096, eps=0.01,
                           dt=1e-3, ic="ensemble", steps=1000),
-    "bh_matched_10m": dict(n=10_000_000, algorithm="barnes_hut", theta=0.5, eps=0.01, dt=1e-3,
-                           ic="collision", steps=3, order=1, matched=True, correction=True),
     # one system split by targets over the ranks (strong scaling; NCCL all-gather per step)
     "allpairs_sharded_262k": dict(n=262144, algorithm="all_pairs_sharded", eps=1e-3, dt=1e-4,
                                   ic="uniform_log_mass", steps=3),
@@ -78,6 +91,9 @@ WORKLOADS = {
     "ensemble_4096_sharded": dict(n=None, algorithm="ensemble", systems=4096, lo=32, hi=4096,
                                   eps=0.01, dt=1e-3, ic="ensemble", steps=1000, sharded=True),
 }
+# compact sub-records of the default run: the other single-GPU configurations
+SECONDARY = ("bh_collision_1m", "allpairs_plummer_16k", "allpairs_precision_262k",
+             "ensemble_4096")
 
 # Matched-accuracy study: the largest opening angle of this grid whose rms
 # relative force error (FP64 direct sum on 4096 seeded targets, initial state)
@@ -85,13 +101,23 @@ WORKLOADS = {
 RMS_TARGET = 1e-3
 THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 0.725, 0.75, 0.8,
               0.9, 1.0)
+# relative opening test over the reference test at theta 1.0: the alphas of its sweep
+ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
+              0.007, 0.01)
+OPENINGS = {"reference": 0, "offset": 1}
+N_TARGETS = 4096  # seeded targets of the FP64 direct-sum oracle
+# energy drift needs the O(N^2) FP64 potential: measured directly up to
+# DRIFT_MAX_N particles, on the DRIFT_N-particle twin of the workload above
+DRIFT_MAX_N = 2_000_000
+DRIFT_N = 1_000_000
+DRIFT_STEPS = 10
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
 # capture of exactly this configuration (the file under profiles/ gives the command).
 PROFILED_TRAFFIC = {
-    ("bh_collision_1m", 0.7, 1, "lists", 16): (
+    ("bh_collision_1m", 0.7, 1, "lists", 16, 0.0): (
         30_559_232, "profiles/walk_lists_kernel_bh_collision_1m.md"),
-    ("allpairs_plummer_16k", None, 1, "lists", 16): (
+    ("allpairs_plummer_16k", None, 1, "lists", 16, 0.0): (
         296_960, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
 }
 
@@ -102,11 +128,38 @@ MLP_FLOPS = 2 * (10 * 64 + 64 * 64 + 64 * 3)  # 9,856: one forward pass of the 1
 
 
 # ---------------------------------------------------------------------------
-# initial conditions (numpy; statistically the reference's Plummer preset,
-# src/c/generation/presets.c:144-202, not its RNG stream)
+# initial conditions
 # ---------------------------------------------------------------------------
 
+def device_initial_state(nb, wl, seed, device=0):
+    """The workload's initial state generated on the device by the library
+    (the reference's parallel-preset streams) and brought to the host, so every
+    method and the e2e loop start from the same arrays."""
+    n = wl["n"]
+    with nb.CudaContext() as ctx:
+        if wl["ic"] == "collision":
+            ctx.generate_plummer_collision(n, seed)
+        elif wl["ic"] == "plummer":
+            ctx.generate_preset("globular_cluster", n, seed)
+        else:
+            raise ValueError(wl["ic"])
+        s = nb.ParticleSystem.zeros(n)
+        ctx.download(s)
+    return s
+
+
+def uniform_log_mass(n, seed=42):
+    """Positions uniform in [0, 1)^3, masses 10^U(-3, 0) normalised to sum 1, at
+    rest (the precision study's state; the reference has no such preset)."""
+    rng = np.random.default_rng(seed)
+    pos = rng.random((n, 3))
+    m = 10.0 ** rng.uniform(-3.0, 0.0, n)
+    return pos, np.zeros((n, 3)), m / m.sum()
+
+
 def plummer_block(rng, n, a, mass, centre):
+    """A Plummer sphere drawn with numpy (the ensemble's systems): statistically
+    the reference's Plummer preset (presets.c:144-202), not its random stream."""
     u = 1.0 - rng.random(n)
     r = a / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
     d = rng.standard_normal((n, 3))
@@ -118,22 +171,44 @@ def plummer_block(rng, n, a, mass, centre):
     return pos, vel, np.full(n, mass / n)
 
 
-def initial_conditions(kind, n, seed=42):
-    rng = np.random.default_rng(seed)
-    if kind == "plummer":
-        return plummer_block(rng, n, 1.0, 1.0, (0.0, 0.0, 0.0))
-    if kind == "collision":
-        h = n // 2
-        p1, v1, m1 = plummer_block(rng, h, 1.0, 0.5, (-5.0, 0.0, 0.0))
-        p2, v2, m2 = plummer_block(rng, n - h, 1.0, 0.5, (5.0, 0.0, 0.0))
-        v1[:, 1] -= 0.15
-        v2[:, 1] += 0.15
-        return np.vstack([p1, p2]), np.vstack([v1, v2]), np.concatenate([m1, m2])
-    if kind == "uniform_log_mass":
-        pos = rng.random((n, 3))
-        m = 10.0 ** rng.uniform(-3.0, 0.0, n)
-        return pos, np.zeros((n, 3)), m / m.sum()
-    raise ValueError(kind)
+def initial_state(nb, wl, seed, device=0):
+    if wl["ic"] == "uniform_log_mass":
+        return nb.ParticleSystem.from_arrays(*uniform_log_mass(wl["n"], seed))
+    return device_initial_state(nb, wl, seed, device)
+
+
+def reference_initial_state(wl, seed):
+    """The same initial state for the reference arm, from the CPU restatement of
+    the reference's parallel-preset generator (bit-identical integer streams;
+    FP64 transcendentals from the host libm, so within a few ulp of the
+    device's)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n = wl["n"]
+    if wl["ic"] == "collision":
+        p = O.plummer_collision_parallel(n, seed)
+    elif wl["ic"] == "plummer":
+        p = O.preset_parallel("globular_cluster", n, seed)
+    else:
+        pos, vel, mass = uniform_log_mass(n, seed)
+        p = O.Particles.zeros(n)
+        p.x[:], p.y[:], p.z[:] = pos.T
+        p.vx[:], p.vy[:], p.vz[:] = vel.T
+        p.m[:] = mass
+    return p
+
+
+def seeded_targets(n, seed=11):
+    return np.random.default_rng(seed).choice(n, min(N_TARGETS, n), replace=False)
+
+
+def rms_and_max(acc, ref):
+    """rms relative error (barnes_hut_test.c:38-57) and the largest per-target
+    relative error |a - a_ref| / |a_ref|."""
+    rms = float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
+    mx = float(np.max(np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+    return rms, mx
 
 
 # ---------------------------------------------------------------------------
@@ -270,10 +345,13 @@ def max_over_ranks(value, world):
 # reference arm / CPU baseline (the reference engine compiled from its sources)
 # ---------------------------------------------------------------------------
 
-def reference_steps(wl, pos, vel, mass, steps, threads):
-    """Time `steps` leapfrog steps of the reference engine on this host:
-    n_body_sim_pro_integrator_advance with its Barnes-Hut (or OpenMP AVX all-pairs)
-    force function.  Returns seconds per step."""
+def reference_run(wl, particles, steps, threads, theta=None):
+    """The reference engine on this host: its force function on the initial
+    state (the accelerations a leapfrog run starts from), then `steps` calls of
+    n_body_sim_pro_integrator_advance(LEAPFROG) with that force function
+    (Barnes-Hut at `theta`, or the OpenMP AVX-512 all-pairs sum).  `particles`
+    (an oracle.Particles) is advanced in place.  Returns the initial
+    accelerations, the initial force call's seconds and the seconds per step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -281,34 +359,35 @@ def reference_steps(wl, pos, vel, mass, steps, threads):
         raise RuntimeError("oracle/_ref not built")
     os.environ["OMP_NUM_THREADS"] = str(threads)
     R = O.ref()
-    p = O.Particles.zeros(mass.shape[0])
-    p.x[:], p.y[:], p.z[:] = pos.T
-    p.vx[:], p.vy[:], p.vz[:] = vel.T
-    p.m[:] = mass
     g = O.Gravity()
     R.n_body_sim_pro_gravity_init(C.byref(g), 1.0, wl["eps"])
     err = O.Error()
-    v = p.view()
+    v = particles.view()
     ctx = None
     if wl["algorithm"] == "barnes_hut":
         ctx = R.n_body_sim_pro_barnes_hut_tree_create(C.byref(err))
-        R.n_body_sim_pro_barnes_hut_tree_set_theta(ctx, wl["theta"])
+        R.n_body_sim_pro_barnes_hut_tree_set_theta(ctx, wl["theta"] if theta is None else theta)
         fn = R.n_body_sim_pro_barnes_hut_compute_acceleration
     else:
         fn = R.n_body_sim_pro_gravity_compute_acceleration_openmp_avx512
     force = C.cast(fn, C.c_void_p)
-    if fn(C.byref(v), C.byref(g), ctx, C.byref(err)) != 0:  # initial forces
-        raise RuntimeError(err.message)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        rc = R.n_body_sim_pro_integrator_advance(C.byref(v), C.byref(g), 1, wl["dt"], force, ctx,
-                                                 C.byref(err))
-        if rc != 0:
+    try:
+        t0 = time.perf_counter()
+        if fn(C.byref(v), C.byref(g), ctx, C.byref(err)) != 0:
             raise RuntimeError(err.message)
-    dt = (time.perf_counter() - t0) / steps
-    if ctx is not None:
-        R.n_body_sim_pro_barnes_hut_tree_destroy(ctx)
-    return dt
+        first = time.perf_counter() - t0
+        acc0 = particles.acc().copy()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            rc = R.n_body_sim_pro_integrator_advance(C.byref(v), C.byref(g), 1, wl["dt"], force,
+                                                     ctx, C.byref(err))
+            if rc != 0:
+                raise RuntimeError(err.message)
+        per_step = (time.perf_counter() - t0) / max(steps, 1)
+    finally:
+        if ctx is not None:
+            R.n_body_sim_pro_barnes_hut_tree_destroy(ctx)
+    return acc0, first, per_step
 
 
 def cpu_model():
@@ -323,167 +402,41 @@ def cpu_model():
 
 
 # ---------------------------------------------------------------------------
-# our arm
+# Barnes-Hut methods
 # ---------------------------------------------------------------------------
 
-def run_ours(args, wl, world, rank, local):
-    import torch
-
-    import n_body_sim_pro_b200 as nb
-
-    n = wl["n"]
-    pos, vel, mass = initial_conditions(wl["ic"], n, seed=42 + rank)
-    g = nb.gravity_init(1.0, wl["eps"])
-    algo = nb.Algorithm.BARNES_HUT if wl["algorithm"] == "barnes_hut" else nb.Algorithm.ALL_PAIRS
-    ctx = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1),
-                         leaf_capacity=wl.get("leaf"))
-    ctx.set_walk(0 if wl.get("walk") == "stackless" else 1)
-    system = nb.ParticleSystem.from_arrays(pos, vel, mass)
-    ctx.upload(system)
-    ctx.compute_acceleration(g, algo)
-    q0, pe0 = ctx.diagnostics(g, potential=True) if n <= 2_000_000 else (ctx.diagnostics(g), None)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
-
-    for _ in range(args.warmup):
-        ctx.advance(g, wl["dt"], 1, algo)
-    barrier_sync(world)
-    launches0 = nb.kernel_launches()
-    step_ms, walk_ms, stats_acc, phases = [], [], [], []
-    torch.cuda.nvtx.range_push("timed_steps")  # profilers can select the timed launches
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            ctx.advance(g, wl["dt"], 1, algo)
-            t = ctx.timings()
-            step_ms.append(t["total_ms"])
-            walk_ms.append(t["walk_ms"])
-            phases.append(t)
-            st = ctx.stats()
-            st["walk_restarts"] = ctx.walk_restarts()
-            stats_acc.append(st)
-    torch.cuda.nvtx.range_pop()
-    launches = nb.kernel_launches() - launches0
-    barrier_sync(world)
-    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
-
-    # accuracy of the final state: forces vs the FP64 device oracle on 4096 targets
-    ctx.compute_acceleration(g, algo)
-    final = nb.ParticleSystem.zeros(n)
-    ctx.download(final)
-    targets = np.random.default_rng(7).choice(n, min(4096, n), replace=False)
-    ref = ctx.reference_acceleration(g, targets)
-    acc = final.acc()[targets]
-    rms = float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
-    max_rel = float(np.max(np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)))
-    drift = None
-    if pe0 is not None:
-        q1, pe1 = ctx.diagnostics(g, potential=True)
-        drift = float(abs((q1[0] + pe1) - (q0[0] + pe0)) / abs(q0[0] + pe0))
-
-    # dominant kernel roofline
-    peaks, peak_kind = measured_peaks()
-    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
-    clk = clocks.summary()
-    mhz_load = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
-    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
-    if wl["algorithm"] == "barnes_hut":
-        approx = np.mean([s["accepted_approximations"] for s in stats_acc])
-        exact = np.mean([s["exact_interactions"] for s in stats_acc])
-        flops = FLOPS_PAIR * exact + (FLOPS_PAIR if wl.get("order", 1) == 1 else FLOPS_QUAD) * approx
-        kernel_ms = float(np.mean(walk_ms))
-        kernel = "walk_kernel"
-        interactions = approx + exact
-    else:
-        flops = FLOPS_PAIR * float(n) * float(n)
-        kernel_ms = float(np.mean(walk_ms)) if np.mean(walk_ms) > 0 else total_ms / args.steps
-        kernel = "allpairs_force_kernel"
-        interactions = float(n) * n
-    achieved = flops / (kernel_ms * 1e-3) / 1e12
-    try:
-        probe = nb.measure_fp32_peak()
-    except nb.CudaError:
-        probe = None
-    roofline = {"bound": "fp32", "kernel": kernel, "achieved": round(achieved, 3),
-                "probe": probe,
-                "peak": round(peak_max, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak_max, 4),
-                "frac_at_load_clock": round(achieved / fp32_peak_tflops(sm_count, mhz_load), 4),
-                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x {peaks.get('sm_max_mhz', 1965.0)} MHz "
-                             f"(sm_max_mhz of {peak_kind} MEASURED_PEAKS.json)",
-                "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4),
-                "traffic": None}
-    measured = PROFILED_TRAFFIC.get((args.workload, wl.get("theta"), wl.get("order", 1),
-                                     wl.get("walk", "lists"), wl.get("leaf", 16)))
-    if measured is not None:
-        roofline["traffic"] = measured[0]
-        roofline["traffic_source"] = measured[1]
-    stages = None
-    if wl["algorithm"] == "barnes_hut" and phases:
-        hbm = float(peaks.get("hbm_gbs", 6650.0))
-        nodes = float(stats_acc[-1]["node_count"])
-        # the moments pass: the monopole walk's reads each particle once and
-        # writes 64 B per node (FP64 moments, the walk's float4, opening
-        # terms), reading 52 (record, level, children's moments); the
-        # quadrupole pass reads the particles twice, writes 156 and reads 108
-        quad = wl.get("order", 1) == 2
-        mom_bytes = (32.0 * n + 264.0 * nodes) if quad else (16.0 * n + 116.0 * nodes)
-        stages = {}
-        for name, key, nbytes in (
-                ("bounds", "bounds_ms", 32.0 * n),
-                ("keys", "keys_ms", 36.0 * n),
-                ("sort", "sort_ms", 8 * 24.0 * n),
-                ("moments", "moments_ms", mom_bytes),
-                ("integrate", "integrate_ms", 36.0 * n + 24.0 * n + 120.0 * n)):
-            ms = float(np.mean([ph[key] for ph in phases]))
-            gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
-            stages[name] = {"ms": round(ms, 4), "algorithmic_bytes": nbytes,
-                            "gbs": round(gbs, 1) if gbs else None,
-                            "frac_of_hbm": round(gbs / hbm, 4) if gbs else None}
-        stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes: "
-                           "bounds 32/particle, keys 24+12, sort 8 passes x (12+12), moments "
-                           + ("2 x 16 per particle + 264 per node" if quad else
-                              "16 per particle + 116 per node")
-                           + ", integrate scatter 36 + kick-drift 24 + 120 per particle")
-
-    # e2e through the plugin call on pinned host arrays
-    e2e = None
-    if rank == 0 or world > 1:
-        e2e = run_e2e(nb, wl, pos, vel, mass, min(args.steps, 5), algo, ctx)
-
-    ctx.close()
-    matched = None
-    if wl["algorithm"] == "barnes_hut" and not args.no_matched:
-        matched = matched_study(nb, torch, wl, system, g, min(args.steps, 5), 3, flush,
-                                with_correction=wl.get("correction", False))
-    value = world * n * args.steps / (total_ms * 1e-3)
-    split = None
-    if wl["algorithm"] == "barnes_hut":  # particle-cell and particle-particle terms apart
-        per_s = world * args.steps / (total_ms * 1e-3)
-        split = {"particle_cell_per_s": approx * per_s, "particle_particle_per_s": exact * per_s}
-    return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
-                roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
-                interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
-                interactions_split=split,
-                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms, phases),
-                matched=matched, stages=stages)
+def method(name, theta, order=1, opening="reference", alpha=0.0, leaf=16, corrected=False):
+    """One Barnes-Hut configuration of the library's context."""
+    return {"name": name, "theta": theta, "multipole_order": order, "opening": opening,
+            "relative_alpha": alpha, "leaf_capacity": leaf, "corrected": corrected}
 
 
-def rms_at_targets(nb, ctx, g, n, targets, ref):
+def make_context(nb, m, correction=None):
+    ctx = nb.CudaContext(theta=m["theta"], multipole_order=m["multipole_order"],
+                         opening=OPENINGS[m["opening"]], leaf_capacity=m["leaf_capacity"])
+    ctx.set_relative_opening(m["relative_alpha"])
+    if m["corrected"]:
+        if correction is None:
+            raise ValueError("a corrected method needs its trained network")
+        ctx.set_correction(correction)
+    return ctx
+
+
+def accuracy(nb, ctx, g, targets, ref):
+    """rms / max relative error of the resident state's Barnes-Hut forces on
+    `targets` against the FP64 direct sum `ref`.  The relative opening test
+    reads the previous evaluation's accelerations (as in a run), so the forces
+    are evaluated twice."""
     ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
-    acc = ctx.download_accelerations()[targets]
-    return float(np.sqrt(np.sum((acc - ref) ** 2) / np.sum(ref ** 2)))
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    return rms_and_max(ctx.download_accelerations()[targets], ref)
 
 
-def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, correction=None,
-                opening=0, alpha=0.0, leaf=16):
-    """Device-timed 1-step advances from `system` (re-uploaded) at (theta, order, opening,
-    relative tolerance alpha, bucket capacity)."""
-    ctx = nb.CudaContext(theta=theta, multipole_order=order, opening=opening,
-                         leaf_capacity=leaf)
-    ctx.set_correction(correction)
-    ctx.set_relative_opening(alpha)
+def timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction=None):
+    """Device-timed 1-step advances of `system` (uploaded afresh) with method `m`."""
+    ctx = make_context(nb, m, correction)
     ctx.upload(system)
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
     for _ in range(warmup):
         ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
     ms = []
@@ -496,142 +449,445 @@ def timed_steps(nb, torch, system, g, wl, theta, order, steps, warmup, flush, co
     return wl["n"] * steps / (sum(ms) * 1e-3), float(np.mean(ms))
 
 
-OPENINGS = {"reference": 0, "offset": 1}
-# relative opening test (G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)) over the
-# reference test at theta 1.0: the alphas of its sweep
-ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
-              0.007, 0.01)
+def energy_drift(nb, system, g, wl, m, steps, correction=None):
+    """|E(steps) - E(0)| / |E(0)| of `system` advanced with method `m`: kinetic
+    energy plus the O(N^2) FP64 device potential (numerics.c:83-116)."""
+    ctx = make_context(nb, m, correction)
+    ctx.upload(system)
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    q0, pe0 = ctx.diagnostics(g, potential=True)
+    ctx.advance(g, wl["dt"], steps, nb.Algorithm.BARNES_HUT)
+    q1, pe1 = ctx.diagnostics(g, potential=True)
+    ctx.close()
+    e0, e1 = q0[0] + pe0, q1[0] + pe1
+    return float(abs(e1 - e0) / abs(e0))
 
 
-def matched_study(nb, torch, wl, system, g, steps, warmup, flush, with_correction=False):
-    """Plain Barnes-Hut (monopole, the reference's opening test, 16-particle
-    buckets) vs the chosen method — the fastest of {monopole, quadrupole} x
-    {reference, offset opening test}, the monopole walk with 32-particle buckets,
-    and the relative test over the reference test at theta 1.0 with 16- and
-    32-particle buckets — each at the largest theta (alpha) of its grid meeting
-    RMS_TARGET, all timed; optionally the learned correction at theta 1.0
-    (trained on 2^22 pairs of the 1M collision) under either opening test and
-    the plain walk at theta 0.5."""
-    n = wl["n"]
-    targets = np.random.default_rng(11).choice(n, min(4096, n), replace=False)
+def train_correction(nb, g, opening, n_train=1_000_000, samples=1 << 22, seed=42):
+    """The learned correction, trained on the GPU on 2^22 cell-target pairs of
+    the 1M collision (labels: exact cell sums by the all-pairs arithmetic)."""
+    corr = nb.CudaCorrection(seed=11)
+    with nb.CudaContext(theta=1.0, opening=OPENINGS[opening]) as c1:
+        c1.generate_plummer_collision(n_train, seed)
+        t0 = time.time()
+        corr.generate(c1, g, theta=1.0, samples=samples, seed=3)
+        _, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
+        seconds = time.time() - t0
+    return corr, {"pairs": samples, "from": f"collision N={n_train}", "epochs": 8,
+                  "final_validation_loss": float(vl[-1]), "seconds": round(seconds, 2)}
+
+
+def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
+                  with_correction=False):
+    """Every method at its largest theta (alpha) of the grid meeting RMS_TARGET
+    on the initial state, timed; the plain walk at theta 0.5 and the learned
+    correction at theta 1.0 timed as well.  Returns the record and the trained
+    corrections (kept alive for the timed region)."""
     ctx = nb.CudaContext(theta=0.5)
     ctx.upload(system)
-    ref = ctx.reference_acceleration(g, targets)
-    table = {}
-    for oname, opening in OPENINGS.items():
-        ctx.set_opening(opening)
+    sweep = {}
+    for oname in OPENINGS:
         for order in (1, 2):
-            ctx.set_multipole_order(order)
             rows = []
             for th in THETA_GRID:
                 ctx.theta = th
-                rows.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
-            table[(order, oname)] = rows
+                ctx.set_multipole_order(order)
+                ctx.set_opening(OPENINGS[oname])
+                r = accuracy(nb, ctx, g, targets, ref)
+                rows.append((th, r))
+            sweep[f"order{order}_{oname}"] = rows
     ctx.set_opening(0)
     ctx.set_multipole_order(1)
     ctx.set_leaf_capacity(32)
-    table_leaf32 = []
+    rows = []
     for th in THETA_GRID:
         ctx.theta = th
-        table_leaf32.append((th, rms_at_targets(nb, ctx, g, n, targets, ref)))
-    ctx.set_leaf_capacity(16)
-    # relative test: each alpha evaluated twice, the second walk reading the
-    # first one's accelerations as a_old (as in a run, where a_old is the
-    # previous step's)
-    ctx.set_opening(0)
-    ctx.set_multipole_order(1)
+        rows.append((th, accuracy(nb, ctx, g, targets, ref)))
+    sweep["order1_reference_leaf32"] = rows
     ctx.theta = 1.0
-    rel_rows = {}
     for leaf in (16, 32):
         ctx.set_leaf_capacity(leaf)
         rows = []
         for alpha in ALPHA_GRID:
             ctx.set_relative_opening(alpha)
-            ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
-            rows.append((alpha, rms_at_targets(nb, ctx, g, n, targets, ref)))
-        rel_rows[leaf] = rows
+            rows.append((alpha, accuracy(nb, ctx, g, targets, ref)))
+        sweep[f"order1_relative_alpha_theta1.0_leaf{leaf}"] = rows
     ctx.set_relative_opening(0.0)
     ctx.close()
-    out = {"rms_target": RMS_TARGET, "oracle": "FP64 device direct sum, 4096 seeded targets, "
-           "initial state",
-           "sweep": {f"order{o}_{on}": [[t, round(r, 6)] for t, r in rows]
-                     for (o, on), rows in table.items()}}
-    out["sweep"]["order1_reference_leaf32"] = [[t, round(r, 6)] for t, r in table_leaf32]
-    for leaf, rows in rel_rows.items():
-        out["sweep"][f"order1_relative_alpha_theta1.0_leaf{leaf}"] = [[a, round(r, 6)]
-                                                                      for a, r in rows]
-    methods = {}
-    for (order, oname), rows in table.items():
-        ok = [t for t, r in rows if r <= RMS_TARGET]
-        if not ok:
-            continue
-        th = max(ok)
-        v, ms = timed_steps(nb, torch, system, g, wl, th, order, steps, warmup, flush,
-                            opening=OPENINGS[oname])
-        methods[(order, oname)] = {"theta": th, "multipole_order": order, "opening": oname,
-                                   "leaf_capacity": 16, "rms": dict(rows)[th], "value": v,
-                                   "ms_per_step": round(ms, 4)}
-    ok = [t for t, r in table_leaf32 if r <= RMS_TARGET]
-    if ok:
-        th = max(ok)
-        v, ms = timed_steps(nb, torch, system, g, wl, th, 1, steps, warmup, flush, leaf=32)
-        methods[(1, "reference", 32)] = {"theta": th, "multipole_order": 1,
-                                         "opening": "reference", "leaf_capacity": 32,
-                                         "rms": dict(table_leaf32)[th], "value": v,
-                                         "ms_per_step": round(ms, 4)}
-    for leaf, rows in rel_rows.items():
-        ok = [a for a, r in rows if r <= RMS_TARGET]
-        if not ok:
-            continue
-        alpha = max(ok)
-        v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush, alpha=alpha,
-                            leaf=leaf)
-        methods[(1, "relative", leaf)] = {"theta": 1.0, "multipole_order": 1,
-                                          "opening": "reference", "relative_alpha": alpha,
-                                          "leaf_capacity": leaf, "rms": dict(rows)[alpha],
-                                          "value": v, "ms_per_step": round(ms, 4)}
-    out["methods"] = list(methods.values())
-    out["plain"] = methods.get((1, "reference"))
-    out["chosen"] = max(methods.values(), key=lambda m: m["value"]) if methods else None
+
+    def best(rows):
+        ok = [(x, r) for x, r in rows if r[0] <= RMS_TARGET]
+        return max(ok, key=lambda t: t[0]) if ok else None
+
+    candidates = []
+    for (order, oname) in ((1, "reference"), (2, "reference"), (1, "offset"), (2, "offset")):
+        b = best(sweep[f"order{order}_{oname}"])
+        if b:
+            candidates.append((method(f"order{order}_{oname}", b[0], order, oname), b[1]))
+    b = best(sweep["order1_reference_leaf32"])
+    if b:
+        candidates.append((method("order1_reference_leaf32", b[0], leaf=32), b[1]))
+    for leaf in (16, 32):
+        b = best(sweep[f"order1_relative_alpha_theta1.0_leaf{leaf}"])
+        if b:
+            candidates.append((method(f"relative_leaf{leaf}", 1.0, alpha=b[0], leaf=leaf), b[1]))
+
+    def timed(m, r, correction=None):
+        v, ms = timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction)
+        return dict(m, rms=r[0], max_rel=r[1], value=v, ms_per_step=round(ms, 4))
+
+    methods = [timed(m, r) for m, r in candidates]
+    out = {"rms_target": RMS_TARGET,
+           "oracle": f"FP64 device direct sum, {len(targets)} seeded targets, initial state",
+           "sweep": {k: [[x, round(r[0], 6)] for x, r in rows] for k, rows in sweep.items()},
+           "methods": methods}
+    out["plain"] = next((m for m in methods if m["name"] == "order1_reference"), None)
+    rel = [m for m in methods if m["name"].startswith("relative")]
+    out["relative"] = max(rel, key=lambda m: m["value"]) if rel else None
+    corrections = {}
+    if with_correction:
+        r05 = dict(sweep["order1_reference"])[0.5]
+        out["plain_theta_0.5"] = timed(method("plain_theta_0.5", 0.5), r05)
+        corrected = {}
+        for oname in OPENINGS:
+            corr, training = train_correction(nb, g, oname)
+            corrections[oname] = corr
+            m = method(f"corrected_{oname}", 1.0, opening=oname, corrected=True)
+            cctx = make_context(nb, m, corr)
+            cctx.upload(system)
+            r = accuracy(nb, cctx, g, targets, ref)
+            evals = cctx.corrected_cells()  # network evaluations of that walk
+            walk_ms = cctx.timings()["walk_ms"]
+            cctx.close()
+            rec = timed(m, r, corr)
+            rec["uncorrected_rms_at_theta_1.0"] = dict(sweep[f"order1_{oname}"])[1.0][0]
+            rec["network"] = {"evaluations_per_walk": evals, "flop_per_evaluation": MLP_FLOPS,
+                              "walk_ms": round(walk_ms, 4),
+                              "tensor_tflops_in_walk": round(evals * MLP_FLOPS / (walk_ms * 1e-3)
+                                                             / 1e12, 3) if walk_ms > 0 else None}
+            rec["training"] = training
+            corrected[oname] = rec
+            if r[0] <= RMS_TARGET:
+                methods.append(rec)
+        out["corrected_theta_1.0"] = corrected
+    out["chosen"] = max(methods, key=lambda m: m["value"]) if methods else None
     if out["plain"] and out["chosen"]:
         out["chosen_over_plain"] = round(out["chosen"]["value"] / out["plain"]["value"], 3)
-    if with_correction:
-        v, ms = timed_steps(nb, torch, system, g, wl, 0.5, 1, steps, warmup, flush)
-        out["plain_theta_0.5"] = {"theta": 0.5, "rms": dict(table[(1, "reference")])[0.5],
-                                  "value": v, "ms_per_step": round(ms, 4)}
-        pos1, vel1, mass1 = initial_conditions("collision", 1_000_000, seed=42)
-        system1 = nb.ParticleSystem.from_arrays(pos1, vel1, mass1)
-        corrected = {}
-        for oname, opening in OPENINGS.items():
-            with nb.CudaContext(theta=1.0, opening=opening) as c1, \
-                    nb.CudaCorrection(seed=11) as corr:
-                c1.upload(system1)
-                t0 = time.time()
-                corr.generate(c1, g, theta=1.0, samples=1 << 22, seed=3)
-                tl, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
-                train_s = time.time() - t0
-                cctx = nb.CudaContext(theta=1.0, opening=opening)
-                cctx.set_correction(corr)
-                cctx.upload(system)
-                rms_c = rms_at_targets(nb, cctx, g, n, targets, ref)
-                evals = cctx.corrected_cells()  # network evaluations of that walk
-                walk_ms = cctx.timings()["walk_ms"]
-                cctx.close()
-                v, ms = timed_steps(nb, torch, system, g, wl, 1.0, 1, steps, warmup, flush,
-                                    correction=corr, opening=opening)
-            corrected[oname] = {
-                "theta": 1.0, "opening": oname, "rms": rms_c, "value": v,
-                "ms_per_step": round(ms, 4),
-                "uncorrected_rms_at_theta_1.0": dict(table[(1, oname)])[1.0],
-                "network": {"evaluations_per_walk": evals, "flop_per_evaluation": MLP_FLOPS,
-                            "walk_ms": round(walk_ms, 4),
-                            "tensor_tflops_in_walk": round(evals * MLP_FLOPS / (walk_ms * 1e-3)
-                                                           / 1e12, 3) if walk_ms > 0 else None},
-                "training": {"pairs": 1 << 22, "from": "collision N=1M", "epochs": 8,
-                             "final_validation_loss": float(vl[-1]),
-                             "seconds": round(train_s, 2)}}
-        out["corrected_theta_1.0"] = corrected
-    return out
+    if out.get("plain_theta_0.5") and out["chosen"]:
+        out["chosen_over_plain_theta_0.5"] = round(
+            out["chosen"]["value"] / out["plain_theta_0.5"]["value"], 3)
+    # energy drift of the reported methods: the O(N^2) FP64 potential is out of
+    # reach at 10M within a bench run, so each method's settings advance the 1M
+    # collision (same generator and seed) over DRIFT_STEPS steps
+    if wl["n"] > DRIFT_MAX_N:
+        wl1 = dict(wl, n=DRIFT_N)
+        small = initial_state(nb, wl1, 42)
+        note = f"the method's settings on the {DRIFT_N}-particle collision, {DRIFT_STEPS} steps"
+    else:
+        wl1, small, note = wl, system, f"{wl['n']} particles, {DRIFT_STEPS} steps"
+    reported = [out.get("plain_theta_0.5"), out["plain"], out["relative"], out["chosen"]]
+    reported += list(out.get("corrected_theta_1.0", {}).values())
+    for rec in reported:
+        if rec is not None and "energy_drift" not in rec:
+            corr = corrections.get(rec["opening"]) if rec["corrected"] else None
+            rec["energy_drift"] = energy_drift(nb, small, g, wl1, rec, DRIFT_STEPS, corr)
+            rec["energy_drift_over"] = note
+    return out, corrections
+
+
+def run_bh(args, wl, world, rank, local, steps, warmup, with_e2e=True):
+    """A Barnes-Hut workload: its method (the matched study's choice, or the
+    workload's plain theta), K timed steps, accuracy, drift, roofline, stages."""
+    import torch
+
+    import n_body_sim_pro_b200 as nb
+
+    n = wl["n"]
+    system = initial_state(nb, wl, 42 + rank, local)
+    g = nb.gravity_init(1.0, wl["eps"])
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    targets = seeded_targets(n)
+    with nb.CudaContext() as c0:
+        c0.upload(system)
+        ref0 = c0.reference_acceleration(g, targets)
+    study, corrections = None, {}
+    if wl.get("matched") and not args.no_matched:
+        study, corrections = matched_study(nb, torch, wl, system, g, targets, ref0,
+                                           min(steps, 5), 3, flush,
+                                           with_correction=wl.get("correction", False))
+        m = {k: study["chosen"][k] for k in ("name", "theta", "multipole_order", "opening",
+                                             "relative_alpha", "leaf_capacity", "corrected")}
+    else:
+        m = method("plain", wl["theta"], wl.get("order", 1), leaf=wl.get("leaf", 16))
+    correction = corrections.get(m["opening"]) if m["corrected"] else None
+    ctx = make_context(nb, m, correction)
+    ctx.set_walk(0 if wl.get("walk") == "stackless" else 1)
+    ctx.upload(system)
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    q0, pe0 = ctx.diagnostics(g, potential=True) if n <= 2_000_000 else (None, None)
+
+    for _ in range(warmup):
+        ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
+    barrier_sync(world)
+    launches0 = nb.kernel_launches()
+    step_ms, walk_ms, stats_acc, phases = [], [], [], []
+    torch.cuda.nvtx.range_push("timed_steps")  # profilers can select the timed launches
+    with ClockSampler(local) as clocks:
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
+            t = ctx.timings()
+            step_ms.append(t["total_ms"])
+            walk_ms.append(t["walk_ms"])
+            phases.append(t)
+            st = ctx.stats()
+            st["walk_restarts"] = ctx.walk_restarts()
+            stats_acc.append(st)
+    torch.cuda.nvtx.range_pop()
+    launches = nb.kernel_launches() - launches0
+    barrier_sync(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+
+    # accuracy of the final state: forces vs the FP64 device direct sum
+    ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
+    final = nb.ParticleSystem.zeros(n)
+    ctx.download(final)
+    with nb.CudaContext() as c1:
+        c1.upload(final)
+        ref1 = c1.reference_acceleration(g, targets)
+    rms, max_rel = rms_and_max(final.acc()[targets], ref1)
+    drift, drift_note = None, None
+    if pe0 is not None:
+        q1, pe1 = ctx.diagnostics(g, potential=True)
+        drift = float(abs((q1[0] + pe1) - (q0[0] + pe0)) / abs(q0[0] + pe0))
+        drift_note = f"{n} particles over the {warmup} warm-up + {steps} timed steps"
+
+    peaks, peak_kind = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    clk = clocks.summary()
+    mhz_load = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
+    approx = float(np.mean([s["accepted_approximations"] for s in stats_acc]))
+    exact = float(np.mean([s["exact_interactions"] for s in stats_acc]))
+    flops = FLOPS_PAIR * exact + (FLOPS_PAIR if m["multipole_order"] == 1 else FLOPS_QUAD) * approx
+    kernel_ms = float(np.mean(walk_ms))
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    try:
+        probe = nb.measure_fp32_peak()
+    except nb.CudaError:
+        probe = None
+    roofline = {"bound": "fp32", "kernel": "walk_lists_kernel", "achieved": round(achieved, 3),
+                "probe": probe, "peak": round(peak_max, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak_max, 4),
+                "frac_at_load_clock": round(achieved / fp32_peak_tflops(sm_count, mhz_load), 4),
+                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x "
+                             f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz of {peak_kind} "
+                             "MEASURED_PEAKS.json; it has no FP32 figure)",
+                "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None}
+    measured = PROFILED_TRAFFIC.get((args.workload, m["theta"], m["multipole_order"],
+                                     wl.get("walk", "lists"), m["leaf_capacity"],
+                                     m["relative_alpha"]))
+    if measured is not None:
+        roofline["traffic"] = measured[0]
+        roofline["traffic_source"] = measured[1]
+    stages = stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind)
+
+    e2e = run_e2e(nb, wl, system, min(steps, 5), m, correction) if with_e2e else None
+    ctx.close()
+    for c in corrections.values():
+        c.close()
+    value = world * n * steps / (total_ms * 1e-3)
+    per_s = world * steps / (total_ms * 1e-3)
+    return dict(value=value, total_ms=total_ms, rms=rms, max_rel=max_rel, drift=drift,
+                drift_note=drift_note, roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
+                interactions_per_s=(approx + exact) * per_s,
+                interactions_split={"particle_cell_per_s": approx * per_s,
+                                    "particle_particle_per_s": exact * per_s},
+                stats=stats_acc[-1], timings=ctx_timings_summary(step_ms, walk_ms, phases),
+                matched=study, stages=stages, method=m, system=system, targets=targets,
+                ref0=ref0, g=g, corrections_used=m["corrected"])
+
+
+def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
+    """Achieved HBM bandwidth of the tree-build stages and the integration, from
+    the library's per-phase CUDA events and the algorithmic bytes per particle
+    (and per node) of each stage."""
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    nodes = float(stats_acc[-1]["node_count"])
+    rel = m["relative_alpha"] > 0.0
+    quad = m["multipole_order"] == 2 or m["corrected"]
+    # moments: the monopole pass reads each particle once (16 B) and per node
+    # writes 64 B (FP64 moments, the walk's float4, opening terms) and reads 52
+    # (record, level, children's moments); the quadrupole pass reads the
+    # particles twice, writes 156 and reads 108 per node
+    mom_bytes = (32.0 * n + 264.0 * nodes) if quad else (16.0 * n + 116.0 * nodes)
+    rows = [
+        # bounds: x, y, z, m (+ the previous accelerations for the relative test)
+        ("bounds", "bounds_ms", (32.0 + (24.0 if rel else 0.0)) * n),
+        # keys: read x, y, z, m; write key 8, index 4, the walk's float4 16
+        # (+ read a_old 24, write the relative tolerance 4)
+        ("keys", "keys_ms", (32.0 + 28.0 + (28.0 if rel else 0.0)) * n),
+        # 8 LSD passes over (key 8 + index 4), read and written
+        ("sort", "sort_ms", 8 * 24.0 * n),
+        ("moments", "moments_ms", mom_bytes),
+        # unsort: inverse index 4 + one 32-byte double4 read, ax/ay/az 24 written
+        ("unsort", "integrate_ms", 60.0 * n),
+    ]
+    stages = {}
+    for name, key, nbytes in rows:
+        ms = float(np.mean([ph[key] for ph in phases]))
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        stages[name] = {"ms": round(ms, 4), "algorithmic_bytes": nbytes,
+                        "gbs": round(gbs, 1) if gbs else None,
+                        "frac_of_hbm": round(gbs / hbm, 4) if gbs else None}
+    # the two kick launches run outside the Barnes-Hut phase events: their time is
+    # the step's minus the phases'; opening kick-drift reads v, a, x (72 B) and
+    # writes v, x (48 B), the closing kick reads v, a (48 B) and writes v (24 B)
+    kick_ms = float(np.mean([ph["total_ms"] - sum(ph[k] for k in (
+        "bounds_ms", "keys_ms", "sort_ms", "build_ms", "moments_ms", "walk_ms", "integrate_ms"))
+        for ph in phases]))
+    kick_bytes = 192.0 * n
+    gbs = kick_bytes / (kick_ms * 1e-3) / 1e9 if kick_ms > 0 else None
+    stages["kick_drift"] = {"ms": round(kick_ms, 4), "algorithmic_bytes": kick_bytes,
+                            "gbs": round(gbs, 1) if gbs else None,
+                            "frac_of_hbm": round(gbs / hbm, 4) if gbs else None,
+                            "timed_as": "step total minus the Barnes-Hut phases (includes "
+                                        "launch gaps)"}
+    stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes per "
+                       "particle: bounds 32 (+24 relative), keys 32 read + 28 written (+28 "
+                       "relative), sort 8 passes x (12 + 12), moments "
+                       + ("2 x 16 + 264 per node" if quad else "16 + 116 per node")
+                       + ", unsort 4 + 32 read + 24 written, kick-drift 120 + kick 72")
+    return stages
+
+
+def run_e2e(nb, wl, system, steps, m=None, correction=None):
+    """The metric end to end through the reference-facing plugin call on pinned
+    host arrays: a host leapfrog (integrator.c:47-85) whose force function is
+    n_body_sim_pro_{barnes_hut_,gravity_}compute_acceleration_cuda through its C
+    ABI; each call copies positions and masses (and, under the relative opening
+    test, the previous accelerations) in and the accelerations out."""
+    import torch
+
+    n = wl["n"]
+    alloc = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    s = nb.ParticleSystem.zeros(n, allocator=alloc)
+    for f in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m"):
+        getattr(s, f)[:] = getattr(system, f)
+    g = nb.gravity_init(1.0, wl["eps"])
+    bh = wl["algorithm"] == "barnes_hut"
+    c2 = make_context(nb, m, correction) if bh else nb.CudaContext()
+    plugin = getattr(nb.library(), "n_body_sim_pro_barnes_hut_compute_acceleration_cuda"
+                     if bh else "n_body_sim_pro_gravity_compute_acceleration_cuda")
+    view, err = s.view(), nb.Error()
+
+    def force():
+        if plugin(C.byref(view), C.byref(g), c2.handle, C.byref(err)) != nb.Status.OK:
+            raise nb.CudaError(err.status, err.message.decode(errors="replace"))
+
+    h, dt = 0.5 * wl["dt"], wl["dt"]
+    for _ in range(3):  # warm-up of the plugin path (and the initial accelerations)
+        force()
+    tv = [torch.from_numpy(getattr(s, f)) for f in ("vx", "vy", "vz")]
+    tx = [torch.from_numpy(getattr(s, f)) for f in ("x", "y", "z")]
+    ta = [torch.from_numpy(getattr(s, f)) for f in ("ax", "ay", "az")]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for v, a in zip(tv, ta):
+            v.add_(a, alpha=h)
+        for x, v in zip(tx, tv):
+            x.add_(v, alpha=dt)
+        force()
+        for v, a in zip(tv, ta):
+            v.add_(a, alpha=h)
+    elapsed = time.perf_counter() - t0
+    c2.close()
+    rel = bh and m is not None and m["relative_alpha"] > 0.0
+    return {"value": n * steps / elapsed, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": (4 + (3 if rel else 0)) * 8 * n,
+            "d2h_bytes_per_step": 3 * 8 * n, "steps": steps,
+            "path": "host leapfrog (in-place, host threads) + the plugin force function "
+                    "through its C ABI on pinned host arrays",
+            "timer": "host wall clock"}
+
+
+# ---------------------------------------------------------------------------
+# all-pairs (one system on one GPU)
+# ---------------------------------------------------------------------------
+
+def run_allpairs(args, wl, world, rank, local, steps, warmup, with_e2e=True):
+    import torch
+
+    import n_body_sim_pro_b200 as nb
+
+    n = wl["n"]
+    system = initial_state(nb, wl, 42 + rank, local)
+    g = nb.gravity_init(1.0, wl["eps"])
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    targets = seeded_targets(n)
+    ctx = nb.CudaContext()
+    ctx.upload(system)
+    ctx.compute_acceleration(g, nb.Algorithm.ALL_PAIRS)
+    ref0 = ctx.reference_acceleration(g, targets)
+    rms0, max0 = rms_and_max(ctx.download_accelerations()[targets], ref0)
+    q0, pe0 = ctx.diagnostics(g, potential=True)
+    for _ in range(warmup):
+        ctx.advance(g, wl["dt"], 1, nb.Algorithm.ALL_PAIRS)
+    barrier_sync(world)
+    launches0 = nb.kernel_launches()
+    step_ms, force_ms = [], []
+    torch.cuda.nvtx.range_push("timed_steps")
+    with ClockSampler(local) as clocks:
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ctx.advance(g, wl["dt"], 1, nb.Algorithm.ALL_PAIRS)
+            t = ctx.timings()
+            step_ms.append(t["total_ms"])
+            force_ms.append(t["walk_ms"])
+    torch.cuda.nvtx.range_pop()
+    launches = nb.kernel_launches() - launches0
+    barrier_sync(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+    q1, pe1 = ctx.diagnostics(g, potential=True)
+    drift = float(abs((q1[0] + pe1) - (q0[0] + pe0)) / abs(q0[0] + pe0))
+    ctx.compute_acceleration(g, nb.Algorithm.ALL_PAIRS)
+    ref1 = ctx.reference_acceleration(g, targets)
+    rms, max_rel = rms_and_max(ctx.download_accelerations()[targets], ref1)
+
+    peaks, peak_kind = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    clk = clocks.summary()
+    mhz_load = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
+    flops = FLOPS_PAIR * float(n) * float(n)
+    kernel_ms = float(np.mean(force_ms))
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "allpairs_force_paired_kernel",
+                "achieved": round(achieved, 3), "peak": round(peak_max, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak_max, 4),
+                "frac_at_load_clock": round(achieved / fp32_peak_tflops(sm_count, mhz_load), 4),
+                "peak_kind": f"FP32 = {sm_count} SMs x 128 lanes x 2 x "
+                             f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz of {peak_kind} "
+                             "MEASURED_PEAKS.json; it has no FP32 figure)",
+                "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None}
+    measured = PROFILED_TRAFFIC.get((args.workload, None, 1, "lists", 16, 0.0))
+    if measured is not None:
+        roofline["traffic"] = measured[0]
+        roofline["traffic_source"] = measured[1]
+    e2e = run_e2e(nb, wl, system, min(steps, 5)) if with_e2e else None
+    ctx.close()
+    return dict(value=world * n * steps / (total_ms * 1e-3), total_ms=total_ms, rms=rms,
+                max_rel=max_rel, rms_initial=rms0, max_rel_initial=max0, drift=drift,
+                drift_note=f"{n} particles over the {warmup} warm-up + {steps} timed steps",
+                roofline=roofline, clocks=clk, launches=launches, e2e=e2e,
+                interactions_per_s=world * float(n) * n * steps / (total_ms * 1e-3),
+                stats={"particles": n},
+                timings={"step_ms_mean": round(float(np.mean(step_ms)), 4),
+                         "force_ms_mean": round(kernel_ms, 4)},
+                system=system, targets=targets, ref0=ref0, g=g)
 
 
 def ensemble_ic(wl, seed=42, systems=None):
@@ -665,7 +921,7 @@ def ensemble_sizes(wl, seed=42):
     return out
 
 
-def run_ensemble(args, wl, world, rank, local):
+def run_ensemble(args, wl, world, rank, local, steps, warmup):
     import torch
 
     import n_body_sim_pro_b200 as nb
@@ -685,13 +941,13 @@ def run_ensemble(args, wl, world, rank, local):
     ens.upload(system, offsets)
     ens.autotune(g, wl["dt"])
     launches0 = None
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         ens.advance(g, wl["dt"], 1)
     barrier_sync(world)
     launches0 = nb.kernel_launches()
     torch.cuda.nvtx.range_push("timed_steps")
     with ClockSampler(local) as clocks:
-        ms = ens.advance(g, wl["dt"], args.steps)
+        ms = ens.advance(g, wl["dt"], steps)
     torch.cuda.nvtx.range_pop()
     launches = nb.kernel_launches() - launches0
     barrier_sync(world)
@@ -708,7 +964,7 @@ def run_ensemble(args, wl, world, rank, local):
     peaks, peak_kind = measured_peaks()
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     peak_max = fp32_peak_tflops(sm_count, peaks.get("sm_max_mhz", 1965.0))
-    flops = FLOPS_PAIR * interactions * (args.steps + 1)  # + the initial force pass
+    flops = FLOPS_PAIR * interactions * (steps + 1)  # + the initial force pass
     achieved = flops / (total_ms * 1e-3) / 1e12
     clk = clocks.summary()
     roofline = {"bound": "fp32", "kernel": "ensemble_kernel", "achieved": round(achieved, 3),
@@ -719,19 +975,19 @@ def run_ensemble(args, wl, world, rank, local):
     ens.close()
     if wl.get("sharded"):
         n_all = max_over_ranks(float(sum(ensemble_sizes(wl))), world)
-        value = n_all * args.steps / (total_ms * 1e-3)
+        value = n_all * steps / (total_ms * 1e-3)
         interactions = float(sum(float(v) ** 2 for v in ensemble_sizes(wl))) / world
     else:
-        value = world * n * args.steps / (total_ms * 1e-3)
+        value = world * n * steps / (total_ms * 1e-3)
     return dict(value=value, total_ms=total_ms, rms=None, max_rel=None, drift=None,
                 roofline=roofline, clocks=clk, launches=launches, e2e=None,
-                interactions_per_s=world * interactions * args.steps / (total_ms * 1e-3),
+                interactions_per_s=world * interactions * steps / (total_ms * 1e-3),
                 stats={"systems": int(len(sizes)), "particles": int(n),
                        "ensemble": info, "one_launch_per_system": baseline},
                 timings={"advance_ms": round(ms, 3)})
 
 
-def run_sharded_allpairs(args, wl, world, rank, local):
+def run_sharded_allpairs(args, wl, world, rank, local, steps, warmup):
     """One all-pairs system split by targets over the ranks (strong scaling):
     each step is shard_begin (kick-drift-pack), an NCCL all-gather of the
     packed sources (16 bytes per particle) and shard_end (forces + kick)."""
@@ -741,7 +997,7 @@ def run_sharded_allpairs(args, wl, world, rank, local):
     from n_body_sim_pro_b200 import shard
 
     n = wl["n"]
-    pos, vel, mass = initial_conditions(wl["ic"], n, seed=42)  # the same system on every rank
+    pos, vel, mass = uniform_log_mass(n, 42)  # the same system on every rank
     first, count = shard.split(n, world)[rank]
     g = nb.gravity_init(1.0, wl["eps"])
     ctx = nb.CudaContext()
@@ -751,7 +1007,7 @@ def run_sharded_allpairs(args, wl, world, rank, local):
     sim = shard.ShardedAllPairs(part, g, shard.CudaShardBackend(ctx), device)
     sim.compute_forces()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         sim.step(wl["dt"], 1)
     barrier_sync(world)
     launches0 = nb.kernel_launches()
@@ -760,7 +1016,7 @@ def run_sharded_allpairs(args, wl, world, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed_steps")
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
             ev0.record()
@@ -816,10 +1072,10 @@ def run_sharded_allpairs(args, wl, world, rank, local):
                 "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None,
                 "all_gather_bytes_per_step": 16 * world * sim.capacity}
     ctx.close()
-    return dict(value=n * args.steps / (total_ms * 1e-3), total_ms=total_ms, rms=rms,
+    return dict(value=n * steps / (total_ms * 1e-3), total_ms=total_ms, rms=rms,
                 max_rel=max_rel, drift=None, roofline=roofline, clocks=clocks.summary(),
                 launches=launches, e2e=None,
-                interactions_per_s=float(n) * n * args.steps / (total_ms * 1e-3),
+                interactions_per_s=float(n) * n * steps / (total_ms * 1e-3),
                 stats={"particles": n, "ranks": world, "slice": count,
                        "slice_capacity": sim.capacity},
                 timings={"step_ms_mean": round(float(np.mean(step_ms)), 4),
@@ -835,53 +1091,122 @@ def ctx_timings_summary(step_ms, walk_ms, phases=()):
     return out
 
 
-def run_e2e(nb, wl, pos, vel, mass, steps, algo, ctx):
-    import torch
+def to_oracle_particles(system):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
 
+    p = O.Particles.zeros(system.n)
+    for f in O.FIELDS:
+        getattr(p, f)[:] = getattr(system, f)
+    return p
+
+
+def cpu_baseline_leg(wl, r, threads):
+    """The reference engine on this host's cores, on the very arrays our arm
+    started from: its initial force evaluation (its rms on the same 4096 targets
+    against the FP64 direct sum) and a bounded sample of leapfrog steps."""
+    unit = "particle-steps/s"
+    try:
+        p = to_oracle_particles(r["system"])
+        steps = 1 if wl["n"] >= 1_000_000 else wl.get("reference_steps", 1)
+        acc0, first, per_step = reference_run(wl, p, steps, threads,
+                                              theta=wl.get("reference_theta"))
+        rms, mx = rms_and_max(acc0[r["targets"]], r["ref0"])
+        what = (f"Barnes-Hut theta {wl.get('reference_theta')}" if wl["algorithm"] == "barnes_hut"
+                else "OpenMP AVX-512 all-pairs")
+        return {"value": wl["n"] / per_step, "unit": unit, "cores": threads, "kind": "reference",
+                "sample": f"the initial force evaluation ({first:.2f} s) and {steps} leapfrog "
+                          f"step(s) of the full {wl['n']}-particle system, reference engine "
+                          f"(oracle/_ref, {what}) with OMP_NUM_THREADS={threads} on "
+                          f"{cpu_model()}; same initial arrays as the device run",
+                "rms_rel_force_err": rms, "max_rel_force_err": mx,
+                "accuracy_oracle": "FP64 device direct sum on the same 4096 targets, "
+                                   "initial state"}
+    except Exception as exc:  # reported, not fatal
+        return {"value": None, "unit": unit, "cores": 0, "kind": "reference",
+                "sample": f"unavailable: {exc}"}
+
+
+def run_workload(args, name, wl, world, rank, local, steps, warmup, with_e2e=True):
+    if wl["algorithm"] == "ensemble":
+        return run_ensemble(args, wl, world, rank, local, steps, warmup)
+    if wl["algorithm"] == "all_pairs_sharded":
+        return run_sharded_allpairs(args, wl, world, rank, local, steps, warmup)
+    if wl["algorithm"] == "barnes_hut":
+        return run_bh(args, wl, world, rank, local, steps, warmup, with_e2e)
+    return run_allpairs(args, wl, world, rank, local, steps, warmup, with_e2e)
+
+
+def secondary_record(args, name, world, rank, local):
+    """One other configuration as a compact sub-record: its throughput at its
+    own step count, its dominant kernel's CUDA-event time and FP32 fraction,
+    its accuracy and drift."""
+    wl = dict(WORKLOADS[name])
+    sub = argparse.Namespace(**vars(args))
+    sub.workload = name
+    sub.no_matched = True
+    t0 = time.time()
+    r = run_workload(sub, name, wl, world, rank, local, wl["steps"], 3, with_e2e=False)
+    rl = r["roofline"]
+    rec = {"value": r["value"], "unit": "particle-steps/s", "steps": wl["steps"], "warmup": 3,
+           "particles": wl["n"] or r["stats"].get("particles"),
+           "ms_per_step": round(r["total_ms"] / wl["steps"], 4),
+           "kernel": rl.get("kernel"), "kernel_ms": rl.get("launch_ms"),
+           "fp32_tflops": rl.get("achieved"), "fp32_peak_frac": rl.get("frac"),
+           "rms_rel_force_err": r.get("rms"), "max_rel_force_err": r.get("max_rel"),
+           "energy_drift": r.get("drift"), "drift_over": r.get("drift_note"),
+           "interactions_per_s": r.get("interactions_per_s"), "seconds": round(time.time() - t0, 1)}
+    if wl["algorithm"] == "barnes_hut":
+        rec["theta"] = wl["theta"]
+        rec["stages_hbm"] = r.get("stages")
+    if wl["algorithm"] == "ensemble":
+        rec["one_launch_per_system"] = r["stats"]["one_launch_per_system"]
+    return rec
+
+
+def reference_arm(args, wl, metric, unit, config):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = os.cpu_count() or 1
+    if wl["algorithm"] not in ("barnes_hut", "all_pairs"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched "
+                          "ensemble or sharded path; per-system reference timings are in the "
+                          "line of our arm"}))
+        return 0
     n = wl["n"]
-    alloc = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
-    s = nb.ParticleSystem.zeros(n, allocator=alloc)
-    s.x[:], s.y[:], s.z[:] = pos.T
-    s.vx[:], s.vy[:], s.vz[:] = vel.T
-    s.m[:] = mass
-    g = nb.gravity_init(1.0, wl["eps"])
-    c2 = nb.CudaContext(theta=wl.get("theta", 0.7), multipole_order=wl.get("order", 1))
-    # the plugin function itself through its C ABI (the ctypes stub a host binds):
-    # one view over the pinned arrays, accelerations written in place
-    import ctypes as C
-
-    plugin = getattr(nb.library(), "n_body_sim_pro_barnes_hut_compute_acceleration_cuda"
-                     if algo == nb.Algorithm.BARNES_HUT
-                     else "n_body_sim_pro_gravity_compute_acceleration_cuda")
-    view, err = s.view(), nb.Error()
-
-    def force(*_):
-        if plugin(C.byref(view), C.byref(g), c2.handle, C.byref(err)) != nb.Status.OK:
-            raise nb.CudaError(err.status, err.message.decode(errors="replace"))
-
-    h, dt = 0.5 * wl["dt"], wl["dt"]
-    for _ in range(3):  # warm-up of the plugin path
-        force()
-    # integrator.c:47-85 on the host (in place, on the host's cores), force on the device
-    tv = [torch.from_numpy(getattr(s, f)) for f in ("vx", "vy", "vz")]
-    tx = [torch.from_numpy(getattr(s, f)) for f in ("x", "y", "z")]
-    ta = [torch.from_numpy(getattr(s, f)) for f in ("ax", "ay", "az")]
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        for v, a in zip(tv, ta):
-            v.add_(a, alpha=h)
-        for x, v in zip(tx, tv):
-            x.add_(v, alpha=dt)
-        force()
-        for v, a in zip(tv, ta):
-            v.add_(a, alpha=h)
-    elapsed = time.perf_counter() - t0
-    c2.close()
-    return {"value": n * steps / elapsed, "unit": "particle-steps/s",
-            "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n,
-            "steps": steps, "path": "host leapfrog (in-place, host threads) + the plugin "
-                                    "force function through its C ABI on pinned host arrays",
-            "timer": "host wall clock"}
+    p = reference_initial_state(wl, 42)
+    targets = seeded_targets(n)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    ref = O.gravity_subset(p.copy(), 1.0, wl["eps"], targets.astype(np.int64))
+    steps = max(1, min(args.steps, wl.get("reference_steps", 3)))
+    acc0, first, per_step = reference_run(wl, p, steps, threads, theta=wl.get("reference_theta"))
+    rms, mx = rms_and_max(acc0[targets], ref)
+    v = n / per_step
+    what = (f"Barnes-Hut (barnes_hut.c) at theta {wl.get('reference_theta')}"
+            if wl["algorithm"] == "barnes_hut" else "OpenMP AVX-512 all-pairs")
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": unit,
+            "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config,
+            "accuracy": {"rms_rel_force_err": rms, "max_rel_force_err": mx,
+                         "oracle": "FP64 direct sum (oracle restatement of gravity.c:37-67) on "
+                                   f"{len(targets)} seeded targets, initial state"},
+            "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "reference",
+                             "sample": f"warm-up: the initial force evaluation ({first:.2f} s); "
+                                       f"timed: {steps} leapfrog step(s) of the full {n}-particle "
+                                       + (f"system (reduced from {args.steps}: one reference "
+                                          f"step takes {per_step:.1f} s)" if steps < args.steps
+                                          else "system")
+                                       + f", reference engine, {what}, "
+                                       f"OMP_NUM_THREADS={threads}, {cpu_model()}"},
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
 
 
 def main(argv=None):
@@ -889,11 +1214,13 @@ def main(argv=None):
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="bh_collision_1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-matched", action="store_true",
                     help="skip the matched-accuracy study of the Barnes-Hut workloads")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the sub-records of the other configurations")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--order", type=int, default=None, choices=[1, 2])
     ap.add_argument("--walk", default=None, choices=["lists", "stackless"])
@@ -906,68 +1233,49 @@ def main(argv=None):
     if args.steps is None:
         args.steps = wl["steps"]
     args.warmup = max(args.warmup, 3)
-    # the headline metric: the throughput of the workload's configuration, with the
-    # chosen-vs-plain figures at rms <= 1e-3 (matched_accuracy) and the dominant
-    # kernel's fraction of FP32 peak (roofline) on the same line
     metric = "particle-steps/s at 1e-3 rms force error, chosen vs plain on B200; % FP32 peak"
     unit = "particle-steps/s"
     config = {"workload": args.workload, "particles": wl["n"], "algorithm": wl["algorithm"],
-              "theta": wl.get("theta"), "softening": wl["eps"], "timestep": wl["dt"],
-              "integrator": "leapfrog_kdk", "multipole_order": wl.get("order"),
-              "walk": wl.get("walk", "lists") if wl["algorithm"] == "barnes_hut" else None,
-              "leaf_capacity": wl.get("leaf", 16) if wl["algorithm"] == "barnes_hut" else None,
+              "softening": wl["eps"], "timestep": wl["dt"], "integrator": "leapfrog_kdk",
               "initial_conditions": wl["ic"], "l2": "256 MiB write between timed steps",
               "parallelism": f"replicas x{args.gpus}"}
-
+    if wl["algorithm"] == "barnes_hut":
+        config.update({"theta": wl.get("theta"), "multipole_order": wl.get("order"),
+                       "walk": wl.get("walk", "lists"), "leaf_capacity": wl.get("leaf", 16)})
+        if wl.get("matched"):
+            config["method"] = ("the fastest Barnes-Hut method at rms <= 1e-3 on the initial "
+                                "state (matched_accuracy.chosen)")
     if args.impl == "reference":
-        world = int(os.environ.get("WORLD_SIZE", "1"))
-        rank = int(os.environ.get("RANK", "0"))
-        if rank != 0:
-            return 0
-        threads = os.cpu_count() or 1
-        pos, vel, mass = initial_conditions(wl["ic"], wl["n"], seed=42)
-        steps = max(1, min(args.steps, 3))
-        for _ in range(1):  # one untimed warm-up step
-            reference_steps(wl, pos, vel, mass, 1, threads)
-        sec = reference_steps(wl, pos, vel, mass, steps, threads)
-        v = wl["n"] / sec
-        line = {"impl": "reference", "metric": metric, "value": v, "unit": unit,
-                "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": sec * 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "reference",
-                                 "sample": f"{steps} leapfrog steps of the full {wl['n']}-particle "
-                                           f"system (reference engine, OMP_NUM_THREADS={threads}, "
-                                           f"{cpu_model()})"},
-                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return 0
+        if wl["algorithm"] == "barnes_hut":
+            config["theta"] = wl.get("reference_theta", wl.get("theta"))
+        return reference_arm(args, wl, metric, unit, config)
 
     world, rank, local = dist_setup(args.gpus)
     sharded = wl["algorithm"] == "all_pairs_sharded" or wl.get("sharded", False)
     if sharded:
         config["parallelism"] = f"sharded x{world}"
+    r = run_workload(args, args.workload, wl, world, rank, local, args.steps, args.warmup)
     if wl["algorithm"] == "ensemble":
-        r = run_ensemble(args, wl, world, rank, local)
         config["particles"] = (sum(ensemble_sizes(wl)) if wl.get("sharded")
                                else r["stats"]["particles"])
-    elif wl["algorithm"] == "all_pairs_sharded":
-        r = run_sharded_allpairs(args, wl, world, rank, local)
-    else:
-        r = run_ours(args, wl, world, rank, local)
+    if wl["algorithm"] == "barnes_hut":
+        m = r["method"]
+        config.update({"theta": m["theta"], "multipole_order": m["multipole_order"],
+                       "leaf_capacity": m["leaf_capacity"], "opening": m["opening"],
+                       "relative_alpha": m["relative_alpha"], "corrected": m["corrected"],
+                       "method_name": m["name"]})
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and wl["algorithm"] != "ensemble":
-        try:
-            pos, vel, mass = initial_conditions(wl["ic"], wl["n"], seed=42)
-            threads = os.cpu_count() or 1
-            sec = reference_steps(wl, pos, vel, mass, 1, threads)
-            cpu = {"value": wl["n"] / sec, "unit": unit, "cores": threads, "kind": "reference",
-                   "sample": f"1 leapfrog step of the full {wl['n']}-particle system, reference "
-                             f"engine (oracle/_ref) with OMP_NUM_THREADS={threads} on {cpu_model()}"}
-        except Exception as exc:  # reported, not fatal
-            cpu = {"value": None, "unit": unit, "cores": 0, "kind": "reference",
-                   "sample": f"unavailable: {exc}"}
+    if (rank == 0 and world == 1 and not args.no_cpu_baseline
+            and wl["algorithm"] in ("barnes_hut", "all_pairs")):
+        cpu = cpu_baseline_leg(wl, r, os.cpu_count() or 1)
+    secondary = None
+    if (args.workload == DEFAULT_WORKLOAD and world == 1 and not args.no_secondary):
+        secondary = {}
+        for name in SECONDARY:
+            try:
+                secondary[name] = secondary_record(args, name, world, rank, local)
+            except Exception as exc:  # reported, not fatal
+                secondary[name] = {"unavailable": repr(exc)}
     if rank == 0:
         line = {"metric": metric, "value": r["value"], "unit": unit, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -976,28 +1284,41 @@ def main(argv=None):
                 "dtype": "f32-force/f64-state",
                 "data": "synthetic", "config": config,
                 "accuracy": {"rms_rel_force_err": r["rms"], "max_rel_force_err": r["max_rel"],
-                             "energy_drift": r["drift"], "oracle": "FP64 device direct sum, "
-                             "4096 seeded targets, final state"},
+                             "energy_drift": r["drift"], "drift_over": r.get("drift_note"),
+                             "oracle": "FP64 device direct sum, 4096 seeded targets, final state"},
                 "interactions_per_s": r["interactions_per_s"], "stats": r["stats"],
                 "phase_ms": r["timings"], "roofline": r["roofline"], "cpu_baseline": cpu,
                 "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"]}
-        if r.get("matched") is not None:
-            line["matched_accuracy"] = r["matched"]
-            m = r["matched"]
-            if m.get("plain") and m.get("chosen"):
-                line["headline"] = {
-                    "value_is": "the configuration's throughput (plain walk at its theta)",
-                    "chosen_at_rms_1e-3": m["chosen"]["value"],
-                    "chosen_method": {k: m["chosen"].get(k) for k in
-                                      ("theta", "multipole_order", "opening", "relative_alpha",
-                                       "leaf_capacity")},
-                    "plain_at_rms_1e-3": m["plain"]["value"],
-                    "chosen_over_plain": m.get("chosen_over_plain"),
-                    "fp32_peak_frac": r["roofline"].get("frac")}
+        study = r.get("matched")
+        if study is not None:
+            line["matched_accuracy"] = study
+            keys = ("name", "theta", "multipole_order", "opening", "relative_alpha",
+                    "leaf_capacity", "corrected", "rms", "max_rel", "value", "ms_per_step",
+                    "energy_drift", "energy_drift_over")
+            pick = lambda m: {k: m.get(k) for k in keys} if m else None  # noqa: E731
+            line["headline"] = {
+                "value_is": "the chosen method (fastest at rms <= 1e-3), timed over the K steps",
+                "chosen": pick(study.get("chosen")),
+                "plain_theta_0.5": pick(study.get("plain_theta_0.5")),
+                "plain_matched": pick(study.get("plain")),
+                "relative": pick(study.get("relative")),
+                "corrected_theta_1.0": {k: pick(v) for k, v in
+                                        study.get("corrected_theta_1.0", {}).items()},
+                "chosen_over_plain_theta_0.5": (round(r["value"] /
+                                                      study["plain_theta_0.5"]["value"], 3)
+                                                if study.get("plain_theta_0.5") else None),
+                "chosen_over_plain_matched": (round(r["value"] / study["plain"]["value"], 3)
+                                              if study.get("plain") else None),
+                "walk_fp32_peak_frac": r["roofline"].get("frac"),
+                "reference_cpu": ({k: cpu.get(k) for k in ("value", "rms_rel_force_err",
+                                                           "max_rel_force_err", "cores")}
+                                  if cpu else None)}
         if r.get("stages") is not None:
             line["stages_hbm"] = r["stages"]
         if r.get("interactions_split") is not None:
             line["interactions_split"] = r["interactions_split"]
+        if secondary is not None:
+            line["secondary"] = secondary
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -348,6 +348,23 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_preset_generate_pa
     const NBodySimProPresetParameters* parameters, NBodySimProError* error);
 
 /*
+ * Joins the parallel presets (src/c/generation/presets_parallel.c): two Plummer
+ * spheres of total mass 1/2 each and scale radius `scale_radius`, built the way
+ * the reference's galaxy_collision builds its two disk blocks (:392-404) but
+ * with its Plummer block (fill_plummer_block, :91-155): block b in
+ * [b * (count/2), ...) draws from the per-particle generators
+ * mix_seed(mix_seed(seed, b), index), is centred at -/+ separation/2 on x and
+ * has its mean velocity removed; then -/+ relative_speed/2 is added on y.
+ * Block 1 takes count - count/2 particles.  The two-Plummer collision
+ * workload (two 500k or 5M spheres 10 apart, relative speed 0.3) is this with
+ * (1, 10, 0.3).  Accelerations start at zero.  count < 2, a non-positive
+ * radius or non-finite arguments -> INVALID_ARGUMENT.
+ */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_plummer_collision_generate(
+    NBodySimProCudaContext* context, size_t count, uint64_t seed, double scale_radius,
+    double separation, double relative_speed, NBodySimProError* error);
+
+/*
  * Replaces n_body_sim_pro_checkpoint_write (checkpoint/checkpoint.h:43-46,
  * src/c/checkpoint/checkpoint.c:9-76) for device-resident state: the file is
  * the reference's format — magic, version, the header struct as stored in

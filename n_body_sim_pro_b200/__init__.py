@@ -178,6 +178,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
     "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
+    "n_body_sim_pro_cuda_plummer_collision_generate",
 )
 
 # NBodySimProSimulationPreset (generation/presets.h:27-38)
@@ -229,6 +230,9 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_corrected_cells": (C.c_size_t, [vp]),
         "n_body_sim_pro_cuda_preset_generate_parallel": (C.c_int, [vp, C.c_int,
                                                                    C.POINTER(C.c_size_t * 2), pe]),
+        "n_body_sim_pro_cuda_plummer_collision_generate": (st, [vp, C.c_size_t, C.c_uint64,
+                                                                C.c_double, C.c_double,
+                                                                C.c_double, pe]),
         "n_body_sim_pro_cuda_checkpoint_write": (C.c_int, [vp, C.c_char_p,
                                                            C.POINTER(CheckpointHeader), pe]),
         "n_body_sim_pro_cuda_checkpoint_read": (C.c_int, [vp, C.c_char_p,
@@ -482,6 +486,16 @@ class CudaContext:
         _check(library().n_body_sim_pro_cuda_preset_generate_parallel(self.handle, pid,
                                                                        C.byref(params),
                                                                        C.byref(err)), err)
+        self.n = n
+
+    def generate_plummer_collision(self, n: int, seed: int, scale_radius: float = 1.0,
+                                   separation: float = 10.0, relative_speed: float = 0.3) -> None:
+        """Two Plummer spheres (mass 1/2 each) from the parallel presets'
+        per-particle streams, -/+ separation/2 on x, -/+ relative_speed/2 on y:
+        the two-Plummer collision workload becomes the resident state."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_plummer_collision_generate(
+            self.handle, n, seed, scale_radius, separation, relative_speed, C.byref(err)), err)
         self.n = n
 
     def checkpoint_write(self, path: str, header: CheckpointHeader) -> None:

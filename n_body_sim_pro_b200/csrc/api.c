@@ -712,6 +712,35 @@ NBodySimProStatus n_body_sim_pro_cuda_preset_generate_parallel(
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
+NBodySimProStatus n_body_sim_pro_cuda_plummer_collision_generate(
+    NBodySimProCudaContext* c, size_t count, uint64_t seed, double scale_radius,
+    double separation, double relative_speed, NBodySimProError* error) {
+    if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
+    if (count < 2) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "too few particles for the preset");
+    if (!(scale_radius > 0.0) || !isfinite(scale_radius) || !isfinite(separation) ||
+        !isfinite(relative_speed))
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
+                    "scale radius must be positive, separation and speed finite");
+    CUDA_TRY(cudaSetDevice(c->device));
+    NBodySimProStatus st = ensure_capacity(c, count, error);
+    if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
+    if ((st = ensure_scratch(c, nbsp_preset_scratch_doubles(count), error)) != N_BODY_SIM_PRO_STATUS_OK)
+        return st;
+    c->n = count;
+    c->n_padded = round_up(count, 256);
+    double* acc[] = {c->ax, c->ay, c->az};
+    for (size_t k = 0; k < 3; ++k)
+        CUDA_TRY(cudaMemsetAsync(acc[k], 0, count * sizeof(double), c->stream));
+    if (nbsp_plummer_collision_generate(count, seed, scale_radius, separation, relative_speed,
+                                        c->x, c->y, c->z, c->vx, c->vy, c->vz, c->m, c->scratch,
+                                        c->stream) != 0)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "too few particles for the preset");
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->resident = 1;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
 NBodySimProStatus n_body_sim_pro_cuda_download(NBodySimProCudaContext* c,
                                                const NBodySimProParticleSystemView* view,
                                                NBodySimProError* error) {

@@ -154,6 +154,13 @@ NBSP_HIDDEN size_t nbsp_preset_scratch_doubles(size_t n);
 NBSP_HIDDEN int nbsp_preset_generate(int preset, size_t n, uint64_t seed, double* x, double* y,
                                      double* z, double* vx, double* vy, double* vz, double* m,
                                      double* scratch, cudaStream_t stream);
+/* Two Plummer spheres from the parallel presets' per-particle streams
+ * (presets.cu); 0 on success, 1 for n < 2. */
+NBSP_HIDDEN int nbsp_plummer_collision_generate(size_t n, uint64_t seed, double a,
+                                                double separation, double relative_speed,
+                                                double* x, double* y, double* z, double* vx,
+                                                double* vy, double* vz, double* m,
+                                                double* scratch, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -82,14 +82,17 @@ NBodySimProStatus report_cuda(NBodySimProError* error, cudaError_t code, int lin
   return report(error, status, line, text);
 }
 
-// True when `p` may be dereferenced by a kernel on the current device.
-bool device_accessible(const void* p) {
+// True when `p` may be dereferenced by a kernel on `device` (the current one):
+// managed memory, or device memory that lives on that same device (a buffer of
+// another GPU would be a peer access, or a fault without peer access).
+bool device_accessible(const void* p, int device) {
   cudaPointerAttributes attr;
   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+  if (attr.type == cudaMemoryTypeManaged) return true;
+  return attr.type == cudaMemoryTypeDevice && attr.device == device;
 }
 
 }  // namespace
@@ -121,9 +124,9 @@ n_body_sim_pro_cuda_allpairs_acceleration_noalloc(
                   "device ordinal beyond the scratch address table");
   }
   for (const void* a : arrays) {
-    if (a == nullptr || !device_accessible(a)) {
+    if (a == nullptr || !device_accessible(a, device)) {
       return report(error, N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, __LINE__,
-                    "all seven arrays must be non-null device pointers");
+                    "all seven arrays must be non-null pointers to the current device's memory");
     }
   }
 

@@ -291,6 +291,14 @@ __global__ void subtract_mean_kernel(State s, size_t start, size_t count,
   }
 }
 
+// Relative velocity of the two-Plummer collision: -speed/2 on y for the first
+// block, +speed/2 for the second (added after each block's mean removal).
+__global__ void shear_kernel(State s, size_t half, size_t count, double half_speed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+       i += (size_t)gridDim.x * blockDim.x)
+    s.vy[i] += i < half ? -half_speed : half_speed;
+}
+
 // presets_parallel.c:393-395: +0.35 on x for the first half, -0.35 for the rest
 __global__ void approach_kernel(State s, size_t half, size_t count) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
@@ -393,6 +401,35 @@ int nbsp_preset_generate(int preset, size_t n, uint64_t seed, double* x, double*
     default:
       return 1;
   }
+}
+
+// Two Plummer spheres (scale radius a, mass 1/2 each) in the reference's
+// parallel-preset form, the way its galaxy_collision (presets_parallel.c:392-404)
+// builds two disk blocks: block b fills [b * half, b * half + count_b) from the
+// per-particle generators mix_seed(mix_seed(seed, b), index) (fill_plummer_block,
+// :91-155), centred at -/+ separation / 2 on x, its mean velocity removed;
+// then -/+ relative_speed / 2 on y.  Block 1 takes n - n/2 particles.
+int nbsp_plummer_collision_generate(size_t n, uint64_t seed, double a, double separation,
+                                    double relative_speed, double* x, double* y, double* z,
+                                    double* vx, double* vy, double* vz, double* m,
+                                    double* scratch, cudaStream_t stream) {
+  const State s{x, y, z, vx, vy, vz, m};
+  double* mean = scratch;
+  double* partial = scratch + 8;
+  const size_t half = n / 2;
+  if (half == 0) return 1;
+  for (int b = 0; b < 2; ++b) {
+    const size_t start = (size_t)b * half;
+    const size_t count = b == 0 ? half : n - half;
+    const double cx = (b == 0 ? -0.5 : 0.5) * separation;
+    NBSP_COUNT_LAUNCH(1), plummer_kernel<<<blocks_for(count), kPresetThreads, 0, stream>>>(
+        s, mix_seed(seed, (uint64_t)b), start, count, a, a * a, 0.5, 0.5 / (double)count, 1, cx,
+        0.0, 0.0, partial);
+    remove_mean(s, start, count, partial, mean, stream);
+  }
+  NBSP_COUNT_LAUNCH(1), shear_kernel<<<grid_stride_blocks(n), 256, 0, stream>>>(
+      s, half, n, 0.5 * relative_speed);
+  return 0;
 }
 
 }  // extern "C"

@@ -287,6 +287,28 @@ static void par_plummer_block(OracleView* v, uint64_t master, size_t start, size
     par_subtract_mean(v, start, count, sx, sy, sz);
 }
 
+/* Two Plummer spheres in the parallel-preset form: the reference's
+ * galaxy_collision layout (presets_parallel.c:392-404: block b seeded with
+ * mix_seed(seed, b), filling [b*half, ...)) with its Plummer block
+ * (fill_plummer_block, :91-155, mass 1/2, centred at -/+ separation/2 on x);
+ * block 1 takes n - n/2 particles; then -/+ relative_speed/2 on y. */
+int oracle_preset_plummer_collision_parallel(OracleView* v, uint64_t seed, double scale_radius,
+                                             double separation, double relative_speed) {
+    const size_t n = v->particle_count;
+    if (n < 2) return 1;
+    const size_t half = n / 2;
+    for (int b = 0; b < 2; ++b) {
+        const size_t start = (size_t)b * half;
+        const size_t count = b == 0 ? half : n - half;
+        const double centre[3] = {(b == 0 ? -0.5 : 0.5) * separation, 0.0, 0.0};
+        par_plummer_block(v, oracle_mix_seed(seed, (uint64_t)b), start, count, scale_radius,
+                          scale_radius * scale_radius, 0.5, 0.5 / (double)count, centre);
+    }
+    for (size_t i = 0; i < n; ++i)
+        v->velocities_y[i] += i < half ? -0.5 * relative_speed : 0.5 * relative_speed;
+    return 0;
+}
+
 /* presets_parallel.c:158-217 (exponential disk block, optional arms). */
 static void par_disk_block(OracleView* v, uint64_t master, size_t start, size_t count, double a,
                            double h, double vc, double sigma, double twist, int arms,

@@ -66,6 +66,12 @@ int oracle_preset_uniform_log_mass(OracleView* view, uint64_t seed);
  * include/n_body_sim_pro/generation/presets.h:73): preset ids as the reference's
  * NBodySimProSimulationPreset enum (presets.h:27-38). 0 on success. */
 int oracle_preset_parallel(OracleView* view, int preset, uint64_t seed);
+/* Two Plummer spheres (mass 1/2 each) from the parallel presets' per-particle
+ * streams, block b seeded with mix_seed(seed, b); -/+ separation/2 on x,
+ * -/+ relative_speed/2 on y.  0 on success. */
+int oracle_preset_plummer_collision_parallel(OracleView* view, uint64_t seed,
+                                             double scale_radius, double separation,
+                                             double relative_speed);
 /* Size of ensemble member k: round(exp(U(ln lo, ln hi))) from rng(mix_seed(master, k)). */
 size_t oracle_ensemble_member_size(uint64_t master_seed, uint64_t k, size_t lo, size_t hi);
 /* Plummer sphere (a = 1, M = 1) for ensemble member k, same stream as the size draw. */

@@ -105,16 +105,20 @@ class Particles:
         return np.stack([self.x, self.y, self.z], axis=1)
 
 
-def build(ref: bool = True) -> None:
-    """Compile the restatement (and the reference, when its sources exist)."""
+def build(ref: bool = True, reference_dir: str | None = None) -> None:
+    """Compile the restatement and, when a reference checkout is given
+    (`reference_dir`, else the environment variable NBSP_REFERENCE_DIR) and
+    holds its C sources, the reference engine into _ref/."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir("/root/reference/src/c"):
-        subprocess.run(["make", "-s", "-C", HERE, "-j8", "ref"], check=True)
+    reference_dir = reference_dir or os.environ.get("NBSP_REFERENCE_DIR")
+    if ref and reference_dir and os.path.isdir(os.path.join(reference_dir, "src", "c")):
+        refdef = "REF=" + os.path.abspath(reference_dir)
+        subprocess.run(["make", "-s", "-C", HERE, "-j8", refdef, "ref"], check=True)
         # the reference's force benchmark with the two CUDA algorithms (needs
         # the B200 library, built first by the package's own build step)
         if os.path.exists(os.path.join(HERE, "..", "n_body_sim_pro_b200", "lib",
                                        "libn_body_sim_pro_cuda.so")):
-            subprocess.run(["make", "-s", "-C", HERE, "integrated"], check=True)
+            subprocess.run(["make", "-s", "-C", HERE, refdef, "integrated"], check=True)
 
 
 _lib = None
@@ -135,6 +139,7 @@ def lib() -> C.CDLL:
             "oracle_preset_globular_cluster": (C.c_int, [pv, u64]),
             "oracle_preset_spiral_galaxy": (C.c_int, [pv, u64]),
             "oracle_preset_plummer_collision": (C.c_int, [pv, u64, d, d, d]),
+            "oracle_preset_plummer_collision_parallel": (C.c_int, [pv, u64, d, d, d]),
             "oracle_preset_uniform_log_mass": (C.c_int, [pv, u64]),
             "oracle_ensemble_member_size": (sz, [u64, u64, sz, sz]),
             "oracle_ensemble_member_generate": (C.c_int, [pv, u64, u64, sz, sz]),
@@ -252,6 +257,18 @@ def preset_parallel(name: str, n: int, seed: int) -> Particles:
     v = p.view()
     if lib().oracle_preset_parallel(C.byref(v), PRESET_IDS[name], seed) != 0:
         raise RuntimeError(f"oracle parallel preset {name} failed")
+    return p
+
+
+def plummer_collision_parallel(n: int, seed: int, scale_radius: float = 1.0,
+                               separation: float = 10.0, relative_speed: float = 0.3) -> Particles:
+    """Two Plummer spheres in the parallel-preset form (per-particle streams,
+    block b seeded with mix_seed(seed, b)): the two-Plummer collision workload."""
+    p = Particles.zeros(n)
+    v = p.view()
+    if lib().oracle_preset_plummer_collision_parallel(C.byref(v), seed, scale_radius, separation,
+                                                      relative_speed) != 0:
+        raise RuntimeError("oracle plummer collision failed")
     return p
 
 

@@ -148,6 +148,38 @@ def test_precision_study_small(cuda, ctx):
     assert rms < 1e-5 and mx < 5e-4
 
 
+def test_precision_study_262k_100_steps(cuda, ctx):
+    """Config 3 as specified: N = 262,144 uniform in the unit cube, masses
+    log-uniform in [1e-3, 1] normalised to 1, eps = 1e-3.  Forces on 4096
+    seeded targets against the oracle's FP64 subset sum (gravity.c:37-67), then
+    100 leapfrog steps at dt = 1e-4 on the device: the energy drift of the FP64
+    device diagnostics, whose final energy is checked against the oracle's
+    numerics.c:5-116 on the downloaded state."""
+    n = 262144
+    p = O.preset("uniform_log_mass", n, 11)
+    targets = np.random.default_rng(1).choice(n, 4096, replace=False)
+    ref = O.gravity_subset(p, 1.0, 1e-3, targets)
+    g = cuda.gravity_init(1.0, 1e-3)
+    ctx.upload(cuda.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS]))
+    ctx.compute_acceleration(g, cuda.Algorithm.ALL_PAIRS)
+    a = ctx.download_accelerations()[targets]
+    rms, mx = O.rms_relative_error(a, ref), vec_max_rel(a, ref)
+    q0, pe0 = ctx.diagnostics(g, potential=True)
+    ctx.advance(g, 1e-4, 100, cuda.Algorithm.ALL_PAIRS)
+    q1, pe1 = ctx.diagnostics(g, potential=True)
+    drift = abs((q1[0] + pe1) - (q0[0] + pe0)) / abs(q0[0] + pe0)
+    s = cuda.ParticleSystem.zeros(n)
+    ctx.download(s)
+    final = O.Particles.zeros(n)
+    for f in O.FIELDS:
+        getattr(final, f)[:] = getattr(s, f)
+    e_oracle = O.diagnostics(final)[0] + O.potential_energy(final, 1.0, 1e-3, openmp=True)
+    print(f"262k: rms={rms:.3e} max={mx:.3e} drift(100 steps)={drift:.3e}")
+    assert rms < 1e-5 and mx < 5e-4
+    assert drift < 1e-6
+    assert abs((q1[0] + pe1) - e_oracle) <= 1e-12 * abs(e_oracle)
+
+
 def test_particle_limit_is_checked_before_allocation(cuda, ctx):
     """More than N_BODY_SIM_PRO_CUDA_MAX_PARTICLES (2^30 - 2^16: 30-bit sort
     counts, 32-bit indices) is INVALID_ARGUMENT, not a failed allocation."""

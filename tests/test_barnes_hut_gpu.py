@@ -164,6 +164,39 @@ def test_collision_config_accuracy(cuda, ctx, walk):
     assert e1 < 1e-2 and e2 < e1
 
 
+def test_collision_1m_config_accuracy(cuda, ctx):
+    """Config 2 at its full size: the 1M two-Plummer collision from the
+    reference's parallel-preset streams, eps 0.01, theta 0.7, against the FP64
+    oracle on 4096 seeded targets; and the relative opening test at its
+    matched setting (alpha 0.004, 32-particle buckets, theta-1.0 safety bound)
+    within the 1e-3 rms of the headline metric."""
+    n = 1_000_000
+    ctx.generate_plummer_collision(n, 42)
+    s = cuda.ParticleSystem.zeros(n)
+    ctx.download(s)
+    p = O.Particles.zeros(n)
+    for f in O.FIELDS:
+        getattr(p, f)[:] = getattr(s, f)
+    targets = np.random.default_rng(11).choice(n, 4096, replace=False)
+    ref = O.gravity_subset(p, 1.0, 0.01, targets)
+    g = cuda.gravity_init(1.0, 0.01)
+    ctx.theta = 0.7
+    ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+    a = ctx.download_accelerations()[targets]
+    e_plain = O.rms_relative_error(a, ref)
+    m_plain = float(np.max(np.linalg.norm(a - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+    ctx.theta = 1.0
+    ctx.set_leaf_capacity(32)
+    ctx.set_relative_opening(0.004)
+    ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old: the theta-0.7 forces
+    ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+    a_rel = ctx.download_accelerations()[targets]
+    e_rel = O.rms_relative_error(a_rel, ref)
+    print(f"collision1M theta0.7 rms={e_plain:.3e} max={m_plain:.3e} relative rms={e_rel:.3e}")
+    assert e_plain < 2.5e-3 and m_plain < 0.1
+    assert e_rel <= 1e-3
+
+
 @pytest.mark.parametrize("theta", [0.5, 1.0])
 def test_offset_opening_is_more_accurate(cuda, ctx, theta, walk):
     """The offset test (2h / theta + |com - cell centre| < d) accepts a subset of

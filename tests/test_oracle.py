@@ -56,6 +56,39 @@ def test_parallel_presets_bit_identical_to_reference(name, n, seed):
 
 
 @needs_ref
+@pytest.mark.parametrize("n,seed", [(1000, 42), (777, 5)])
+def test_plummer_collision_blocks_are_the_reference_plummer_block(n, seed):
+    """The two-Plummer collision (parallel-preset form) is pinned to the
+    reference's own fill_plummer_block through its exported presets: with no
+    separation and no shear, block 0 holds the positions of the reference's
+    parallel globular cluster of n/2 particles seeded mix_seed(seed, 0), block 1
+    particles [n/2, n) of the one of n particles seeded mix_seed(seed, 1), bit
+    for bit; block 0's velocities are that preset's scaled by sqrt(1/2) (the
+    dispersion of a sphere of mass 1/2) and its masses are half its masses."""
+    _reference_openmp_single_thread()
+    half = n // 2
+    c = O.plummer_collision_parallel(n, seed, separation=0.0, relative_speed=0.0)
+    b0 = O.ref_preset("globular_cluster", half, O.lib().oracle_mix_seed(seed, 0), parallel=True)
+    b1 = O.ref_preset("globular_cluster", n, O.lib().oracle_mix_seed(seed, 1), parallel=True)
+    for f in ("x", "y", "z"):
+        assert np.array_equal(getattr(c, f)[:half], getattr(b0, f)), f
+        assert np.array_equal(getattr(c, f)[half:], getattr(b1, f)[half:]), f
+    assert np.array_equal(c.m[:half], 0.5 * b0.m)
+    assert np.allclose(c.m[half:], 0.5 / (n - half), rtol=0, atol=0)
+    for f in ("vx", "vy", "vz"):
+        v, ref = getattr(c, f)[:half], np.sqrt(0.5) * getattr(b0, f)
+        assert np.max(np.abs(v - ref)) <= 1e-14 * np.max(np.abs(ref)), f
+    # the workload's geometry: centres -/+ 5 on x, zero net momentum per block,
+    # then -/+ 0.15 on y
+    w = O.plummer_collision_parallel(n, seed)
+    assert np.array_equal(w.x[:half], c.x[:half] + -5.0)
+    assert np.array_equal(w.x[half:], c.x[half:] + 5.0)
+    assert np.array_equal(w.vy[:half], c.vy[:half] + -0.15)
+    for blk in (slice(0, half), slice(half, n)):
+        assert abs(np.sum(c.m[blk] * c.vx[blk])) < 1e-15
+
+
+@needs_ref
 @pytest.mark.parametrize("eps", [0.02, 0.0])
 def test_gravity_bit_identical_to_reference(eps):
     p = O.preset("random_cloud", 512, 42)

@@ -87,3 +87,27 @@ def test_device_preset_then_step(cuda, ctx):
     O.gravity_reference(ref, 1.0, 0.01, openmp=True)
     O.advance(ref, 1.0, 0.01, 1e-3, 2, integrator=1, force=1)
     assert np.max(np.abs(got.x - ref.x)) < 1e-9
+
+
+@pytest.mark.parametrize("n,seed", [(20001, 42), (4096, 7)])
+def test_device_plummer_collision_matches_oracle(cuda, ctx, n, seed):
+    """The two-Plummer collision of the Barnes-Hut workloads (two spheres of
+    mass 1/2 from the parallel presets' streams, -/+5 on x, -/+0.15 on y)
+    against its oracle restatement, which tests/test_oracle.py pins to the
+    reference's own Plummer block; same bars as the presets above."""
+    ctx.generate_plummer_collision(n, seed)
+    got = download(cuda, ctx, n)
+    ref = O.plummer_collision_parallel(n, seed)
+    assert np.array_equal(got.m, ref.m)
+    num = den = worst = 0.0
+    for f in ("x", "y", "z", "vx", "vy", "vz"):
+        a, b = getattr(got, f), getattr(ref, f)
+        worst = max(worst, float((np.abs(a - b) / np.maximum(np.abs(b), 1.0)).max()))
+        num += float(np.sum((a - b) ** 2))
+        den += float(np.sum(b ** 2))
+    assert worst <= 1e-9
+    assert np.sqrt(num / den) <= 1e-13
+    half = n // 2
+    assert abs(np.mean(got.x[:half]) + 5.0) < 0.1 and abs(np.mean(got.x[half:]) - 5.0) < 0.1
+    assert abs(np.sum(got.m[:half] * got.vy[:half]) / np.sum(got.m[:half]) + 0.15) < 1e-12
+    assert np.all(got.ax == 0.0)

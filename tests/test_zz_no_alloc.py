@@ -5,11 +5,13 @@ It exists for callers that cannot allocate device memory (during CUDA graph
 capture, inside frameworks that own every allocation, in loops that must not
 touch the allocator); it keeps its working memory in a static device array
 limited to 16384 particles.  Its output must agree with the allocating entry
-point n_body_sim_pro_gravity_compute_acceleration_cuda within the all-pairs
-tolerances of tests/test_allpairs_gpu.py, on two calls in a row (the second
-smaller, so stale contents left in the shared array by the first call must
-not leak into it).  This test allocates its own device buffers with torch:
-it plays the caller, who owns inputs and outputs.
+point n_body_sim_pro_gravity_compute_acceleration_cuda and with the FP64
+oracle (the reference's scalar all-pairs sum, gravity.c:15-70) within the
+all-pairs tolerances of tests/test_allpairs_gpu.py, on calls in a row: the
+first at exactly the 16384-particle limit, which fills the whole scratch
+array, then smaller ones, so stale contents left in the shared array by an
+earlier call must not leak into a later one.  This test allocates its own
+device buffers with torch: it plays the caller, who owns inputs and outputs.
 
 The file name sorts last so a stop-at-first-failure run has run every other
 test before this one.
@@ -39,16 +41,20 @@ def _max_rel(a, ref):
     return float(np.max(np.linalg.norm(a - ref, axis=1) / np.linalg.norm(ref, axis=1)))
 
 
-def test_noalloc_matches_allocating_entry_point_on_two_calls(cuda):
+LIMIT = 16384  # particles: the static scratch array's capacity
+
+
+def test_noalloc_matches_allocating_entry_point_and_oracle_on_calls_in_a_row(cuda):
     import torch
 
     noalloc = _entry(cuda)
     g = cuda.gravity_init(1.0, 0.01)
     side_stream = torch.cuda.Stream()
-    for call, (n, seed) in enumerate(((9000, 1), (3000, 2))):
+    for call, (n, seed) in enumerate(((LIMIT, 1), (9000, 2), (3000, 3))):
         p = O.preset("globular_cluster", n, seed)
         s = cuda.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS])
         expected = cuda.n_body_sim_pro_gravity_compute_acceleration_cuda(s, g)
+        oracle = O.gravity_reference(p.copy(), 1.0, 0.01, openmp=True)
 
         inputs = [torch.tensor(getattr(p, f), dtype=torch.float64, device="cuda")
                   for f in ("x", "y", "z", "m")]
@@ -65,6 +71,8 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(cuda):
         assert np.all(np.isfinite(got))
         assert O.rms_relative_error(got, expected) < RMS_TOL
         assert _max_rel(got, expected) < MAX_TOL
+        assert O.rms_relative_error(got, oracle) < RMS_TOL
+        assert _max_rel(got, oracle) < MAX_TOL
 
 
 def test_noalloc_rejects_what_it_cannot_do(cuda):
