@@ -167,9 +167,9 @@ def test_collision_config_accuracy(cuda, ctx, walk):
 def test_collision_1m_config_accuracy(cuda, ctx):
     """Config 2 at its full size: the 1M two-Plummer collision from the
     reference's parallel-preset streams, eps 0.01, theta 0.7, against the FP64
-    oracle on 4096 seeded targets; and the relative opening test at its
-    matched setting (alpha 0.004, 32-particle buckets, theta-1.0 safety bound)
-    within the 1e-3 rms of the headline metric."""
+    oracle on 4096 seeded targets; and the relative opening test (alpha 0.0015,
+    32-particle buckets, theta-1.0 safety bound) within the 1e-3 rms of the
+    headline metric (measured on this state: alpha 0.004 gives 1.2e-3)."""
     n = 1_000_000
     ctx.generate_plummer_collision(n, 42)
     s = cuda.ParticleSystem.zeros(n)
@@ -187,7 +187,7 @@ def test_collision_1m_config_accuracy(cuda, ctx):
     m_plain = float(np.max(np.linalg.norm(a - ref, axis=1) / np.linalg.norm(ref, axis=1)))
     ctx.theta = 1.0
     ctx.set_leaf_capacity(32)
-    ctx.set_relative_opening(0.004)
+    ctx.set_relative_opening(0.0015)
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old: the theta-0.7 forces
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
     a_rel = ctx.download_accelerations()[targets]
