@@ -104,6 +104,9 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 
 # relative opening test over the reference test at theta 1.0: the alphas of its sweep
 ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
               0.007, 0.01)
+# the corrected walk under the relative test: the correction lowers the error
+# of the cells it accepts, so the sweep reaches further
+ALPHA_GRID_CORRECTED = ALPHA_GRID + (0.0125, 0.015, 0.02)
 OPENINGS = {"reference": 0, "offset": 1}
 N_TARGETS = 4096  # seeded targets of the FP64 direct-sum oracle
 # energy drift needs the O(N^2) FP64 potential: measured directly up to
@@ -570,6 +573,24 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
             corrected[oname] = rec
             if r[0] <= RMS_TARGET:
                 methods.append(rec)
+            if oname == "reference":  # the corrected walk with the relative test on top
+                cctx = make_context(nb, method("", 1.0, leaf=32, corrected=True), corr)
+                cctx.upload(system)
+                rows = []
+                for alpha in ALPHA_GRID_CORRECTED:
+                    cctx.set_relative_opening(alpha)
+                    rows.append((alpha, accuracy(nb, cctx, g, targets, ref)))
+                cctx.close()
+                out["sweep"]["corrected_relative_alpha_theta1.0_leaf32"] = [
+                    [a, round(r[0], 6)] for a, r in rows]
+                b = best(rows)
+                if b:
+                    m = method("corrected_relative_leaf32", 1.0, alpha=b[0], leaf=32,
+                               corrected=True)
+                    rec = timed(m, b[1], corr)
+                    rec["training"] = training
+                    methods.append(rec)
+                    out["corrected_relative"] = rec
         out["corrected_theta_1.0"] = corrected
     out["chosen"] = max(methods, key=lambda m: m["value"]) if methods else None
     if out["plain"] and out["chosen"]:
@@ -586,7 +607,8 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
         note = f"the method's settings on the {DRIFT_N}-particle collision, {DRIFT_STEPS} steps"
     else:
         wl1, small, note = wl, system, f"{wl['n']} particles, {DRIFT_STEPS} steps"
-    reported = [out.get("plain_theta_0.5"), out["plain"], out["relative"], out["chosen"]]
+    reported = [out.get("plain_theta_0.5"), out["plain"], out["relative"],
+                out.get("corrected_relative"), out["chosen"]]
     reported += list(out.get("corrected_theta_1.0", {}).values())
     for rec in reported:
         if rec is not None and "energy_drift" not in rec:
@@ -1304,6 +1326,7 @@ def main(argv=None):
                 "relative": pick(study.get("relative")),
                 "corrected_theta_1.0": {k: pick(v) for k, v in
                                         study.get("corrected_theta_1.0", {}).items()},
+                "corrected_relative": pick(study.get("corrected_relative")),
                 "chosen_over_plain_theta_0.5": (round(r["value"] /
                                                       study["plain_theta_0.5"]["value"], 3)
                                                 if study.get("plain_theta_0.5") else None),

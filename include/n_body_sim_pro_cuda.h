@@ -545,6 +545,23 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_samples
     NBodySimProCudaCorrection* correction, size_t* rows, float* features, float* labels,
     size_t max_rows, NBodySimProError* error);
 
+/* Engines of n_body_sim_pro_cuda_correction_evaluate. */
+typedef enum NBodySimProCudaMlpEngine {
+    N_BODY_SIM_PRO_CUDA_MLP_TCGEN05 = 0,  /* 5th-generation tensor cores, 128-row tiles, TMEM */
+    N_BODY_SIM_PRO_CUDA_MLP_MMA_SYNC = 1  /* warp-level mma.sync, 16-row tiles */
+} NBodySimProCudaMlpEngine;
+
+/* The trained network on `rows` raw feature rows (10 floats each, the
+ * features of the corrected walk: cell-to-target offset / side, side /
+ * distance, trace-free quadrupole / (M side^2), spread): standardised, through
+ * the BF16 layers, de-standardised into `outputs` (3 floats per row: the
+ * residual (a_exact - a_monopole) |d|^2 / M in units of G).  Host arrays.  No
+ * range masking: rows outside the training range are evaluated as given.
+ * No reference counterpart (the reference has no learned correction). */
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_correction_evaluate(
+    NBodySimProCudaCorrection* correction, const float* features, size_t rows, float* outputs,
+    int engine, NBodySimProError* error);
+
 /* Correct the Barnes-Hut walk of `context` with `correction` (NULL: plain). */
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_correction(
     NBodySimProCudaContext* context, const NBodySimProCudaCorrection* correction,

@@ -178,8 +178,11 @@ EXPORTS = (
     "n_body_sim_pro_cuda_preset_generate_parallel", "n_body_sim_pro_cuda_checkpoint_write",
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
     "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
-    "n_body_sim_pro_cuda_plummer_collision_generate",
+    "n_body_sim_pro_cuda_plummer_collision_generate", "n_body_sim_pro_cuda_correction_evaluate",
 )
+
+# NBodySimProCudaMlpEngine
+MLP_ENGINES = {"tcgen05": 0, "mma_sync": 1}
 
 # NBodySimProSimulationPreset (generation/presets.h:27-38)
 PRESETS = {"two_body": 0, "random_cloud": 1, "solar_system": 2, "open_cluster": 3,
@@ -285,6 +288,8 @@ def library() -> C.CDLL:
                                                         C.POINTER(C.c_float),
                                                         C.POINTER(C.c_float), C.c_size_t, pe]),
         "n_body_sim_pro_cuda_context_set_correction": (st, [vp, vp, pe]),
+        "n_body_sim_pro_cuda_correction_evaluate": (st, [vp, C.POINTER(C.c_float), C.c_size_t,
+                                                         C.POINTER(C.c_float), C.c_int, pe]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -759,6 +764,17 @@ class CudaCorrection:
             self.handle, _fptr(x), _fptr(y), x.shape[0], _fptr(g), C.byref(loss), C.byref(err)),
             err)
         return g, loss.value
+
+    def evaluate(self, features: np.ndarray, engine: str = "tcgen05") -> np.ndarray:
+        """The network on raw feature rows (n x 10) -> outputs (n x 3), on the
+        tcgen05 tensor cores ("tcgen05") or with warp-level mma.sync ("mma_sync")."""
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros((x.shape[0], 3), dtype=np.float32)
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_correction_evaluate(
+            self.handle, _fptr(x), x.shape[0], _fptr(out), MLP_ENGINES[engine], C.byref(err)),
+            err)
+        return out
 
     def samples(self, max_rows: int = 1 << 20):
         rows = C.c_size_t(0)

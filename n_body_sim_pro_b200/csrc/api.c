@@ -364,6 +364,9 @@ static NBodySimProStatus check_device_status(NBodySimProCudaContext* c, NBodySim
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "Barnes-Hut walk exceeded its step limit");
     if (bits & NBSP_DEVICE_ERROR_ENSEMBLE_LIMIT)
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "ensemble kernel exceeded its limits");
+    if (bits & NBSP_DEVICE_ERROR_MMA_TIMEOUT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE,
+                    "correction network: a tensor-core product did not complete in time");
     if (bits != 0) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_STATE, "unknown device status");
     return N_BODY_SIM_PRO_STATUS_OK;
 }

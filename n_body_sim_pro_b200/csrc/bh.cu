@@ -22,6 +22,7 @@
 // particles are summed exactly (a single particle is always exact).
 #include "bh.h"
 #include "mlp.cuh"
+#include "mlp_umma.cuh"
 
 #include <cuda_runtime.h>
 #include <limits.h>
@@ -1351,59 +1352,6 @@ __device__ __forceinline__ void quad_tile(const QuadTile& s, float4 p, float eps
   fold(hz, lz, v);
 }
 
-// Corrections of the learned walk: per cell its centre of mass and Y = M y
-// (the network's residual in units of M / |d|^2), pair-interleaved.
-struct CorrTile {
-  ulonglong2 xy[kStage / 2];  // {x}, {y}
-  ulonglong2 zu[kStage / 2];  // {z}, {Yx}
-  ulonglong2 vw[kStage / 2];  // {Yy}, {Yz}
-};
-
-__device__ __forceinline__ void stage_correction(CorrTile& s, int k, float4 c, float yx, float yy,
-                                                 float yz) {
-  const int i = k >> 1, o = k & 1;
-  float* a = reinterpret_cast<float*>(&s.xy[i]) + o;
-  float* b = reinterpret_cast<float*>(&s.zu[i]) + o;
-  float* e = reinterpret_cast<float*>(&s.vw[i]) + o;
-  a[0] = c.x;
-  a[2] = c.y;
-  b[0] = c.z;
-  b[2] = yx;
-  e[0] = yy;
-  e[2] = yz;
-}
-
-// a += Y / |d|^2 for the kStage corrections of a CorrTile (d = com - target,
-// unsoftened: accepted cells have |d| > 2h / theta > 0); far padding adds 0.
-__device__ __forceinline__ void corr_tile(const CorrTile& s, float4 p, float& hx, float& hy,
-                                          float& hz, float& lx, float& ly, float& lz) {
-  const unsigned long long PX = pack2(p.x, p.x), PY = pack2(p.y, p.y), PZ = pack2(p.z, p.z);
-  unsigned long long ax = 0ull, ay = 0ull, az = 0ull;
-#pragma unroll 8
-  for (int j = 0; j < kStage / 2; ++j) {
-    const ulonglong2 a = s.xy[j], b = s.zu[j], e = s.vw[j];
-    const unsigned long long dx = sub2(a.x, PX), dy = sub2(a.y, PY), dz = sub2(b.x, PZ);
-    const unsigned long long d2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
-    float d2a, d2b;
-    unpack2(d2, d2a, d2b);
-    const unsigned long long R = pack2(rsqrt_mufu(d2a), rsqrt_mufu(d2b));
-    const unsigned long long R2 = mul2(R, R);
-    ax = fma2(R2, b.y, ax);
-    ay = fma2(R2, e.x, ay);
-    az = fma2(R2, e.y, az);
-  }
-  float u, v;
-  unpack2(ax, u, v);
-  fold(hx, lx, u);
-  fold(hx, lx, v);
-  unpack2(ay, u, v);
-  fold(hy, ly, u);
-  fold(hy, ly, v);
-  unpack2(az, u, v);
-  fold(hz, lz, u);
-  fold(hz, lz, v);
-}
-
 // True when the target's own term in source_terms is W * 0 with W finite:
 // eps^2 a normal number and m * rsqrt(eps^2)^3, in the same operation order,
 // below overflow.
@@ -1705,9 +1653,7 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
-constexpr int kCorrRows = 96;      // corrected walk: network rows (< 32 waiting + < kListCap new)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
-constexpr int kCorrStack = 768;    // the corrected walk's (its network rows share the 48 KiB)
 
 // Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
 // traversal.  Each step the lanes pop up to 32 nodes from the warp's
@@ -1727,48 +1673,39 @@ constexpr int kCorrStack = 768;    // the corrected walk's (its network rows sha
 // A quadrupole cell goes into a QuadTile with its moments when it is accepted.
 // A warp whose stack would overflow restarts with the stackless walk.
 //
-// CORR: the learned far-field correction.  At every cell flush the gathered
-// cells' features are taken at the group centre, standardised, and pushed
-// through the MLP 16 cells at a time (one m16 tile per mma.sync); each target
-// then adds (M / |d|^2) * y to its monopole term, y the de-standardised network
-// output and d its own distance to the cell's centre of mass.  Cells whose
-// features fall outside the range seen in training, or that lie closer than
-// 1/kCorrGroup group radii to the group centre (where one evaluation cannot
-// stand for all 32 targets), keep the plain monopole.
+// CORR: the learned far-field correction, listed here and applied by the
+// correction pipeline that runs after the walk (corr_rows_kernel on the
+// tcgen05 tensor cores, then corr_apply_kernel).  An accepted monopole cell
+// whose opening ratio side / |com - group centre| lies in the range the
+// network saw in training, and that lies further than 1/kCorrGroup group radii
+// from the group centre (so one evaluation there stands for all 32 targets),
+// is appended to the group's list; the walk itself computes the plain
+// monopole, exactly as without the correction.
 // Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
-// walk 102 (5 blocks), corrected walk 170 (3 blocks; the network's tiles spill a little).
+// walk 102 (5 blocks).
 template <int ORDER, int STACK, bool CORR, bool REL>
-__global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
     double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status,
-    const nbsp_mlp::Net* __restrict__ net) {
-  static_assert(!(CORR && REL), "the network corrects cells the geometric test accepts");
+    const nbsp_mlp::Net* __restrict__ net, NbspCorrectionLists lists) {
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ float s_probe_k[kListThreads / 32][REL ? 32 : 1];  // their M side^2
-  __shared__ int s_cells[kListThreads / 32][CORR ? kListCap : 1];
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
   __shared__ int s_pref[kListThreads / 32][kListCap];     // exclusive prefix of the counts
-  // corrected walk: network input rows waiting for a full tile, their cells,
-  // and the outputs of one run of the network
-  __shared__ uint32_t s_x[kListThreads / 32][CORR ? kCorrRows * 8 : 1];
-  __shared__ int s_row[kListThreads / 32][CORR ? kCorrRows : 1];
-  __shared__ float s_y[kListThreads / 32][CORR ? kStage * 4 : 1];
-  // ORDER 1: accepted cells are point masses in the source tile (CORR: their
-  // corrections come from a separate list); ORDER 2: cells fill a QuadTile
+  // ORDER 1: accepted cells are point masses in the source tile; ORDER 2:
+  // cells fill a QuadTile
   static_assert(!(CORR && ORDER == 2), "the network corrects the monopole");
   __shared__ __align__(16) SourceTile s_src[kListThreads / 32];
   __shared__ __align__(16) QuadTile s_quad[ORDER == 2 ? kListThreads / 32 : 1];
-  __shared__ __align__(16) CorrTile s_corr[CORR ? kListThreads / 32 : 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   SourceTile& src = s_src[wib];
   int staged = 0;   // sources waiting in src (warp-uniform)
-  int pending = 0;  // corrected walk: network rows waiting in s_x (warp-uniform)
+  int listed = 0;   // corrected walk: cells listed for the network (warp-uniform)
   int qstaged = 0;  // cells waiting in the QuadTile (ORDER 2)
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
   int* stack = s_stack[wib];
-  int* cells = s_cells[wib];
   int2* leaves = s_leaves[wib];
   const int s = warp * 32 + lane;
   const bool active = s < n;
@@ -1794,15 +1731,16 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
   const float gx = 0.5f * (bx0 + bx1), gy = 0.5f * (by0 + by1), gz = 0.5f * (bz0 + bz1);
   const float ex = 0.5f * (bx1 - bx0), ey = 0.5f * (by1 - by0), ez = 0.5f * (bz1 - bz0);
   const float rg2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));  // group radius^2
+  if (CORR && lane == 0) reinterpret_cast<float4*>(lists.centre)[warp] = make_float4(gx, gy, gz, rg2);
 
   const int total = (int)t.offset[n];
   float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
   unsigned approx = 0, exact = 0;
-  int top = 1, ncell = 0, nleaf = 0, iters = 0;
+  int top = 1, nleaf = 0, iters = 0;
   bool overflow = false;
   if (lane == 0) stack[0] = 0;
   __syncwarp();
-  while (top > 0 || ncell > 0 || nleaf > 0) {
+  while (top > 0 || nleaf > 0) {
     if (top > 0) {
       if (++iters > total + 64) {  // every node is popped at most once
         if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
@@ -1885,8 +1823,21 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
         // this lane's registers from the opening test: it goes straight into
         // the source tile (evaluated whenever 64 sources have gathered).  The
         // corrected walk also lists the cell for its network evaluation.
-        if (CORR && accept) cells[ncell + __popc(m & lt)] = node;
-        if (CORR) ncell += __popc(m);
+        if (CORR) {
+          bool listme = false;
+          if (accept) {
+            const float side = t.side[node];
+            const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
+            const float dg2 = fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz));
+            const float lo = __ldg(&net->x_min[3]), hi = __ldg(&net->x_max[3]);
+            listme = kCorrGroup * kCorrGroup * dg2 > rg2 && side * side >= lo * lo * dg2 &&
+                     side * side <= hi * hi * dg2;
+          }
+          const unsigned lm = __ballot_sync(kFull, listme);
+          const int at = listed + __popc(lm & lt);
+          if (listme && at < lists.capacity) lists.cells[(size_t)warp * lists.capacity + at] = node;
+          listed += __popc(lm);
+        }
         const int nacc = __popc(m), rank = __popc(m & lt), room = kStage - staged;
         if (accept && rank < room) stage_source(src, staged + rank, c);
         if (nacc >= room) {
@@ -1939,106 +1890,6 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
       __syncwarp();
     }
     const bool drain = top == 0;
-    const bool flush_cells = ncell >= 32 || (drain && ncell > 0);
-    if (CORR && flush_cells) {
-      // Features of the listed cells; the cells the network may correct (in
-      // its training range, far enough from the group) are appended as rows
-      // to the warp's pending rows, so the network runs on full tiles.
-      uint32_t* xs = s_x[wib];
-      int* rows = s_row[wib];
-      int added = 0;
-      for (int r0 = 0; r0 < ncell; r0 += 32) {  // ncell < kListCap
-        const int r = r0 + lane;
-        float f[nbsp_mlp::kIn];
-        bool ok = false;
-        int node = 0;
-        if (r < ncell) {
-          node = cells[r];
-          const float4 c = t.com[node];
-          ok = cell_features(t, node, c, gx, gy, gz, f);
-          // the group centre must stand for every target: group radius
-          // below kCorrGroup of the distance, else the plain monopole
-          const float gdx = c.x - gx, gdy = c.y - gy, gdz = c.z - gz;
-          ok = ok && kCorrGroup * kCorrGroup * fmaf(gdx, gdx, fmaf(gdy, gdy, gdz * gdz)) > rg2;
-#pragma unroll
-          for (int q = 0; q < nbsp_mlp::kIn; ++q)
-            ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
-        }
-        const unsigned okm = __ballot_sync(kFull, ok);
-        const int row = pending + added + __popc(okm & lt);  // < kCorrRows
-        if (ok) {
-#pragma unroll
-          for (int w = 0; w < 8; ++w) {
-            const int q0 = 2 * w, q1 = 2 * w + 1;
-            const float v0 = q0 < nbsp_mlp::kIn ? (f[q0] - net->x_mean[q0]) * net->x_inv_std[q0] : 0.f;
-            const float v1 = q1 < nbsp_mlp::kIn ? (f[q1] - net->x_mean[q1]) * net->x_inv_std[q1] : 0.f;
-            xs[row * 8 + w] = nbsp_mlp::pack_bf16(v0, v1);
-          }
-          rows[row] = node;
-        }
-        added += __popc(okm);
-      }
-      if (lane == 0 && added > 0) atomicAdd(&counters[6], (unsigned long long)added);
-      pending += added;
-      __syncwarp();
-    }
-    // Run the network on whole 16-row tiles of the pending rows (up to kStage
-    // at a time) once 32 are waiting, and on all of them when the walk ends;
-    // each corrected cell becomes a correction source (centre of mass, Y = M y)
-    // in a CorrTile padded with far zero sources, and every lane adds
-    // Y / |d|^2 for its own target, two cells per instruction.
-    while (CORR && (pending >= 32 || (drain && pending > 0))) {
-      uint32_t* xs = s_x[wib];
-      int* rows = s_row[wib];
-      float* ys = s_y[wib];
-      const int nrun = drain ? min(pending, kStage) : min(pending & ~15, kStage);
-      const int padded = (nrun + 15) & ~15;  // rows past nrun are free only when nrun = pending
-      for (int r = nrun + lane; r < padded; r += 32)
-#pragma unroll
-        for (int w = 0; w < 8; ++w) xs[r * 8 + w] = 0u;
-      __syncwarp();
-      const int gq = lane >> 2, tq = lane & 3;
-      for (int mt = 0; mt < padded / 16; ++mt) {
-        const int ra = mt * 16 + gq, rb = ra + 8;
-        const uint32_t xa[4] = {xs[ra * 8 + tq], xs[rb * 8 + tq], xs[ra * 8 + tq + 4],
-                                xs[rb * 8 + tq + 4]};
-        float out[4];
-        nbsp_mlp::forward_tile(xa, net->w1, net->b1, net->w2, net->b2, net->w3, net->b3, lane,
-                               out);
-        if (tq < 2) {
-          ys[ra * 4 + 2 * tq] = out[0];
-          ys[ra * 4 + 2 * tq + 1] = out[1];
-          ys[rb * 4 + 2 * tq] = out[2];
-          ys[rb * 4 + 2 * tq + 1] = out[3];
-        }
-      }
-      __syncwarp();
-      CorrTile& ct = s_corr[CORR ? wib : 0];
-      const float ym0 = net->y_mean[0], ym1 = net->y_mean[1], ym2 = net->y_mean[2];
-      const float ys0 = net->y_std[0], ys1 = net->y_std[1], ys2 = net->y_std[2];
-      for (int r = lane; r < kStage; r += 32) {
-        float4 c = make_float4(kFarAway, kFarAway, kFarAway, 0.f);
-        float yx = 0.f, yy = 0.f, yz = 0.f;
-        if (r < nrun) {
-          c = t.com[rows[r]];
-          const float* ye = &ys[r * 4];
-          yx = c.w * fmaf(ye[0], ys0, ym0);
-          yy = c.w * fmaf(ye[1], ys1, ym1);
-          yz = c.w * fmaf(ye[2], ys2, ym2);
-        }
-        stage_correction(ct, r, c, yx, yy, yz);
-      }
-      __syncwarp();
-      corr_tile(ct, p, hx, hy, hz, lx, ly, lz);
-      // the rows not run move to the front (destinations lie >= 16 rows below
-      // their sources, so no word is overwritten before it is read)
-      const int left = pending - nrun;
-      for (int k = lane; k < left * 8; k += 32) xs[k] = xs[k + nrun * 8];
-      for (int k = lane; k < left; k += 32) rows[k] = rows[k + nrun];
-      pending = left;
-      __syncwarp();
-    }
-    if (CORR && flush_cells) ncell = 0;  // monopoles already staged, corrections applied
     if (nleaf >= 32 || (drain && nleaf > 0)) {
       // The buckets' particles, concatenated, fill the tile: each lane finds
       // the bucket of its slot by binary search over the exclusive prefix of
@@ -2098,6 +1949,11 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
     }
     __syncwarp();
   }
+  if (CORR && lane == 0) {  // a group walked again keeps the plain monopole
+    lists.count[warp] = overflow ? 0 : min(listed, lists.capacity);
+    if (!overflow && listed > lists.capacity)
+      atomicAdd(&counters[7], (unsigned long long)(listed - lists.capacity));
+  }
   WalkAcc a;
   if (overflow) {
     if (lane == 0) atomicAdd(&counters[5], 1ull);  // groups walked again
@@ -2113,6 +1969,156 @@ __global__ void __launch_bounds__(kListThreads, CORR ? 4 : ORDER == 1 ? 8 : 5) w
     a.exact = exact;
   }
   store_walk(a, s, active, lane, acc, counters);
+}
+
+// ---- the correction pipeline after a corrected walk ------------------------
+//
+// 1. corr_scan_kernel: exclusive prefix of the per-group list lengths (one
+//    row per listed (cell, group) pair, groups in order);
+// 2. corr_rows_kernel: every row's 10 features at its group centre, the
+//    network on 128-row tiles on the tcgen05 tensor cores, the de-standardised
+//    output (zero for features outside the training range: the plain
+//    monopole, the fallback);
+// 3. corr_apply_kernel: one warp per group adds (M / |d|^2) * y of its rows,
+//    in list order, to each target's walk result (deterministic).
+
+__global__ void __launch_bounds__(1024) corr_scan_kernel(NbspCorrectionLists lists, int groups,
+                                                         unsigned long long* counters) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < groups; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < groups ? lists.count[i] : 0;
+    int x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int u = __shfl_up_sync(kFull, x, off);
+      if (lane >= off) x += u;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = warp_sums[lane];
+      for (int off = 1; off < 32; off <<= 1) {
+        const int u = __shfl_up_sync(kFull, w, off);
+        if (lane >= off) w += u;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const int incl = x + (wid > 0 ? warp_sums[wid - 1] : 0);
+    const int c = carry;
+    if (i < groups) lists.offset[i] = c + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = c + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    lists.offset[groups] = carry;
+    atomicAdd(&counters[6], (unsigned long long)carry);  // network evaluations
+  }
+}
+
+__global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
+    const nbsp_mlp::Net* __restrict__ net, Tree t, NbspCorrectionLists lists, int groups,
+    int* status) {
+  extern __shared__ __align__(128) unsigned char umma_smem[];
+  nbsp_umma::Smem& sm = *reinterpret_cast<nbsp_umma::Smem*>(umma_smem);
+  nbsp_umma::setup(sm, nbsp_umma::weights_of(net), net);
+  const uint32_t tmem = sm.tmem;
+  uint32_t phase = 0;
+  const int rows = lists.offset[groups];
+  const int tiles = (rows + nbsp_umma::kRows - 1) / nbsp_umma::kRows;
+  const float4* centre = reinterpret_cast<const float4*>(lists.centre);
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int r = tile * nbsp_umma::kRows + threadIdx.x;
+    float v[nbsp_mlp::kIn];
+    bool ok = false;
+    if (r < rows) {
+      int lo = 0, hi = groups - 1;  // the group g with offset[g] <= r < offset[g + 1]
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (lists.offset[mid] <= r) lo = mid; else hi = mid - 1;
+      }
+      const int node = lists.cells[(size_t)lo * lists.capacity + (r - lists.offset[lo])];
+      const float4 g = centre[lo];
+      float f[nbsp_mlp::kIn];
+      ok = cell_features(t, node, t.com[node], g.x, g.y, g.z, f);
+#pragma unroll
+      for (int q = 0; q < nbsp_mlp::kIn; ++q) {
+        ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
+        v[q] = (f[q] - net->x_mean[q]) * net->x_inv_std[q];
+      }
+    }
+    if (!ok)
+#pragma unroll
+      for (int q = 0; q < nbsp_mlp::kIn; ++q) v[q] = 0.f;
+    nbsp_umma::put_inputs(sm, v);
+    nbsp_umma::fence_async_smem();
+    __syncthreads();
+    float y[3];
+    if (!nbsp_umma::forward(sm, tmem, phase, y)) {
+      if (threadIdx.x == 0) atomicOr(status, NBSP_DEVICE_ERROR_MMA_TIMEOUT);
+      break;
+    }
+    if (r < rows)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        lists.y[(size_t)r * 3 + c] = ok ? fmaf(y[c], net->y_std[c], net->y_mean[c]) : 0.f;
+  }
+  nbsp_umma::teardown(sm, tmem);
+}
+
+__global__ void __launch_bounds__(128) corr_apply_kernel(const float4* __restrict__ pos, int n,
+                                                         Tree t, NbspCorrectionLists lists,
+                                                         double4* __restrict__ acc) {
+  const int lane = threadIdx.x & 31;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g * 32 >= n) return;
+  const int s = g * 32 + lane;
+  const bool active = s < n;
+  const float4 p = pos[active ? s : n - 1];
+  const int cnt = lists.count[g], off = lists.offset[g];
+  float hx = 0.f, hy = 0.f, hz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+  for (int i0 = 0; i0 < cnt; i0 += 32) {
+    const int k = i0 + lane;
+    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+    float yx = 0.f, yy = 0.f, yz = 0.f;
+    if (k < cnt) {
+      c = t.com[lists.cells[(size_t)g * lists.capacity + k]];
+      const float* y = &lists.y[(size_t)(off + k) * 3];
+      yx = c.w * y[0];
+      yy = c.w * y[1];
+      yz = c.w * y[2];
+    }
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const int take = min(32, cnt - i0);
+    for (int j = 0; j < take; ++j) {
+      const float cx = __shfl_sync(kFull, c.x, j), cy = __shfl_sync(kFull, c.y, j);
+      const float cz = __shfl_sync(kFull, c.z, j);
+      const float Yx = __shfl_sync(kFull, yx, j), Yy = __shfl_sync(kFull, yy, j);
+      const float Yz = __shfl_sync(kFull, yz, j);
+      const float dx = cx - p.x, dy = cy - p.y, dz = cz - p.z;
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float r = d2 > 0.f ? rsqrt_mufu(d2) : 0.f;
+      const float w = r * r;
+      ax = fmaf(w, Yx, ax);
+      ay = fmaf(w, Yy, ay);
+      az = fmaf(w, Yz, az);
+    }
+    fold(hx, lx, ax);
+    fold(hy, ly, ay);
+    fold(hz, lz, az);
+  }
+  if (active && cnt > 0) {
+    double4 a = acc[s];
+    a.x += (double)hx + (double)lx;
+    a.y += (double)hy + (double)ly;
+    a.z += (double)hz + (double)lz;
+    acc[s] = a;
+  }
 }
 
 __global__ void tree_counts_kernel(Tree t, unsigned long long* counters) {
@@ -2131,19 +2137,20 @@ int grid_for(size_t n, int threads) {
 
 template <bool REL>
 void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order, int mode,
-                 const nbsp_mlp::Net* net, float eps2, double4* out, unsigned long long* counters,
-                 int* status, cudaStream_t stream) {
+                 const nbsp_mlp::Net* net, const NbspCorrectionLists* lists, float eps2,
+                 double4* out, unsigned long long* counters, int* status, cudaStream_t stream) {
   if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
-    if (!REL && net != nullptr) {  // the network corrects the monopole term
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kCorrStack, true, false><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, net);
+    NbspCorrectionLists none{};
+    if (net != nullptr && lists != nullptr) {  // the network corrects the monopole term
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true, REL><<<blocks, kListThreads, 0, stream>>>(
+          p, tol, (int)n, t, eps2, out, counters, status, net, *lists);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, nullptr);
+          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
     } else {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, nullptr);
+          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
     }
     return;
   }
@@ -2270,16 +2277,33 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
 }
 
 void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree, int order,
-                  int mode, const void* correction, float eps2, void* acc,
-                  unsigned long long* counters, int* status, cudaStream_t stream) {
+                  int mode, const void* correction, const NbspCorrectionLists* lists, float eps2,
+                  void* acc, unsigned long long* counters, int* status, cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
   const float4* p = (const float4*)pos4;
   double4* out = (double4*)acc;
-  if (tol != nullptr && net == nullptr)
-    launch_walk<true>(p, tol, n, t, order, mode, net, eps2, out, counters, status, stream);
+  if (tol != nullptr)
+    launch_walk<true>(p, tol, n, t, order, mode, net, lists, eps2, out, counters, status, stream);
   else
-    launch_walk<false>(p, nullptr, n, t, order, mode, net, eps2, out, counters, status, stream);
+    launch_walk<false>(p, nullptr, n, t, order, mode, net, lists, eps2, out, counters, status,
+                       stream);
+}
+
+void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* correction,
+                     const NbspCorrectionLists* lists, void* acc, unsigned long long* counters,
+                     int* status, cudaStream_t stream) {
+  Tree t = tree_view(const_cast<void*>(tree), n);
+  const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
+  const int groups = (int)((n + 31) / 32);
+  NBSP_COUNT_LAUNCH(1), corr_scan_kernel<<<1, 1024, 0, stream>>>(*lists, groups, counters);
+  const int smem = (int)sizeof(nbsp_umma::Smem);
+  cudaFuncSetAttribute(corr_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // persistent: three 62-KB CTAs per SM, each holding 128 TMEM columns
+  NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * 3, nbsp_umma::kThreads, smem, stream>>>(
+      net, t, *lists, groups, status);
+  NBSP_COUNT_LAUNCH(1), corr_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
+      (const float4*)pos4, (int)n, t, *lists, (double4*)acc);
 }
 
 void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n, double g, double* ax,

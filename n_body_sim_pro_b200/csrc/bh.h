@@ -142,12 +142,32 @@ enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
  * mode NBSP_BH_WALK_STACKLESS: warp-coherent skip-link walk, per-target test;
  * mode NBSP_BH_WALK_LISTS: lane-parallel node tests against the warp's group
  * box, dense evaluation of gathered interaction lists. */
+/* Per 32-target group, the cells a corrected walk lists for the network, and
+ * the pipeline's rows: row r = offset[g] + k is cell k of group g. */
+typedef struct NbspCorrectionLists {
+    int* cells;     /* [groups * capacity] node ids, in the walk's order */
+    int* count;     /* [groups] listed cells kept (<= capacity) */
+    int* offset;    /* [groups + 1] exclusive prefix of count */
+    float* centre;  /* [groups * 4] group centre x, y, z and group radius^2 */
+    float* y;       /* [groups * capacity * 3] network outputs per row */
+    int capacity;   /* cells per group; more are left to the plain monopole and counted */
+} NbspCorrectionLists;
+
 NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree,
                               int order, int mode, const void* correction,
-                              float softening_squared, void* acc, unsigned long long* counters,
-                              int* status, cudaStream_t stream);
-/* (tol != NULL and no correction: every opening test also takes the relative
- * test with the per-target tolerances tol, Morton order) */
+                              const NbspCorrectionLists* lists, float softening_squared,
+                              void* acc, unsigned long long* counters, int* status,
+                              cudaStream_t stream);
+/* (tol != NULL: every opening test also takes the relative test with the
+ * per-target tolerances tol, Morton order; correction != NULL: the monopole
+ * walk lists cells into `lists` for nbsp_bh_correct) */
+
+/* After a corrected walk: the network on every listed (cell, group) row on the
+ * tcgen05 tensor cores and the corrections added to the walk's result acc. */
+NBSP_HIDDEN void nbsp_bh_correct(const void* pos4, size_t n, const void* tree,
+                                 const void* correction, const NbspCorrectionLists* lists,
+                                 void* acc, unsigned long long* counters, int* status,
+                                 cudaStream_t stream);
 
 /* Learned correction: training pairs (target, accepted cell) sampled with the
  * opening criterion `opening` at theta, their features and exact-sum labels, and

@@ -13,6 +13,9 @@
 #include <string.h>
 
 enum { BH_EVENTS = 8, BH_COUNTERS = 8 };
+/* cells a corrected walk lists per 32-target group for the network; further
+ * ones keep the plain monopole (counted in counters[7]) */
+enum { BH_CORRECTION_CAPACITY = 512 };
 
 struct NbspBarnesHut {
     size_t capacity;
@@ -30,6 +33,8 @@ struct NbspBarnesHut {
     uint32_t* inverse;  /* Morton slot of each input particle */
     float* tol_unsorted; /* relative opening test: tolerance per particle, input order */
     float* tol;          /* the same in Morton order */
+    NbspCorrectionLists lists;          /* corrected walk (allocated on first use) */
+    size_t lists_groups;
     unsigned long long* counters;       /* device */
     unsigned long long* host_counters;  /* pinned */
     cudaEvent_t events[BH_EVENTS];
@@ -64,6 +69,31 @@ static NBodySimProStatus bh_cuda(NBodySimProError* error, cudaError_t code, cons
             return bh_cuda(error, bh_try_code, #call, __LINE__);         \
     } while (0)
 
+static void release_lists(NbspBarnesHut* b) {
+    cudaFree(b->lists.cells);
+    cudaFree(b->lists.count);
+    cudaFree(b->lists.offset);
+    cudaFree(b->lists.centre);
+    cudaFree(b->lists.y);
+    memset(&b->lists, 0, sizeof(b->lists));
+    b->lists_groups = 0;
+}
+
+static NBodySimProStatus ensure_lists(NbspBarnesHut* b, size_t n, NBodySimProError* error) {
+    const size_t groups = (n + 31) / 32;
+    if (groups <= b->lists_groups) return N_BODY_SIM_PRO_STATUS_OK;
+    release_lists(b);
+    const size_t cap = BH_CORRECTION_CAPACITY;
+    BH_TRY(cudaMalloc((void**)&b->lists.cells, groups * cap * sizeof(int)));
+    BH_TRY(cudaMalloc((void**)&b->lists.count, groups * sizeof(int)));
+    BH_TRY(cudaMalloc((void**)&b->lists.offset, (groups + 1) * sizeof(int)));
+    BH_TRY(cudaMalloc((void**)&b->lists.centre, groups * 4 * sizeof(float)));
+    BH_TRY(cudaMalloc((void**)&b->lists.y, groups * cap * 3 * sizeof(float)));
+    b->lists.capacity = (int)cap;
+    b->lists_groups = groups;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
 static void release_buffers(NbspBarnesHut* b) {
     void* buffers[] = {b->partial, b->geometry, b->keys, b->keys_alt, b->index, b->index_alt,
                        b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->inverse,
@@ -82,6 +112,7 @@ static void release_buffers(NbspBarnesHut* b) {
 void nbsp_bh_destroy(NbspBarnesHut* b) {
     if (b == NULL) return;
     release_buffers(b);
+    release_lists(b);
     cudaFree(b->counters);
     cudaFreeHost(b->host_counters);
     for (int k = 0; k < BH_EVENTS; ++k)
@@ -158,12 +189,11 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     }
     BH_TRY(cudaMemsetAsync(b->counters, 0, BH_COUNTERS * sizeof(unsigned long long), stream));
     cudaEventRecord(b->events[0], stream);
-    /* relative opening test: tolerance alpha |a_old| / G (the correction uses
-     * the geometric test its network was trained with) */
+    /* relative opening test: tolerance alpha |a_old| / G */
     const double g = fabs(p->gravitational_constant);
-    const double tol_scale = p->tolerance > 0.0 && p->correction == NULL
-                                 ? (g > 0.0 ? p->tolerance / g : INFINITY)
-                                 : 0.0;
+    const double tol_scale = p->tolerance > 0.0 ? (g > 0.0 ? p->tolerance / g : INFINITY) : 0.0;
+    if (p->correction != NULL && (st = ensure_lists(b, n, error)) != N_BODY_SIM_PRO_STATUS_OK)
+        return st;
     const int rel = tol_scale > 0.0;
     morton(b, s, tol_scale, status, stream);
     nbsp_bh_duplicates(b->keys, b->index, s->x, s->y, s->z, n, status, stream);
@@ -176,8 +206,11 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
                     status, stream);
     cudaEventRecord(b->events[5], stream);
     nbsp_bh_walk(b->pos4, rel ? b->tol : NULL, n, b->tree, p->multipole_order, p->walk_mode,
-                 p->correction,
+                 p->correction, p->correction != NULL ? &b->lists : NULL,
                  (float)p->softening_squared, b->acc, b->counters, status, stream);
+    if (p->correction != NULL)
+        nbsp_bh_correct(b->pos4, n, b->tree, p->correction, &b->lists, b->acc, b->counters,
+                        status, stream);
     cudaEventRecord(b->events[6], stream);
     nbsp_bh_unsort(b->acc, b->inverse, n, p->gravitational_constant, s->ax, s->ay, s->az,
                    stream);

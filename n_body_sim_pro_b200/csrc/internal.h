@@ -29,7 +29,9 @@ enum {
     NBSP_DEVICE_ERROR_WALK_LIMIT = 2,
     NBSP_DEVICE_ERROR_TREE_INCONSISTENT = 4,
     NBSP_DEVICE_ERROR_ENSEMBLE_LIMIT = 8,
-    NBSP_DEVICE_ERROR_DUPLICATE_POSITION = 16
+    NBSP_DEVICE_ERROR_DUPLICATE_POSITION = 16,
+    /* a tensor-core product (tcgen05) did not complete within its wait limit */
+    NBSP_DEVICE_ERROR_MMA_TIMEOUT = 32
 };
 
 /* ---- all-pairs / KDK / diagnostics (allpairs.cu) ------------------------- */

@@ -13,6 +13,7 @@
 // L = 1 / (3 B) sum_r sum_c (y_rc - t_rc)^2.
 #include "internal.h"
 #include "mlp.cuh"
+#include "mlp_umma.cuh"
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -351,6 +352,69 @@ __global__ void build_frags_kernel(const float* __restrict__ params, TrainFrags*
       net->b2[i] = f->b2[i];
     }
     for (int i = threadIdx.x; i < kOutPad; i += blockDim.x) net->b3[i] = f->b3[i];
+    nbsp_umma::build_weights(params, reinterpret_cast<nbsp_umma::Weights*>(net->umma_w));
+  }
+}
+
+// The network on raw feature rows (10 per row): standardised, through the
+// three layers, de-standardised into out (3 per row).  tcgen05 path: one
+// 128-row tile per iteration of a persistent CTA.
+__global__ void __launch_bounds__(nbsp_umma::kThreads) evaluate_umma_kernel(
+    const Net* __restrict__ net, const float* __restrict__ feat, int rows,
+    float* __restrict__ out, int* status) {
+  extern __shared__ __align__(128) unsigned char umma_smem[];
+  nbsp_umma::Smem& s = *reinterpret_cast<nbsp_umma::Smem*>(umma_smem);
+  nbsp_umma::setup(s, nbsp_umma::weights_of(net), net);
+  const uint32_t tmem = s.tmem;
+  uint32_t phase = 0;
+  const int tiles = (rows + nbsp_umma::kRows - 1) / nbsp_umma::kRows;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int r = tile * nbsp_umma::kRows + threadIdx.x;
+    float v[kIn];
+#pragma unroll
+    for (int q = 0; q < kIn; ++q)
+      v[q] = r < rows ? (feat[(size_t)r * kIn + q] - net->x_mean[q]) * net->x_inv_std[q] : 0.f;
+    nbsp_umma::put_inputs(s, v);
+    nbsp_umma::fence_async_smem();
+    __syncthreads();
+    float y[3];
+    if (!nbsp_umma::forward(s, tmem, phase, y)) {
+      if (threadIdx.x == 0) atomicOr(status, NBSP_DEVICE_ERROR_MMA_TIMEOUT);
+      break;
+    }
+    if (r < rows)
+      for (int c = 0; c < kOut; ++c)
+        out[(size_t)r * kOut + c] = fmaf(y[c], net->y_std[c], net->y_mean[c]);
+  }
+  nbsp_umma::teardown(s, tmem);
+}
+
+// The same with mma.sync: one warp per 16 rows (the corrected walk's former
+// per-warp path, kept as the cross-check of the tcgen05 one).
+__global__ void evaluate_sync_kernel(const Net* __restrict__ net, const float* __restrict__ feat,
+                                     int rows, float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (tile * 16 >= rows) return;
+  const int g = lane >> 2, t = lane & 3;
+  auto val = [&](int row, int q) -> float {
+    const int r = tile * 16 + row;
+    return (r < rows && q < kIn) ? (feat[(size_t)r * kIn + q] - net->x_mean[q]) * net->x_inv_std[q]
+                                 : 0.f;
+  };
+  const uint32_t x[4] = {pack_bf16(val(g, 2 * t), val(g, 2 * t + 1)),
+                         pack_bf16(val(g + 8, 2 * t), val(g + 8, 2 * t + 1)),
+                         pack_bf16(val(g, 2 * t + 8), val(g, 2 * t + 9)),
+                         pack_bf16(val(g + 8, 2 * t + 8), val(g + 8, 2 * t + 9))};
+  float o[4];
+  forward_tile(x, net->w1, net->b1, net->w2, net->b2, net->w3, net->b3, lane, o);
+  // o: C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]; outputs are columns 0..2
+  for (int h = 0; h < 2; ++h) {
+    const int r = tile * 16 + g + 8 * h;
+    for (int k = 0; k < 2; ++k) {
+      const int c = 2 * t + k;
+      if (r < rows && c < kOut) out[(size_t)r * kOut + c] = fmaf(o[2 * h + k], net->y_std[c], net->y_mean[c]);
+    }
   }
 }
 
@@ -411,6 +475,23 @@ void nbsp_mlp_train_step(const uint32_t* x, const float* y, const int* order, in
   cudaFuncSetAttribute(train_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   NBSP_COUNT_LAUNCH(1), train_step_kernel<<<ctas, kRows * 2, smem, stream>>>(
       x, y, order, first_row, rows_total, inv_batch3, (const TrainFrags*)frags, partial, loss);
+}
+
+void nbsp_mlp_evaluate(const void* net, const float* feat, int rows, float* out, int tcgen05,
+                       int* status, cudaStream_t stream) {
+  if (rows <= 0) return;
+  if (tcgen05) {
+    const int smem = (int)sizeof(nbsp_umma::Smem);
+    cudaFuncSetAttribute(evaluate_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int tiles = (rows + nbsp_umma::kRows - 1) / nbsp_umma::kRows;
+    const int grid = tiles < 148 * 3 ? tiles : 148 * 3;
+    NBSP_COUNT_LAUNCH(1), evaluate_umma_kernel<<<grid, nbsp_umma::kThreads, smem, stream>>>(
+        (const Net*)net, feat, rows, out, status);
+  } else {
+    const int warps = (rows + 15) / 16;
+    NBSP_COUNT_LAUNCH(1), evaluate_sync_kernel<<<(warps + 3) / 4, 128, 0, stream>>>(
+        (const Net*)net, feat, rows, out);
+  }
 }
 
 void nbsp_mlp_reduce_adam(const float* partial, int slots, float* grad_out, float* params, float* m,

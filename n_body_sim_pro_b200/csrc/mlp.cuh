@@ -55,6 +55,9 @@ struct Net {
   float b3[kOutPad];
   float x_mean[kIn], x_inv_std[kIn], x_min[kIn], x_max[kIn];
   float y_mean[kOut], y_std[kOut];
+  // the same weights as BF16 operand images of the tcgen05 products
+  // (nbsp_umma::Weights, mlp_umma.cuh): W1 64 x 16, W2 64 x 64, W3 16 x 64
+  uint4 umma_w[(64 * 16 + 64 * 64 + 16 * 64) / 8];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {

@@ -35,6 +35,8 @@ NBSP_HIDDEN void nbsp_mlp_train_step(const uint32_t* x, const float* y, const in
 NBSP_HIDDEN void nbsp_mlp_reduce_adam(const float* partial, int slots, float* grad_out,
                                       float* params, float* m, float* v, float lr, int step,
                                       int apply, cudaStream_t stream);
+NBSP_HIDDEN void nbsp_mlp_evaluate(const void* net, const float* feat, int rows, float* out,
+                                   int tcgen05, int* status, cudaStream_t stream);
 NBSP_HIDDEN void nbsp_mlp_set_scaling(void* net, const float* table, cudaStream_t stream);
 NBSP_HIDDEN void nbsp_mlp_get_scaling(const void* net, float* table, cudaStream_t stream);
 
@@ -531,5 +533,51 @@ NBodySimProStatus n_body_sim_pro_cuda_correction_samples(NBodySimProCudaCorrecti
         MTRY(cudaMemcpy(features, c->feat, k * IN * sizeof(float), cudaMemcpyDeviceToHost));
     if (labels != NULL && k > 0)
         MTRY(cudaMemcpy(labels, c->lab, k * OUT * sizeof(float), cudaMemcpyDeviceToHost));
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_correction_evaluate(NBodySimProCudaCorrection* c,
+                                                          const float* features, size_t rows,
+                                                          float* outputs, int engine,
+                                                          NBodySimProError* error) {
+    if (c == NULL || (rows > 0 && (features == NULL || outputs == NULL)))
+        return mfail(error, N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, __LINE__,
+                     "correction, features and outputs must not be null");
+    if (engine != N_BODY_SIM_PRO_CUDA_MLP_TCGEN05 && engine != N_BODY_SIM_PRO_CUDA_MLP_MMA_SYNC)
+        return mfail(error, N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, __LINE__, "unknown engine");
+    if (rows > (size_t)(1 << 30))
+        return mfail(error, N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, __LINE__,
+                     "at most 2^30 rows per call");
+    if (rows == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    MTRY(cudaSetDevice(c->device));
+    float *d_in = NULL, *d_out = NULL;
+    int* d_status = NULL;
+    int host_status = 0;
+    cudaError_t code = cudaMalloc((void**)&d_in, rows * IN * sizeof(float));
+    if (code == cudaSuccess) code = cudaMalloc((void**)&d_out, rows * OUT * sizeof(float));
+    if (code == cudaSuccess) code = cudaMalloc((void**)&d_status, sizeof(int));
+    if (code == cudaSuccess) code = cudaMemsetAsync(d_status, 0, sizeof(int), c->stream);
+    if (code == cudaSuccess)
+        code = cudaMemcpyAsync(d_in, features, rows * IN * sizeof(float), cudaMemcpyHostToDevice,
+                               c->stream);
+    if (code == cudaSuccess) {
+        nbsp_mlp_evaluate(c->net, d_in, (int)rows, d_out, engine == N_BODY_SIM_PRO_CUDA_MLP_TCGEN05,
+                          d_status, c->stream);
+        code = cudaGetLastError();
+    }
+    if (code == cudaSuccess)
+        code = cudaMemcpyAsync(outputs, d_out, rows * OUT * sizeof(float), cudaMemcpyDeviceToHost,
+                               c->stream);
+    if (code == cudaSuccess)
+        code = cudaMemcpyAsync(&host_status, d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream);
+    if (code == cudaSuccess) code = cudaStreamSynchronize(c->stream);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFree(d_status);
+    if (code != cudaSuccess) return mcuda(error, code, __LINE__, "correction evaluate");
+    if (host_status != 0)
+        return mfail(error, N_BODY_SIM_PRO_STATUS_INVALID_STATE, __LINE__,
+                     "correction network: a tensor-core product did not complete in time");
     return N_BODY_SIM_PRO_STATUS_OK;
 }

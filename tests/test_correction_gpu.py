@@ -41,6 +41,33 @@ def test_gradient_matches_fp64_cpu(cuda):
         k += n
 
 
+@pytest.mark.parametrize("rows", [128, 1000])
+def test_tcgen05_forward_matches_mma_sync_and_fp64(cuda, rows):
+    """The tcgen05 inference (128-row tiles, operands in shared memory,
+    accumulators in tensor memory) against the warp-level mma.sync forward and
+    the FP64 CPU MLP on the same BF16-rounded inputs and weights.  Both GPU
+    paths round the hidden activations to BF16, so they agree to ~1e-3 and the
+    FP64 chain to ~1e-2 (relative L2)."""
+    rng = np.random.default_rng(5)
+    feat = rng.standard_normal((rows, 10)).astype(np.float32)
+    with cuda.CudaCorrection(seed=7) as corr:
+        p, s = corr.parameters()
+        y_tc = corr.evaluate(feat, "tcgen05")
+        y_ms = corr.evaluate(feat, "mma_sync")
+    x_mean, x_inv, y_mean, y_std = s[0:10], s[10:20], s[40:43], s[43:46]
+    x = M.bf16((feat - x_mean) * x_inv)
+    w = M.unpack(p)
+    for k in ("W1", "W2", "W3"):
+        w[k] = M.bf16(w[k])
+    ref = M.forward(M.pack(w), x) * y_std + y_mean
+    assert np.all(np.isfinite(y_tc)) and np.all(np.isfinite(y_ms))
+    d_sync = np.linalg.norm(y_tc - y_ms) / np.linalg.norm(y_ms)
+    d_ref = np.linalg.norm(y_tc - ref) / np.linalg.norm(ref)
+    print(f"rows={rows}: tcgen05 vs mma.sync {d_sync:.2e}, vs FP64 {d_ref:.2e}")
+    assert d_sync < 1e-2
+    assert d_ref < 2e-2
+
+
 def test_parameters_round_trip(cuda):
     with cuda.CudaCorrection(seed=5) as corr:
         p, s = corr.parameters()
