@@ -104,9 +104,10 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 
 # relative opening test over the reference test at theta 1.0: the alphas of its sweep
 ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
               0.007, 0.01)
-# the corrected walk under the relative test: the correction lowers the error
-# of the cells it accepts, so the sweep reaches further
-ALPHA_GRID_CORRECTED = ALPHA_GRID + (0.0125, 0.015, 0.02)
+# the learned correction at matched accuracy: trained and evaluated at each of
+# these opening angles (its training pairs are the near cells the walk at that
+# angle accepts)
+CORRECTED_THETAS = (0.7, 0.75, 0.8, 0.9)
 OPENINGS = {"reference": 0, "offset": 1}
 N_TARGETS = 4096  # seeded targets of the FP64 direct-sum oracle
 # energy drift needs the O(N^2) FP64 potential: measured directly up to
@@ -467,17 +468,18 @@ def energy_drift(nb, system, g, wl, m, steps, correction=None):
     return float(abs(e1 - e0) / abs(e0))
 
 
-def train_correction(nb, g, opening, n_train=1_000_000, samples=1 << 22, seed=42):
+def train_correction(nb, g, opening, theta=1.0, n_train=1_000_000, samples=1 << 22, seed=42):
     """The learned correction, trained on the GPU on 2^22 cell-target pairs of
-    the 1M collision (labels: exact cell sums by the all-pairs arithmetic)."""
+    the 1M collision sampled with the opening test at `theta` (labels: exact
+    cell sums by the all-pairs arithmetic)."""
     corr = nb.CudaCorrection(seed=11)
-    with nb.CudaContext(theta=1.0, opening=OPENINGS[opening]) as c1:
+    with nb.CudaContext(theta=theta, opening=OPENINGS[opening]) as c1:
         c1.generate_plummer_collision(n_train, seed)
         t0 = time.time()
-        corr.generate(c1, g, theta=1.0, samples=samples, seed=3)
+        corr.generate(c1, g, theta=theta, samples=samples, seed=3)
         _, vl = corr.train(epochs=8, batch=1024, learning_rate=1e-3)
         seconds = time.time() - t0
-    return corr, {"pairs": samples, "from": f"collision N={n_train}", "epochs": 8,
+    return corr, {"pairs": samples, "from": f"collision N={n_train}", "theta": theta, "epochs": 8,
                   "final_validation_loss": float(vl[-1]), "seconds": round(seconds, 2)}
 
 
@@ -553,10 +555,12 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
         r05 = dict(sweep["order1_reference"])[0.5]
         out["plain_theta_0.5"] = timed(method("plain_theta_0.5", 0.5), r05)
         corrected = {}
-        for oname in OPENINGS:
+        for oname in OPENINGS:  # theta 1.0, the opening angle of the target
             corr, training = train_correction(nb, g, oname)
-            corrections[oname] = corr
+            key = f"{oname}@1.0"
+            corrections[key] = corr
             m = method(f"corrected_{oname}", 1.0, opening=oname, corrected=True)
+            m["correction"] = key
             cctx = make_context(nb, m, corr)
             cctx.upload(system)
             r = accuracy(nb, cctx, g, targets, ref)
@@ -566,31 +570,37 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
             rec = timed(m, r, corr)
             rec["uncorrected_rms_at_theta_1.0"] = dict(sweep[f"order1_{oname}"])[1.0][0]
             rec["network"] = {"evaluations_per_walk": evals, "flop_per_evaluation": MLP_FLOPS,
-                              "walk_ms": round(walk_ms, 4),
+                              "walk_ms_with_network": round(walk_ms, 4),
                               "tensor_tflops_in_walk": round(evals * MLP_FLOPS / (walk_ms * 1e-3)
                                                              / 1e12, 3) if walk_ms > 0 else None}
             rec["training"] = training
             corrected[oname] = rec
             if r[0] <= RMS_TARGET:
                 methods.append(rec)
-            if oname == "reference":  # the corrected walk with the relative test on top
-                cctx = make_context(nb, method("", 1.0, leaf=32, corrected=True), corr)
-                cctx.upload(system)
-                rows = []
-                for alpha in ALPHA_GRID_CORRECTED:
-                    cctx.set_relative_opening(alpha)
-                    rows.append((alpha, accuracy(nb, cctx, g, targets, ref)))
-                cctx.close()
-                out["sweep"]["corrected_relative_alpha_theta1.0_leaf32"] = [
-                    [a, round(r[0], 6)] for a, r in rows]
-                b = best(rows)
-                if b:
-                    m = method("corrected_relative_leaf32", 1.0, alpha=b[0], leaf=32,
-                               corrected=True)
-                    rec = timed(m, b[1], corr)
-                    rec["training"] = training
-                    methods.append(rec)
-                    out["corrected_relative"] = rec
+        # the corrected walk at matched accuracy: the largest angle whose
+        # corrected error meets the target, the network trained at that angle
+        rows = []
+        for th in CORRECTED_THETAS:
+            corr, training = train_correction(nb, g, "reference", theta=th)
+            key = f"reference@{th}"
+            corrections[key] = corr
+            m = method("corrected_matched", th, corrected=True)
+            m["correction"] = key
+            cctx = make_context(nb, m, corr)
+            cctx.upload(system)
+            r = accuracy(nb, cctx, g, targets, ref)
+            cctx.close()
+            rows.append((th, r, m, training))
+        out["sweep"]["corrected_reference_trained_at_theta"] = [[th, round(r[0], 6)]
+                                                               for th, r, _, _ in rows]
+        ok = [row for row in rows if row[1][0] <= RMS_TARGET]
+        if ok:
+            th, r, m, training = max(ok, key=lambda row: row[0])
+            rec = timed(m, r, corrections[m["correction"]])
+            rec["uncorrected_rms"] = dict(sweep["order1_reference"]).get(th, (None,))[0]
+            rec["training"] = training
+            methods.append(rec)
+            out["corrected_matched"] = rec
         out["corrected_theta_1.0"] = corrected
     out["chosen"] = max(methods, key=lambda m: m["value"]) if methods else None
     if out["plain"] and out["chosen"]:
@@ -608,11 +618,11 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
     else:
         wl1, small, note = wl, system, f"{wl['n']} particles, {DRIFT_STEPS} steps"
     reported = [out.get("plain_theta_0.5"), out["plain"], out["relative"],
-                out.get("corrected_relative"), out["chosen"]]
+                out.get("corrected_matched"), out["chosen"]]
     reported += list(out.get("corrected_theta_1.0", {}).values())
     for rec in reported:
         if rec is not None and "energy_drift" not in rec:
-            corr = corrections.get(rec["opening"]) if rec["corrected"] else None
+            corr = corrections.get(rec.get("correction")) if rec["corrected"] else None
             rec["energy_drift"] = energy_drift(nb, small, g, wl1, rec, DRIFT_STEPS, corr)
             rec["energy_drift_over"] = note
     return out, corrections
@@ -638,11 +648,13 @@ def run_bh(args, wl, world, rank, local, steps, warmup, with_e2e=True):
         study, corrections = matched_study(nb, torch, wl, system, g, targets, ref0,
                                            min(steps, 5), 3, flush,
                                            with_correction=wl.get("correction", False))
-        m = {k: study["chosen"][k] for k in ("name", "theta", "multipole_order", "opening",
-                                             "relative_alpha", "leaf_capacity", "corrected")}
+        m = {k: study["chosen"].get(k) for k in ("name", "theta", "multipole_order", "opening",
+                                                 "relative_alpha", "leaf_capacity", "corrected",
+                                                 "correction")}
     else:
-        m = method("plain", wl["theta"], wl.get("order", 1), leaf=wl.get("leaf", 16))
-    correction = corrections.get(m["opening"]) if m["corrected"] else None
+        m = method("configured" if wl.get("alpha") else "plain", wl["theta"], wl.get("order", 1),
+                   alpha=wl.get("alpha", 0.0), leaf=wl.get("leaf", 16))
+    correction = corrections.get(m.get("correction")) if m["corrected"] else None
     ctx = make_context(nb, m, correction)
     ctx.set_walk(0 if wl.get("walk") == "stackless" else 1)
     ctx.upload(system)
@@ -1247,9 +1259,11 @@ def main(argv=None):
     ap.add_argument("--order", type=int, default=None, choices=[1, 2])
     ap.add_argument("--walk", default=None, choices=["lists", "stackless"])
     ap.add_argument("--leaf", type=int, default=None)
+    ap.add_argument("--alpha", type=float, default=None,
+                    help="relative opening test tolerance (with --no-matched)")
     args = ap.parse_args(argv)
     wl = dict(WORKLOADS[args.workload])
-    for key in ("theta", "order", "walk", "leaf"):
+    for key in ("theta", "order", "walk", "leaf", "alpha"):
         if getattr(args, key) is not None:
             wl[key] = getattr(args, key)
     if args.steps is None:
@@ -1326,7 +1340,7 @@ def main(argv=None):
                 "relative": pick(study.get("relative")),
                 "corrected_theta_1.0": {k: pick(v) for k, v in
                                         study.get("corrected_theta_1.0", {}).items()},
-                "corrected_relative": pick(study.get("corrected_relative")),
+                "corrected_matched": pick(study.get("corrected_matched")),
                 "chosen_over_plain_theta_0.5": (round(r["value"] /
                                                       study["plain_theta_0.5"]["value"], 3)
                                                 if study.get("plain_theta_0.5") else None),

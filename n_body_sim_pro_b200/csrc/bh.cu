@@ -2021,6 +2021,15 @@ __global__ void __launch_bounds__(1024) corr_scan_kernel(NbspCorrectionLists lis
   }
 }
 
+// Row r -> its group, one warp per group (the rows kernel then needs no search).
+__global__ void __launch_bounds__(128) corr_rowmap_kernel(NbspCorrectionLists lists, int groups) {
+  const int lane = threadIdx.x & 31;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g >= groups) return;
+  const int cnt = lists.count[g], off = lists.offset[g];
+  for (int k = lane; k < cnt; k += 32) lists.group[off + k] = g;
+}
+
 __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
     const nbsp_mlp::Net* __restrict__ net, Tree t, NbspCorrectionLists lists, int groups,
     int* status) {
@@ -2037,13 +2046,9 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
     float v[nbsp_mlp::kIn];
     bool ok = false;
     if (r < rows) {
-      int lo = 0, hi = groups - 1;  // the group g with offset[g] <= r < offset[g + 1]
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (lists.offset[mid] <= r) lo = mid; else hi = mid - 1;
-      }
-      const int node = lists.cells[(size_t)lo * lists.capacity + (r - lists.offset[lo])];
-      const float4 g = centre[lo];
+      const int grp = lists.group[r];
+      const int node = lists.cells[(size_t)grp * lists.capacity + (r - lists.offset[grp])];
+      const float4 g = centre[grp];
       float f[nbsp_mlp::kIn];
       ok = cell_features(t, node, t.com[node], g.x, g.y, g.z, f);
 #pragma unroll
@@ -2297,10 +2302,12 @@ void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* c
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
   const int groups = (int)((n + 31) / 32);
   NBSP_COUNT_LAUNCH(1), corr_scan_kernel<<<1, 1024, 0, stream>>>(*lists, groups, counters);
+  NBSP_COUNT_LAUNCH(1), corr_rowmap_kernel<<<(unsigned)((groups + 3) / 4), 128, 0, stream>>>(
+      *lists, groups);
   const int smem = (int)sizeof(nbsp_umma::Smem);
   cudaFuncSetAttribute(corr_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  // persistent: three 62-KB CTAs per SM, each holding 128 TMEM columns
-  NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * 3, nbsp_umma::kThreads, smem, stream>>>(
+  // persistent: four 49-KB CTAs per SM, each holding 128 of the 512 TMEM columns
+  NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * 4, nbsp_umma::kThreads, smem, stream>>>(
       net, t, *lists, groups, status);
   NBSP_COUNT_LAUNCH(1), corr_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
       (const float4*)pos4, (int)n, t, *lists, (double4*)acc);
