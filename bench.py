@@ -107,7 +107,7 @@ ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005,
 # the learned correction at matched accuracy: trained and evaluated at each of
 # these opening angles (its training pairs are the near cells the walk at that
 # angle accepts)
-CORRECTED_THETAS = (0.7, 0.75, 0.8, 0.9)
+CORRECTED_THETAS = (0.6, 0.65, 0.7, 0.75, 0.8)
 OPENINGS = {"reference": 0, "offset": 1}
 N_TARGETS = 4096  # seeded targets of the FP64 direct-sum oracle
 # energy drift needs the O(N^2) FP64 potential: measured directly up to

@@ -700,15 +700,41 @@ __global__ void scan_reduce_kernel(Tree t) {
   if (threadIdx.x == 0) t.block_sums[blockIdx.x] = sh[0];
 }
 
-__global__ void scan_blocks_kernel(Tree t, int blocks) {
-  if (threadIdx.x != 0) return;
-  uint32_t run = 0;
-  for (int b = 0; b < blocks; ++b) {
-    const uint32_t c = t.block_sums[b];
-    t.block_sums[b] = run;
-    run += c;
+// Exclusive scan of the block sums in place (one block of 1024 threads, in
+// chunks of 1024), total into offset[n].
+__global__ void __launch_bounds__(1024) scan_blocks_kernel(Tree t, int blocks) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < blocks; base += 1024) {
+    const int b = base + threadIdx.x;
+    const uint32_t v = b < blocks ? t.block_sums[b] : 0u;
+    uint32_t x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t u = __shfl_up_sync(kFull, x, off);
+      if (lane >= off) x += u;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t w = warp_sums[lane];
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFull, w, off);
+        if (lane >= off) w += u;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t incl = x + (wid > 0 ? warp_sums[wid - 1] : 0u);
+    const uint32_t c = carry;
+    if (b < blocks) t.block_sums[b] = c + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = c + incl;
+    __syncthreads();
   }
-  t.offset[t.n] = run;
+  if (threadIdx.x == 0) t.offset[t.n] = carry;
 }
 
 __global__ void scan_apply_kernel(Tree t) {
@@ -2255,7 +2281,7 @@ void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree
   NBSP_COUNT_LAUNCH(1), keep_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
   const int blocks = (int)((n + kScanItems - 1) / kScanItems);
   NBSP_COUNT_LAUNCH(1), scan_reduce_kernel<<<blocks, 256, 0, stream>>>(t);
-  NBSP_COUNT_LAUNCH(1), scan_blocks_kernel<<<1, 32, 0, stream>>>(t, blocks);
+  NBSP_COUNT_LAUNCH(1), scan_blocks_kernel<<<1, 1024, 0, stream>>>(t, blocks);
   NBSP_COUNT_LAUNCH(1), scan_apply_kernel<<<blocks, 256, 0, stream>>>(t);
   NBSP_COUNT_LAUNCH(1), place_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
 }
