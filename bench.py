@@ -443,14 +443,16 @@ def timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction=No
     ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
     for _ in range(warmup):
         ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
-    ms = []
+    ms, walk = [], []
     for _ in range(steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         ctx.advance(g, wl["dt"], 1, nb.Algorithm.BARNES_HUT)
-        ms.append(ctx.timings()["total_ms"])
+        t = ctx.timings()
+        ms.append(t["total_ms"])
+        walk.append(t["walk_ms"])
     ctx.close()
-    return wl["n"] * steps / (sum(ms) * 1e-3), float(np.mean(ms))
+    return wl["n"] * steps / (sum(ms) * 1e-3), float(np.mean(ms)), float(np.mean(walk))
 
 
 def energy_drift(nb, system, g, wl, m, steps, correction=None):
@@ -539,8 +541,9 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
             candidates.append((method(f"relative_leaf{leaf}", 1.0, alpha=b[0], leaf=leaf), b[1]))
 
     def timed(m, r, correction=None):
-        v, ms = timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction)
-        return dict(m, rms=r[0], max_rel=r[1], value=v, ms_per_step=round(ms, 4))
+        v, ms, walk = timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction)
+        return dict(m, rms=r[0], max_rel=r[1], value=v, ms_per_step=round(ms, 4),
+                    walk_ms=round(walk, 4))
 
     methods = [timed(m, r) for m, r in candidates]
     out = {"rms_target": RMS_TARGET,
@@ -569,6 +572,12 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
             cctx.close()
             rec = timed(m, r, corr)
             rec["uncorrected_rms_at_theta_1.0"] = dict(sweep[f"order1_{oname}"])[1.0][0]
+            # the same walk without the network: what the correction costs
+            plain1 = method(f"plain_{oname}_theta_1.0", 1.0, opening=oname)
+            _, ms1, walk1 = timed_steps(nb, torch, system, g, wl, plain1, steps, warmup, flush)
+            rec["uncorrected_ms_per_step"] = round(ms1, 4)
+            rec["uncorrected_walk_ms"] = round(walk1, 4)
+            rec["walk_over_uncorrected_walk"] = round(rec["walk_ms"] / walk1, 3)
             rec["network"] = {"evaluations_per_walk": evals, "flop_per_evaluation": MLP_FLOPS,
                               "walk_ms_with_network": round(walk_ms, 4),
                               "tensor_tflops_in_walk": round(evals * MLP_FLOPS / (walk_ms * 1e-3)

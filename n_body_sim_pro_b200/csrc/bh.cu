@@ -2047,13 +2047,16 @@ __global__ void __launch_bounds__(1024) corr_scan_kernel(NbspCorrectionLists lis
   }
 }
 
-// Row r -> its group, one warp per group (the rows kernel then needs no search).
+// Row r -> (its group, its cell), one warp per group: the rows kernel reads
+// both with one 8-byte load and needs no search.
 __global__ void __launch_bounds__(128) corr_rowmap_kernel(NbspCorrectionLists lists, int groups) {
   const int lane = threadIdx.x & 31;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (g >= groups) return;
   const int cnt = lists.count[g], off = lists.offset[g];
-  for (int k = lane; k < cnt; k += 32) lists.group[off + k] = g;
+  int2* rows = reinterpret_cast<int2*>(lists.row);
+  for (int k = lane; k < cnt; k += 32)
+    rows[off + k] = make_int2(g, lists.cells[(size_t)g * lists.capacity + k]);
 }
 
 __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
@@ -2072,9 +2075,9 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
     float v[nbsp_mlp::kIn];
     bool ok = false;
     if (r < rows) {
-      const int grp = lists.group[r];
-      const int node = lists.cells[(size_t)grp * lists.capacity + (r - lists.offset[grp])];
-      const float4 g = centre[grp];
+      const int2 gn = reinterpret_cast<const int2*>(lists.row)[r];
+      const int node = gn.y;
+      const float4 g = centre[gn.x];
       float f[nbsp_mlp::kIn];
       ok = cell_features(t, node, t.com[node], g.x, g.y, g.z, f);
 #pragma unroll
@@ -2332,8 +2335,8 @@ void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* c
       *lists, groups);
   const int smem = (int)sizeof(nbsp_umma::Smem);
   cudaFuncSetAttribute(corr_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  // persistent: four 49-KB CTAs per SM, each holding 128 of the 512 TMEM columns
-  NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * 4, nbsp_umma::kThreads, smem, stream>>>(
+  // persistent: kCtasPerSm CTAs per SM, each holding 64 of the 512 TMEM columns
+  NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * nbsp_umma::kCtasPerSm, nbsp_umma::kThreads, smem, stream>>>(
       net, t, *lists, groups, status);
   NBSP_COUNT_LAUNCH(1), corr_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
       (const float4*)pos4, (int)n, t, *lists, (double4*)acc);

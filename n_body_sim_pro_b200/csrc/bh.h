@@ -150,7 +150,7 @@ typedef struct NbspCorrectionLists {
     int* offset;    /* [groups + 1] exclusive prefix of count */
     float* centre;  /* [groups * 4] group centre x, y, z and group radius^2 */
     float* y;       /* [groups * capacity * 3] network outputs per row */
-    int* group;     /* [groups * capacity] the group of each row */
+    int* row;       /* [groups * capacity * 2] (group, cell) of each row */
     int capacity;   /* cells per group; more are left to the plain monopole and counted */
 } NbspCorrectionLists;
 

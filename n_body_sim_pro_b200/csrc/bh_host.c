@@ -75,7 +75,7 @@ static void release_lists(NbspBarnesHut* b) {
     cudaFree(b->lists.offset);
     cudaFree(b->lists.centre);
     cudaFree(b->lists.y);
-    cudaFree(b->lists.group);
+    cudaFree(b->lists.row);
     memset(&b->lists, 0, sizeof(b->lists));
     b->lists_groups = 0;
 }
@@ -90,7 +90,7 @@ static NBodySimProStatus ensure_lists(NbspBarnesHut* b, size_t n, NBodySimProErr
     BH_TRY(cudaMalloc((void**)&b->lists.offset, (groups + 1) * sizeof(int)));
     BH_TRY(cudaMalloc((void**)&b->lists.centre, groups * 4 * sizeof(float)));
     BH_TRY(cudaMalloc((void**)&b->lists.y, groups * cap * 3 * sizeof(float)));
-    BH_TRY(cudaMalloc((void**)&b->lists.group, groups * cap * sizeof(int)));
+    BH_TRY(cudaMalloc((void**)&b->lists.row, groups * cap * 2 * sizeof(int)));
     b->lists.capacity = (int)cap;
     b->lists_groups = groups;
     return N_BODY_SIM_PRO_STATUS_OK;

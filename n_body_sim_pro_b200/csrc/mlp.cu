@@ -484,7 +484,8 @@ void nbsp_mlp_evaluate(const void* net, const float* feat, int rows, float* out,
     const int smem = (int)sizeof(nbsp_umma::Smem);
     cudaFuncSetAttribute(evaluate_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int tiles = (rows + nbsp_umma::kRows - 1) / nbsp_umma::kRows;
-    const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
+    const int cap = 148 * nbsp_umma::kCtasPerSm;
+    const int grid = tiles < cap ? tiles : cap;
     NBSP_COUNT_LAUNCH(1), evaluate_umma_kernel<<<grid, nbsp_umma::kThreads, smem, stream>>>(
         (const Net*)net, feat, rows, out, status);
   } else {

