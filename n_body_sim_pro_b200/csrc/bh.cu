@@ -362,18 +362,18 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(
   }
   gofs[t] = base[t] + prefix;
   __syncthreads();
-  {  // exclusive scan of the tile's digit totals
-    const uint32_t own = start[t];
-    uint32_t v = own;
-    for (int off = 1; off < kRadix; off <<= 1) {
-      __syncthreads();
-      const uint32_t add = t >= off ? start[t - off] : 0u;
-      __syncthreads();
-      v += add;
-      start[t] = v;
+  {  // exclusive scan of the tile's digit totals: warp shuffles, then the warp sums
+    __shared__ uint32_t s_wsum[kSortWarps];
+    uint32_t v = count;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t u = __shfl_up_sync(kFull, v, off);
+      if (lane >= off) v += u;
     }
+    if (lane == 31) s_wsum[w] = v;
     __syncthreads();
-    start[t] = v - own;
+    uint32_t before = 0;
+    for (int k = 0; k < w; ++k) before += s_wsum[k];
+    start[t] = before + v - count;
   }
   __syncthreads();
 #pragma unroll
@@ -903,50 +903,82 @@ __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
 // writes the sorted list back for the interaction-list walk.
 // QUAD: also the trace-free quadrupoles and the spread (the quadrupole walk,
 // the correction's features); the monopole walk reads neither.
+// Sum over the kTeam lanes of a team (lanes 8k .. 8k+7 of a warp), the same
+// pairing order on every run (deterministic).
+constexpr int kTeam = 8;
+__device__ __forceinline__ double team_sum(double v) {
+#pragma unroll
+  for (int off = 1; off < kTeam; off <<= 1) v += __shfl_xor_sync(kFull, v, off);
+  return v;
+}
+
+// Leaves: a team of 8 lanes per leaf (lane k sums particles k, k + 8, ...,
+// then the team reduces by shuffles); the team's first lane finishes the leaf
+// and climbs: the last child to arrive at a parent combines the children.
 template <bool QUAD>
 __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
                                                       Opening open, int* status) {
   const int total = (int)t.offset[t.n];
-  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < total;
-       node += gridDim.x * blockDim.x) {
-    const int4 info = t.info[node];
-    if (info.z == 0) continue;  // internal nodes are finished by their last child
-    if (info.z < 0 || info.y < 0 || info.y + info.z > t.n) {
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-      continue;
+  const int sub = threadIdx.x & (kTeam - 1);
+  const int teams = gridDim.x * (blockDim.x / kTeam);
+  // every lane of a warp runs the same number of iterations (team shuffles)
+  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / kTeam;
+  const int warp_first = first & ~(32 / kTeam - 1);
+  for (int base = warp_first; base < total; base += teams) {
+    const int node = base + (first - warp_first);
+    int4 info = make_int4(0, 0, 0, 0);
+    bool leaf = false;
+    if (node < total) {
+      info = t.info[node];
+      leaf = info.z != 0;  // internal nodes are finished by their last child
+      if (leaf && (info.z < 0 || info.y < 0 || info.y + info.z > t.n)) {
+        if (sub == 0) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        leaf = false;
+      }
     }
+    const int count = leaf ? info.z : 0;
     Moments mo;
     {
       double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-#pragma unroll 4
-      for (int j = info.y; j < info.y + info.z; ++j) {
+      for (int j = info.y + sub; j < info.y + count; j += kTeam) {
         const float4 p = pos[j];
         m += (double)p.w;
         sx += (double)p.w * (double)p.x;
         sy += (double)p.w * (double)p.y;
         sz += (double)p.w * (double)p.z;
       }
+      m = team_sum(m);
+      sx = team_sum(sx);
+      sy = team_sum(sy);
+      sz = team_sum(sz);
+      float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (leaf && m == 0.0) p0 = pos[info.y];
       mo.m = m;
-      mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
-      mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
-      mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
+      mo.cx = m != 0.0 ? sx / m : (double)p0.x;
+      mo.cy = m != 0.0 ? sy / m : (double)p0.y;
+      mo.cz = m != 0.0 ? sz / m : (double)p0.z;
       for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
       mo.t2 = 0.0;
-#pragma unroll 4
-      for (int j = info.y; QUAD && j < info.y + info.z; ++j) {
-        const float4 p = pos[j];
-        const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        const double w = (double)p.w;
-        mo.t2 += w * r2;
-        mo.q[0] += w * (3.0 * dx * dx - r2);
-        mo.q[1] += w * (3.0 * dx * dy);
-        mo.q[2] += w * (3.0 * dx * dz);
-        mo.q[3] += w * (3.0 * dy * dy - r2);
-        mo.q[4] += w * (3.0 * dy * dz);
-        mo.q[5] += w * (3.0 * dz * dz - r2);
+      if (QUAD) {
+        for (int j = info.y + sub; j < info.y + count; j += kTeam) {
+          const float4 p = pos[j];
+          const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy,
+                       dz = (double)p.z - mo.cz;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const double w = (double)p.w;
+          mo.t2 += w * r2;
+          mo.q[0] += w * (3.0 * dx * dx - r2);
+          mo.q[1] += w * (3.0 * dx * dy);
+          mo.q[2] += w * (3.0 * dx * dz);
+          mo.q[3] += w * (3.0 * dy * dy - r2);
+          mo.q[4] += w * (3.0 * dy * dz);
+          mo.q[5] += w * (3.0 * dz * dz - r2);
+        }
+        mo.t2 = team_sum(mo.t2);
+        for (int k = 0; k < 6; ++k) mo.q[k] = team_sum(mo.q[k]);
       }
     }
+    if (!leaf || sub != 0) continue;
     finish_node<QUAD>(t, node, mo, info.y, t.level[node], open);
     int parent = info.w;
     for (int climb = 0; parent >= 0; ++climb) {
@@ -1418,9 +1450,9 @@ __device__ __forceinline__ void source_tile(const SourceTile& s, float4 p, float
 //   f4..8 = trace-free Q / (M side^2): xx, xy, xz, yy, yz
 //   f9    = sum m |x - com|^2 / (M side^2)
 // false for a massless cell.
-__device__ __forceinline__ bool cell_features(const Tree& t, int node, float4 c, float tx,
-                                              float ty, float tz, float* f) {
-  const float s = t.side[node];
+__device__ __forceinline__ bool features_of(float4 c, float s, float4 qa, float qyz,
+                                            float spread, float tx, float ty, float tz,
+                                            float* f) {
   if (!(c.w > 0.f) || !(s > 0.f)) return false;
   const float rx = tx - c.x, ry = ty - c.y, rz = tz - c.z;
   const float inv_s = 1.f / s;
@@ -1430,16 +1462,20 @@ __device__ __forceinline__ bool cell_features(const Tree& t, int node, float4 c,
   f[1] = ry * inv_s;
   f[2] = rz * inv_s;
   f[3] = s / d;
-  const float4 qa = t.quad[2 * node];
-  const float qyz = t.quad[2 * node + 1].x;
   const float qs = 1.f / (c.w * s * s);
   f[4] = qa.x * qs;
   f[5] = qa.y * qs;
   f[6] = qa.z * qs;
   f[7] = qa.w * qs;
   f[8] = qyz * qs;
-  f[9] = t.spread[node];
+  f[9] = spread;
   return true;
+}
+
+__device__ __forceinline__ bool cell_features(const Tree& t, int node, float4 c, float tx,
+                                              float ty, float tz, float* f) {
+  return features_of(c, t.side[node], t.quad[2 * node], t.quad[2 * node + 1].x, t.spread[node],
+                     tx, ty, tz, f);
 }
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
@@ -2059,6 +2095,30 @@ __global__ void __launch_bounds__(128) corr_rowmap_kernel(NbspCorrectionLists li
     rows[off + k] = make_int2(g, lists.cells[(size_t)g * lists.capacity + k]);
 }
 
+// What the features of one row are computed from, loaded one tile ahead so the
+// loads are in flight while the tensor cores run the current tile.
+struct RowData {
+  float4 c;    // cell centre of mass, mass
+  float4 g;    // group centre, radius^2
+  float4 qa;   // quadrupole xx, xy, xz, yy
+  float qyz, side, spread;
+  bool valid;
+};
+
+__device__ __forceinline__ RowData load_row(const Tree& t, const float4* centre, int2 gn,
+                                            bool valid) {
+  RowData d;
+  d.valid = valid;
+  const int node = valid ? gn.y : 0, grp = valid ? gn.x : 0;
+  d.c = t.com[node];
+  d.g = centre[grp];
+  d.qa = t.quad[2 * node];
+  d.qyz = t.quad[2 * node + 1].x;
+  d.side = t.side[node];
+  d.spread = t.spread[node];
+  return d;
+}
+
 __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
     const nbsp_mlp::Net* __restrict__ net, Tree t, NbspCorrectionLists lists, int groups,
     int* status) {
@@ -2070,16 +2130,19 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
   const int rows = lists.offset[groups];
   const int tiles = (rows + nbsp_umma::kRows - 1) / nbsp_umma::kRows;
   const float4* centre = reinterpret_cast<const float4*>(lists.centre);
-  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int r = tile * nbsp_umma::kRows + threadIdx.x;
+  const int2* rowmap = reinterpret_cast<const int2*>(lists.row);
+  const int stride = gridDim.x * nbsp_umma::kRows;
+  // pipeline: the row map two tiles ahead, the row data one tile ahead
+  int r = blockIdx.x * nbsp_umma::kRows + threadIdx.x;
+  RowData cur = load_row(t, centre, r < rows ? rowmap[r] : make_int2(0, 0), r < rows);
+  int2 ahead = r + stride < rows ? rowmap[r + stride] : make_int2(0, 0);
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, r += stride) {
     float v[nbsp_mlp::kIn];
     bool ok = false;
-    if (r < rows) {
-      const int2 gn = reinterpret_cast<const int2*>(lists.row)[r];
-      const int node = gn.y;
-      const float4 g = centre[gn.x];
+    if (cur.valid) {
       float f[nbsp_mlp::kIn];
-      ok = cell_features(t, node, t.com[node], g.x, g.y, g.z, f);
+      ok = features_of(cur.c, cur.side, cur.qa, cur.qyz, cur.spread, cur.g.x, cur.g.y, cur.g.z,
+                       f);
 #pragma unroll
       for (int q = 0; q < nbsp_mlp::kIn; ++q) {
         ok = ok && f[q] >= net->x_min[q] && f[q] <= net->x_max[q];
@@ -2092,6 +2155,8 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
     nbsp_umma::put_inputs(sm, v);
     nbsp_umma::fence_async_smem();
     __syncthreads();
+    const RowData next = load_row(t, centre, ahead, r + stride < rows);
+    ahead = r + 2 * stride < rows ? rowmap[r + 2 * stride] : make_int2(0, 0);
     float y[3];
     if (!nbsp_umma::forward(sm, tmem, phase, y)) {
       if (threadIdx.x == 0) atomicOr(status, NBSP_DEVICE_ERROR_MMA_TIMEOUT);
@@ -2101,6 +2166,7 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
 #pragma unroll
       for (int c = 0; c < 3; ++c)
         lists.y[(size_t)r * 3 + c] = ok ? fmaf(y[c], net->y_std[c], net->y_mean[c]) : 0.f;
+    cur = next;
   }
   nbsp_umma::teardown(sm, tmem);
 }
