@@ -903,82 +903,50 @@ __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
 // writes the sorted list back for the interaction-list walk.
 // QUAD: also the trace-free quadrupoles and the spread (the quadrupole walk,
 // the correction's features); the monopole walk reads neither.
-// Sum over the kTeam lanes of a team (lanes 8k .. 8k+7 of a warp), the same
-// pairing order on every run (deterministic).
-constexpr int kTeam = 8;
-__device__ __forceinline__ double team_sum(double v) {
-#pragma unroll
-  for (int off = 1; off < kTeam; off <<= 1) v += __shfl_xor_sync(kFull, v, off);
-  return v;
-}
-
-// Leaves: a team of 8 lanes per leaf (lane k sums particles k, k + 8, ...,
-// then the team reduces by shuffles); the team's first lane finishes the leaf
-// and climbs: the last child to arrive at a parent combines the children.
 template <bool QUAD>
 __global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
                                                       Opening open, int* status) {
   const int total = (int)t.offset[t.n];
-  const int sub = threadIdx.x & (kTeam - 1);
-  const int teams = gridDim.x * (blockDim.x / kTeam);
-  // every lane of a warp runs the same number of iterations (team shuffles)
-  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / kTeam;
-  const int warp_first = first & ~(32 / kTeam - 1);
-  for (int base = warp_first; base < total; base += teams) {
-    const int node = base + (first - warp_first);
-    int4 info = make_int4(0, 0, 0, 0);
-    bool leaf = false;
-    if (node < total) {
-      info = t.info[node];
-      leaf = info.z != 0;  // internal nodes are finished by their last child
-      if (leaf && (info.z < 0 || info.y < 0 || info.y + info.z > t.n)) {
-        if (sub == 0) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-        leaf = false;
-      }
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < total;
+       node += gridDim.x * blockDim.x) {
+    const int4 info = t.info[node];
+    if (info.z == 0) continue;  // internal nodes are finished by their last child
+    if (info.z < 0 || info.y < 0 || info.y + info.z > t.n) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      continue;
     }
-    const int count = leaf ? info.z : 0;
     Moments mo;
     {
       double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-      for (int j = info.y + sub; j < info.y + count; j += kTeam) {
+#pragma unroll 4
+      for (int j = info.y; j < info.y + info.z; ++j) {
         const float4 p = pos[j];
         m += (double)p.w;
         sx += (double)p.w * (double)p.x;
         sy += (double)p.w * (double)p.y;
         sz += (double)p.w * (double)p.z;
       }
-      m = team_sum(m);
-      sx = team_sum(sx);
-      sy = team_sum(sy);
-      sz = team_sum(sz);
-      float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (leaf && m == 0.0) p0 = pos[info.y];
       mo.m = m;
-      mo.cx = m != 0.0 ? sx / m : (double)p0.x;
-      mo.cy = m != 0.0 ? sy / m : (double)p0.y;
-      mo.cz = m != 0.0 ? sz / m : (double)p0.z;
+      mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
+      mo.cy = m != 0.0 ? sy / m : (double)pos[info.y].y;
+      mo.cz = m != 0.0 ? sz / m : (double)pos[info.y].z;
       for (int k = 0; k < 6; ++k) mo.q[k] = 0.0;
       mo.t2 = 0.0;
-      if (QUAD) {
-        for (int j = info.y + sub; j < info.y + count; j += kTeam) {
-          const float4 p = pos[j];
-          const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy,
-                       dz = (double)p.z - mo.cz;
-          const double r2 = dx * dx + dy * dy + dz * dz;
-          const double w = (double)p.w;
-          mo.t2 += w * r2;
-          mo.q[0] += w * (3.0 * dx * dx - r2);
-          mo.q[1] += w * (3.0 * dx * dy);
-          mo.q[2] += w * (3.0 * dx * dz);
-          mo.q[3] += w * (3.0 * dy * dy - r2);
-          mo.q[4] += w * (3.0 * dy * dz);
-          mo.q[5] += w * (3.0 * dz * dz - r2);
-        }
-        mo.t2 = team_sum(mo.t2);
-        for (int k = 0; k < 6; ++k) mo.q[k] = team_sum(mo.q[k]);
+#pragma unroll 4
+      for (int j = info.y; QUAD && j < info.y + info.z; ++j) {
+        const float4 p = pos[j];
+        const double dx = (double)p.x - mo.cx, dy = (double)p.y - mo.cy, dz = (double)p.z - mo.cz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double w = (double)p.w;
+        mo.t2 += w * r2;
+        mo.q[0] += w * (3.0 * dx * dx - r2);
+        mo.q[1] += w * (3.0 * dx * dy);
+        mo.q[2] += w * (3.0 * dx * dz);
+        mo.q[3] += w * (3.0 * dy * dy - r2);
+        mo.q[4] += w * (3.0 * dy * dz);
+        mo.q[5] += w * (3.0 * dz * dz - r2);
       }
     }
-    if (!leaf || sub != 0) continue;
     finish_node<QUAD>(t, node, mo, info.y, t.level[node], open);
     int parent = info.w;
     for (int climb = 0; parent >= 0; ++climb) {
