@@ -110,6 +110,8 @@ ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005,
 CORRECTED_THETAS = (0.6, 0.65, 0.7, 0.75, 0.8)
 OPENINGS = {"reference": 0, "offset": 1}
 N_TARGETS = 4096  # seeded targets of the FP64 direct-sum oracle
+# NBodySimProCudaWalk; "default" keeps the context's own
+WALK_MODES = {"stackless": 0, "lists": 1, "shared": 2, "default": -1}
 # energy drift needs the O(N^2) FP64 potential: measured directly up to
 # DRIFT_MAX_N particles, on the DRIFT_N-particle twin of the workload above
 DRIFT_MAX_N = 2_000_000
@@ -665,7 +667,8 @@ def run_bh(args, wl, world, rank, local, steps, warmup, with_e2e=True):
                    alpha=wl.get("alpha", 0.0), leaf=wl.get("leaf", 16))
     correction = corrections.get(m.get("correction")) if m["corrected"] else None
     ctx = make_context(nb, m, correction)
-    ctx.set_walk(0 if wl.get("walk") == "stackless" else 1)
+    if WALK_MODES[wl.get("walk", "default")] >= 0:
+        ctx.set_walk(WALK_MODES[wl["walk"]])
     ctx.upload(system)
     ctx.compute_acceleration(g, nb.Algorithm.BARNES_HUT)
     q0, pe0 = ctx.diagnostics(g, potential=True) if n <= 2_000_000 else (None, None)
@@ -1266,7 +1269,7 @@ def main(argv=None):
                     help="skip the sub-records of the other configurations")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--order", type=int, default=None, choices=[1, 2])
-    ap.add_argument("--walk", default=None, choices=["lists", "stackless"])
+    ap.add_argument("--walk", default=None, choices=["lists", "stackless", "shared"])
     ap.add_argument("--leaf", type=int, default=None)
     ap.add_argument("--alpha", type=float, default=None,
                     help="relative opening test tolerance (with --no-matched)")

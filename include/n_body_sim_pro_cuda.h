@@ -230,18 +230,24 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_multip
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_capacity(
     NBodySimProCudaContext* context, int capacity, NBodySimProError* error);
 
-/* Barnes-Hut walk.  Both accept a cell only when the reference's test
+/* Barnes-Hut walk.  All accept a cell only when the reference's test
  * (2h)^2 < theta^2 d^2 holds for every one of the 32 Morton-consecutive
- * targets it is applied to (src/c/barnes_hut/barnes_hut.c:596-599), so both
+ * targets it is applied to (src/c/barnes_hut/barnes_hut.c:596-599), so all
  * accept the same cells; they differ in how the traversal is scheduled:
  *   STACKLESS          one node at a time per warp along depth-first skip
  *                      links;
  *   INTERACTION_LISTS  (default) 32 nodes per step tested in parallel from a
  *                      per-warp stack, accepted cells and leaves gathered and
- *                      evaluated in dense loops. */
+ *                      evaluated in dense loops;
+ *   SHARED_TOP         INTERACTION_LISTS with the top of the tree traversed
+ *                      once per block of 4 groups: nodes every group accepts
+ *                      or opens are decided once, the rest by each group
+ *                      (monopole walk; the others fall back to
+ *                      INTERACTION_LISTS). */
 typedef enum NBodySimProCudaWalk {
     N_BODY_SIM_PRO_CUDA_WALK_STACKLESS = 0,
-    N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS = 1
+    N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS = 1,
+    N_BODY_SIM_PRO_CUDA_WALK_SHARED_TOP = 2
 } NBodySimProCudaWalk;
 
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(

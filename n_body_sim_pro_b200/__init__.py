@@ -442,7 +442,8 @@ class CudaContext:
                                                                          C.byref(err)), err)
 
     def set_walk(self, walk: int) -> None:
-        """0: stackless skip-link walk; 1: interaction-list walk (default)."""
+        """0: stackless skip-link walk; 1: interaction-list walk (default); 2: the
+        interaction-list walk with the top of the tree shared by 4 groups."""
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_walk(self.handle, int(walk),
                                                               C.byref(err)), err)

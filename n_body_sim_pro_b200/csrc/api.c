@@ -234,10 +234,12 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_leaf_capacity(NBodySimProCudaC
 NBodySimProStatus n_body_sim_pro_cuda_context_set_walk(NBodySimProCudaContext* c, int walk,
                                                        NBodySimProError* error) {
     if (c == NULL || (walk != N_BODY_SIM_PRO_CUDA_WALK_STACKLESS &&
-                      walk != N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS))
+                      walk != N_BODY_SIM_PRO_CUDA_WALK_INTERACTION_LISTS &&
+                      walk != N_BODY_SIM_PRO_CUDA_WALK_SHARED_TOP))
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown Barnes-Hut walk");
-    c->walk_mode = walk == N_BODY_SIM_PRO_CUDA_WALK_STACKLESS ? NBSP_BH_WALK_STACKLESS
-                                                              : NBSP_BH_WALK_LISTS;
+    c->walk_mode = walk == N_BODY_SIM_PRO_CUDA_WALK_STACKLESS   ? NBSP_BH_WALK_STACKLESS
+                   : walk == N_BODY_SIM_PRO_CUDA_WALK_SHARED_TOP ? NBSP_BH_WALK_SHARED
+                                                                 : NBSP_BH_WALK_LISTS;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 

@@ -1684,6 +1684,11 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
+// SHARED walk: the block's top-of-tree traversal keeps its stack and frontier
+// in the warps' stack space (it ends before any warp walks)
+constexpr int kCtaStack = 2048;    // warps 0 and 1's stacks
+constexpr int kFrontier = 384;     // the start of warp 2's stack
+static_assert(kCtaStack + kFrontier <= 3 * kListStack, "frontier inside warp 2's stack");
 
 // Interaction-list walk.  The 32 Morton-consecutive targets of a warp share a
 // traversal.  Each step the lanes pop up to 32 nodes from the warp's
@@ -1713,11 +1718,23 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // monopole, exactly as without the correction.
 // Register budgets: monopole walk 64 (8 blocks of 4 warps per SM), quadrupole
 // walk 102 (5 blocks).
-template <int ORDER, int STACK, bool CORR, bool REL>
+//
+// SHARED: the top of the tree is traversed once for the block's 4 groups.  The
+// 128 threads test up to 128 nodes at a time against the 4 group boxes: a node
+// every group's box test accepts is staged once for all four (into every
+// warp's source tile); an internal node whose opening test fails for every
+// target of every group (the box's farthest point fails) is opened once for
+// all; any other node goes to a frontier that each warp then walks on its own
+// exactly as above.  Every group accepts, opens and sums exactly the nodes it
+// would alone (the same interactions; only the order of the FP32 sums moves).
+// A block whose shared stack or frontier would overflow starts every group
+// from the root instead.
+template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED = false>
 __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
     double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net, NbspCorrectionLists lists) {
+  static_assert(!SHARED || (ORDER == 1 && !CORR && STACK == kListStack), "shared top: monopole walk");
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ float s_probe_k[kListThreads / 32][REL ? 32 : 1];  // their M side^2
   __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
@@ -1734,7 +1751,8 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
   int listed = 0;   // corrected walk: cells listed for the network (warp-uniform)
   int qstaged = 0;  // cells waiting in the QuadTile (ORDER 2)
   const int warp = (blockIdx.x * kListThreads + threadIdx.x) >> 5;
-  if (warp * 32 >= n) return;
+  const bool live = warp * 32 < n;  // (a SHARED block's idle warps join its shared phase)
+  if (!SHARED && !live) return;
   int* stack = s_stack[wib];
   int2* leaves = s_leaves[wib];
   const int s = warp * 32 + lane;
@@ -1768,9 +1786,170 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
   unsigned approx = 0, exact = 0;
   int top = 1, nleaf = 0, iters = 0;
   bool overflow = false;
-  if (lane == 0) stack[0] = 0;
+  if (SHARED) {
+    constexpr int kGroups = kListThreads / 32;
+    __shared__ float s_box[kGroups][8];  // centre, half extents, least and most tolerant
+    __shared__ int s_live[kGroups];
+    __shared__ int s_sum[kGroups][3];    // per warp: accepted, children, frontier nodes
+    __shared__ int s_ctop, s_nfront, s_abort;
+    int* cstack = &s_stack[0][0];
+    int* front = &s_stack[0][0] + kCtaStack;
+    float tmax = REL && active ? tl : -INFINITY;
+    if (REL)
+      for (int off = 16; off > 0; off >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(kFull, tmax, off));
+    if (lane == 0) {
+      s_box[wib][0] = gx;
+      s_box[wib][1] = gy;
+      s_box[wib][2] = gz;
+      s_box[wib][3] = ex;
+      s_box[wib][4] = ey;
+      s_box[wib][5] = ez;
+      s_box[wib][6] = tmin;
+      s_box[wib][7] = tmax;
+      s_live[wib] = live;
+    }
+    if (threadIdx.x == 0) {
+      s_ctop = 1;
+      cstack[0] = 0;
+      s_nfront = 0;
+      s_abort = 0;
+    }
+    __syncthreads();
+    for (int csteps = 0;; ++csteps) {
+      const int ctop = s_ctop;  // block-uniform: read after a barrier
+      if (ctop == 0 || s_abort) break;
+      if (csteps > total + 64) {  // every node is popped at most once
+        if (threadIdx.x == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
+        break;
+      }
+      const int take = min(kListThreads, ctop);
+      int node = (int)threadIdx.x < take ? cstack[ctop - 1 - threadIdx.x] : -1;
+      if (node >= total) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        node = -1;
+      }
+      const bool valid = node >= 0;
+      const int at = valid ? node : 0;
+      const int4 info = t.info[at];
+      const float4 c = t.com[at];
+      const float ro = t.ropen2[at];
+      const float km = REL ? t.kmass[at] : 0.f;
+      const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
+      if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      const bool ok = valid && !bad;
+      bool all_accept = ok && info.z != 1, all_open = ok && info.z == 0;
+#pragma unroll
+      for (int w = 0; w < kGroups; ++w) {
+        if (!s_live[w]) continue;
+        const float ax = fabsf(c.x - s_box[w][0]), ay = fabsf(c.y - s_box[w][1]),
+                    az = fabsf(c.z - s_box[w][2]);
+        const float qx = fmaxf(ax - s_box[w][3], 0.f), qy = fmaxf(ay - s_box[w][4], 0.f),
+                    qz = fmaxf(az - s_box[w][5], 0.f);
+        const float fx = ax + s_box[w][3], fy = ay + s_box[w][4], fz = az + s_box[w][5];
+        const float dmin2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+        const float dmax2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+        all_accept = all_accept && opening_passes<REL>(dmin2, ro, km, s_box[w][6]);
+        all_open = all_open && (dmax2 <= ro || (REL && dmax2 * dmax2 * s_box[w][7] < km));
+      }
+      const bool to_front = ok && !all_accept && !all_open;
+      int4 ca = make_int4(-1, -1, -1, -1), cb = make_int4(-1, -1, -1, -1);
+      if (all_open) {
+        ca = reinterpret_cast<const int4*>(t.children)[2 * node];
+        cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
+      }
+      const int kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) +
+                       (cb.y >= 0) + (cb.z >= 0) + (cb.w >= 0);
+      // block-wide exclusive prefixes of the three counts
+      int ia = all_accept, ik = kids, ifr = to_front;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int ua = __shfl_up_sync(kFull, ia, off), uk = __shfl_up_sync(kFull, ik, off),
+                  uf = __shfl_up_sync(kFull, ifr, off);
+        if (lane >= off) {
+          ia += ua;
+          ik += uk;
+          ifr += uf;
+        }
+      }
+      if (lane == 31) {
+        s_sum[wib][0] = ia;
+        s_sum[wib][1] = ik;
+        s_sum[wib][2] = ifr;
+      }
+      __syncthreads();  // (every entry popped above has been read)
+      int ba = 0, bk = 0, bf = 0, na = 0, nk = 0, nf = 0;
+#pragma unroll
+      for (int w = 0; w < kGroups; ++w) {
+        if (w < wib) {
+          ba += s_sum[w][0];
+          bk += s_sum[w][1];
+          bf += s_sum[w][2];
+        }
+        na += s_sum[w][0];
+        nk += s_sum[w][1];
+        nf += s_sum[w][2];
+      }
+      const int ra = ba + ia - (int)all_accept, rk = bk + ik - kids, rf = bf + ifr - (int)to_front;
+      const int cbase = ctop - take, front0 = s_nfront;
+      const bool abort = cbase + nk > kCtaStack || front0 + nf > kFrontier;  // block-uniform
+      if (!abort) {
+        const int kid[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (k < kids) cstack[cbase + rk + k] = kid[k];
+        if (to_front) front[front0 + rf] = node;
+        // cells every group accepts: into every live warp's source tile, in
+        // rounds of what fits before the tiles are evaluated
+        approx += active ? (unsigned)na : 0u;
+        for (int done = 0; done < na;) {
+          const int put = min(kStage - staged, na - done);
+          const int r = ra - done;
+          if (all_accept && r >= 0 && r < put)
+#pragma unroll
+            for (int w = 0; w < kGroups; ++w)
+              if (s_live[w]) stage_source(s_src[w], staged + r, c);
+          staged += put;
+          done += put;
+          __syncthreads();
+          if (staged == kStage) {
+            if (live) source_tile(src, p, eps2, guard, hx, hy, hz, lx, ly, lz);
+            staged = 0;
+            __syncthreads();
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        if (abort) {
+          s_abort = 1;
+        } else {
+          s_ctop = cbase + nk;
+          s_nfront = front0 + nf;
+        }
+      }
+      __syncthreads();
+    }
+    const int nfront = s_nfront;
+    const bool restart = s_abort != 0;
+    __syncthreads();  // the shared stack's last reads
+    if (restart) {  // start every group from the root, discarding the shared phase
+      hx = hy = hz = lx = ly = lz = 0.f;
+      approx = 0;
+      staged = 0;
+      top = 1;
+      if (lane == 0) stack[0] = 0;
+    } else {
+      for (int k = lane; k < nfront; k += 32) stack[k] = front[k];
+      top = nfront;
+    }
+    __syncthreads();  // warp 2's copy is in place before any warp walks
+    if (!live) return;
+  } else if (lane == 0) {
+    stack[0] = 0;
+  }
   __syncwarp();
-  while (top > 0 || nleaf > 0) {
+  // (staged > 0 with nothing left to walk: cells the shared phase staged; the
+  // draining iteration evaluates them)
+  while (top > 0 || nleaf > 0 || staged > 0) {
     if (top > 0) {
       if (++iters > total + 64) {  // every node is popped at most once
         if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
@@ -2207,12 +2386,15 @@ template <bool REL>
 void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order, int mode,
                  const nbsp_mlp::Net* net, const NbspCorrectionLists* lists, float eps2,
                  double4* out, unsigned long long* counters, int* status, cudaStream_t stream) {
-  if (mode == NBSP_BH_WALK_LISTS || net != nullptr) {
+  if (mode == NBSP_BH_WALK_LISTS || mode == NBSP_BH_WALK_SHARED || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
     NbspCorrectionLists none{};
     if (net != nullptr && lists != nullptr) {  // the network corrects the monopole term
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true, REL><<<blocks, kListThreads, 0, stream>>>(
           p, tol, (int)n, t, eps2, out, counters, status, net, *lists);
+    } else if (order == 1 && mode == NBSP_BH_WALK_SHARED) {
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL, true><<<blocks, kListThreads, 0, stream>>>(
+          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
           p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);

@@ -135,7 +135,7 @@ NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t 
                                  const double* geometry, double theta, int opening,
                                  int quadrupoles, void* tree, int* status, cudaStream_t stream);
 
-enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1 };
+enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1, NBSP_BH_WALK_SHARED = 2 };
 
 /* Walk: a_sorted / G (double4 per target: the compensated sums combined in
  * FP64) and interaction counters.

@@ -21,10 +21,10 @@ def to_system(nb, p):
     return nb.ParticleSystem(*[getattr(p, f).copy() for f in O.FIELDS])
 
 
-WALKS = [0, 1]  # stackless skip-link walk, interaction-list walk
+WALKS = [0, 1, 2]  # stackless skip-link walk, interaction-list walk, lists with a shared top
 
 
-@pytest.fixture(params=WALKS, ids=["stackless", "lists"])
+@pytest.fixture(params=WALKS, ids=["stackless", "lists", "shared"])
 def walk(request):
     return request.param
 
@@ -195,6 +195,43 @@ def test_collision_1m_config_accuracy(cuda, ctx):
     print(f"collision1M theta0.7 rms={e_plain:.3e} max={m_plain:.3e} relative rms={e_rel:.3e}")
     assert e_plain < 2.5e-3 and m_plain < 0.1
     assert e_rel <= 1e-3
+
+
+@pytest.mark.parametrize("name,n,seed,theta,alpha", [
+    ("plummer_collision", 200000, 42, 0.7, 0.0), ("plummer_collision", 200000, 42, 1.0, 0.004),
+    ("globular_cluster", 40, 3, 0.7, 0.0), ("random_cloud", 1000, 8, 0.5, 0.0),
+    ("globular_cluster", 50001, 5, 1.0, 0.003)])
+def test_shared_top_walk_makes_the_same_decisions(cuda, ctx, name, n, seed, theta, alpha):
+    """The walk whose top of the tree is traversed once per block of 4 groups
+    accepts, opens and sums exactly the nodes of the per-group walk: the same
+    counts of accepted cells and particle terms, and forces equal up to the
+    order of the FP32 sums; partial blocks (n not a multiple of 128) included."""
+    p = O.preset(name, n, seed)
+    g = cuda.gravity_init(1.0, 0.01)
+    if alpha > 0:  # the relative test reads previous forces: the same ones for both walks
+        ctx.theta = theta
+        ctx.upload(to_system(cuda, p))
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+        a_old = ctx.download_accelerations()
+        p.ax[:], p.ay[:], p.az[:] = a_old.T
+    out = {}
+    for walk in (1, 2):
+        ctx.set_walk(walk)
+        ctx.theta = theta
+        ctx.set_leaf_capacity(32 if alpha > 0 else 16)
+        ctx.set_relative_opening(alpha)
+        ctx.upload(to_system(cuda, p))
+        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+        out[walk] = (ctx.download_accelerations(), ctx.stats(), ctx.walk_restarts())
+    (a1, s1, r1), (a2, s2, r2) = out[1], out[2]
+    assert s1["accepted_approximations"] == s2["accepted_approximations"]
+    assert s1["exact_interactions"] == s2["exact_interactions"]
+    assert r1 == r2
+    rel = np.linalg.norm(a1 - a2, axis=1) / np.maximum(np.linalg.norm(a1, axis=1), 1e-300)
+    print(f"{name} n={n}: max rel {rel.max():.2e}, terms {s1['accepted_approximations']} + "
+          f"{s1['exact_interactions']}")
+    assert rel.max() < 1e-5
+    assert O.rms_relative_error(a2, a1) < 1e-6
 
 
 @pytest.mark.parametrize("theta", [0.5, 1.0])
