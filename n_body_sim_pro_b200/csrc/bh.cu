@@ -491,6 +491,7 @@ struct Tree {
   int* parent;        // [2n-1] binary parent id (root: -1)
   int* cell;          // [2n-1] octree level of a cell node, -1 otherwise
   int* kept;          // [2n-1] 1 if the node is in the bucketed octree
+  int* oparent;       // [2n-1] octree parent (binary id) of a cell node, from keep_kernel
   uint32_t* mask;     // [n]   levels of kept nodes starting at particle k
   uint32_t* offset;   // [n+1] exclusive scan of popcounts; offset[n] = node count
   uint32_t* block_sums;  // scan scratch
@@ -536,6 +537,7 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.parent = carve<int>(p, nb);
   t.cell = carve<int>(p, nb);
   t.kept = carve<int>(p, nb);
+  t.oparent = carve<int>(p, nb);
   t.mask = carve<uint32_t>(p, n);
   t.offset = carve<uint32_t>(p, n + 1);
   t.block_sums = carve<uint32_t>(p, (n + kScanItems - 1) / kScanItems + 1);
@@ -670,12 +672,14 @@ __global__ void keep_kernel(Tree t, int leaf_capacity, int* status) {
   int kept = 0;
   const int lvl = t.cell[b];
   if (lvl >= 0) {
+    int p = -1;
     if (b == 0) {
       kept = 1;
     } else {
-      const int p = octree_parent(t, b, status);
+      p = octree_parent(t, b, status);
       kept = p >= 0 && (last_of(t, p) - first_of(t, p) + 1) > leaf_capacity;
     }
+    t.oparent[b] = p;  // place_kernel reads it instead of climbing again
     if (kept) atomicOr(&t.mask[first_of(t, b)], 1u << lvl);
   }
   t.kept[b] = kept;
@@ -788,8 +792,11 @@ __global__ void place_kernel(Tree t, int leaf_capacity, int* status) {
   const bool leaf = b >= n - 1 || count <= leaf_capacity || lvl >= 21;
   int parent_node = -1;
   if (b != 0) {
-    const int p = octree_parent(t, b, status);
-    if (p < 0) return;
+    const int p = t.oparent[b];  // kept nodes are cells: keep_kernel stored it
+    if (p < 0 || p >= n - 1) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return;
+    }
     parent_node = dfs_index(t, first_of(t, p), t.cell[p]);
     if (parent_node < 0 || parent_node >= node) {  // parents precede children in DFS order
       atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
