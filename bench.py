@@ -16,8 +16,8 @@ One step = one kick-drift-force-kick of all N particles; metric: particle-steps/
 initial state: for each Barnes-Hut method — the monopole and quadrupole walks
 under the reference's opening test and under the offset test, 16- and
 32-particle buckets, the relative opening test (G M (2h)^2 / d^4 <=
-alpha max(|a_old|, rms |a_old|)) over the reference test at theta 1.0, and the
-learned correction at theta 1.0 — the largest theta (alpha) of its grid whose
+alpha max(|a_old|, rms |a_old|)) over the reference test at theta 0.9, 1.0 or
+1.2, and the learned correction — the largest theta (alpha) of its grid whose
 rms error on 4096 seeded targets is at most 1e-3 is timed.  "plain" is the
 monopole walk with the reference's test; `value` is the fastest method meeting
 the bar ("chosen"), timed over the K steps of the timed region; the line also
@@ -104,6 +104,8 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 
 # relative opening test over the reference test at theta 1.0: the alphas of its sweep
 ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
               0.007, 0.01)
+# (geometric safety bound theta, bucket capacity) of the relative-test sweeps
+RELATIVE_SWEEPS = ((1.0, 16), (1.0, 32), (0.9, 32), (1.2, 32))
 # the learned correction at matched accuracy: trained and evaluated at each of
 # these opening angles (its training pairs are the near cells the walk at that
 # angle accepts)
@@ -514,14 +516,14 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
         ctx.theta = th
         rows.append((th, accuracy(nb, ctx, g, targets, ref)))
     sweep["order1_reference_leaf32"] = rows
-    ctx.theta = 1.0
-    for leaf in (16, 32):
+    for bound, leaf in RELATIVE_SWEEPS:
+        ctx.theta = bound
         ctx.set_leaf_capacity(leaf)
         rows = []
         for alpha in ALPHA_GRID:
             ctx.set_relative_opening(alpha)
             rows.append((alpha, accuracy(nb, ctx, g, targets, ref)))
-        sweep[f"order1_relative_alpha_theta1.0_leaf{leaf}"] = rows
+        sweep[f"order1_relative_alpha_theta{bound}_leaf{leaf}"] = rows
     ctx.set_relative_opening(0.0)
     ctx.close()
 
@@ -537,10 +539,11 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
     b = best(sweep["order1_reference_leaf32"])
     if b:
         candidates.append((method("order1_reference_leaf32", b[0], leaf=32), b[1]))
-    for leaf in (16, 32):
-        b = best(sweep[f"order1_relative_alpha_theta1.0_leaf{leaf}"])
+    for bound, leaf in RELATIVE_SWEEPS:
+        b = best(sweep[f"order1_relative_alpha_theta{bound}_leaf{leaf}"])
         if b:
-            candidates.append((method(f"relative_leaf{leaf}", 1.0, alpha=b[0], leaf=leaf), b[1]))
+            name = f"relative_leaf{leaf}" + ("" if bound == 1.0 else f"_theta{bound}")
+            candidates.append((method(name, bound, alpha=b[0], leaf=leaf), b[1]))
 
     def timed(m, r, correction=None):
         v, ms, walk = timed_steps(nb, torch, system, g, wl, m, steps, warmup, flush, correction)
