@@ -16,8 +16,8 @@ One step = one kick-drift-force-kick of all N particles; metric: particle-steps/
 initial state: for each Barnes-Hut method — the monopole and quadrupole walks
 under the reference's opening test and under the offset test, 16- and
 32-particle buckets, the relative opening test (G M (2h)^2 / d^4 <=
-alpha max(|a_old|, rms |a_old|)) over the reference test at theta 0.9, 1.0 or
-1.2, and the learned correction — the largest theta (alpha) of its grid whose
+alpha max(|a_old|, rms |a_old|)) over the reference test at theta 1.0 to 1.7
+as the safety bound, and the learned correction — the largest theta (alpha) of its grid whose
 rms error on 4096 seeded targets is at most 1e-3 is timed.  "plain" is the
 monopole walk with the reference's test; `value` is the fastest method meeting
 the bar ("chosen"), timed over the K steps of the timed region; the line also
@@ -105,7 +105,7 @@ THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 
 ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
               0.007, 0.01)
 # (geometric safety bound theta, bucket capacity) of the relative-test sweeps
-RELATIVE_SWEEPS = ((1.0, 16), (1.0, 32), (0.9, 32), (1.2, 32))
+RELATIVE_SWEEPS = ((1.0, 16), (1.0, 32), (1.2, 32), (1.4, 32), (1.7, 32))
 # the learned correction at matched accuracy: trained and evaluated at each of
 # these opening angles (its training pairs are the near cells the walk at that
 # angle accepts)
