@@ -16,9 +16,10 @@ One step = one kick-drift-force-kick of all N particles; metric: particle-steps/
 initial state: for each Barnes-Hut method — the monopole and quadrupole walks
 under the reference's opening test and under the offset test, 16- and
 32-particle buckets, the relative opening test (G M (2h)^2 / d^4 <=
-alpha max(|a_old|, rms |a_old|)) over the reference test at theta 1.0 to 1.7
+alpha max(|a_old|, rms |a_old|)) over the reference test at theta 1.0 to 5.0
 as the safety bound, and the learned correction — the largest theta (alpha) of its grid whose
-rms error on 4096 seeded targets is at most 1e-3 is timed.  "plain" is the
+rms error on 4096 seeded targets is at most 0.97e-3 (3% under the 1e-3 target,
+so the state the timed steps reach stays within it) is timed.  "plain" is the
 monopole walk with the reference's test; `value` is the fastest method meeting
 the bar ("chosen"), timed over the K steps of the timed region; the line also
 carries plain at theta 0.5, plain at its matched theta, the relative test and the
@@ -99,13 +100,17 @@ SECONDARY = ("bh_collision_1m", "allpairs_plummer_16k", "allpairs_precision_262k
 # relative force error (FP64 direct sum on 4096 seeded targets, initial state)
 # stays at or below RMS_TARGET, per method.
 RMS_TARGET = 1e-3
+# a method qualifies at RMS_SELECT on the initial state, 3% under the target,
+# so that the state it reaches over the timed steps (its rms is in the line)
+# stays within the target too; every method is held to the same margin
+RMS_SELECT = 0.97 * RMS_TARGET
 THETA_GRID = (0.4, 0.45, 0.5, 0.525, 0.55, 0.575, 0.6, 0.625, 0.65, 0.675, 0.7, 0.725, 0.75, 0.8,
               0.9, 1.0)
 # relative opening test over the reference test at theta 1.0: the alphas of its sweep
-ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.0045, 0.005, 0.0055, 0.006,
-              0.007, 0.01)
+ALPHA_GRID = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.0035, 0.004, 0.00425, 0.0045, 0.00475,
+              0.005, 0.00525, 0.0055, 0.00575, 0.006, 0.007, 0.01)
 # (geometric safety bound theta, bucket capacity) of the relative-test sweeps
-RELATIVE_SWEEPS = ((1.0, 16), (1.0, 32), (1.2, 32), (1.4, 32), (1.7, 32))
+RELATIVE_SWEEPS = ((1.0, 16), (1.0, 32), (1.7, 32), (2.5, 32), (3.5, 32), (5.0, 32))
 # the learned correction at matched accuracy: trained and evaluated at each of
 # these opening angles (its training pairs are the near cells the walk at that
 # angle accepts)
@@ -491,7 +496,7 @@ def train_correction(nb, g, opening, theta=1.0, n_train=1_000_000, samples=1 << 
 
 def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
                   with_correction=False):
-    """Every method at its largest theta (alpha) of the grid meeting RMS_TARGET
+    """Every method at its largest theta (alpha) of the grid meeting RMS_SELECT
     on the initial state, timed; the plain walk at theta 0.5 and the learned
     correction at theta 1.0 timed as well.  Returns the record and the trained
     corrections (kept alive for the timed region)."""
@@ -528,7 +533,7 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
     ctx.close()
 
     def best(rows):
-        ok = [(x, r) for x, r in rows if r[0] <= RMS_TARGET]
+        ok = [(x, r) for x, r in rows if r[0] <= RMS_SELECT]
         return max(ok, key=lambda t: t[0]) if ok else None
 
     candidates = []
@@ -551,7 +556,7 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
                     walk_ms=round(walk, 4))
 
     methods = [timed(m, r) for m, r in candidates]
-    out = {"rms_target": RMS_TARGET,
+    out = {"rms_target": RMS_TARGET, "rms_select": RMS_SELECT,
            "oracle": f"FP64 device direct sum, {len(targets)} seeded targets, initial state",
            "sweep": {k: [[x, round(r[0], 6)] for x, r in rows] for k, rows in sweep.items()},
            "methods": methods}
@@ -589,7 +594,7 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
                                                              / 1e12, 3) if walk_ms > 0 else None}
             rec["training"] = training
             corrected[oname] = rec
-            if r[0] <= RMS_TARGET:
+            if r[0] <= RMS_SELECT:
                 methods.append(rec)
         # the corrected walk at matched accuracy: the largest angle whose
         # corrected error meets the target, the network trained at that angle
@@ -607,7 +612,7 @@ def matched_study(nb, torch, wl, system, g, targets, ref, steps, warmup, flush,
             rows.append((th, r, m, training))
         out["sweep"]["corrected_reference_trained_at_theta"] = [[th, round(r[0], 6)]
                                                                for th, r, _, _ in rows]
-        ok = [row for row in rows if row[1][0] <= RMS_TARGET]
+        ok = [row for row in rows if row[1][0] <= RMS_SELECT]
         if ok:
             th, r, m, training = max(ok, key=lambda row: row[0])
             rec = timed(m, r, corrections[m["correction"]])
