@@ -132,6 +132,9 @@ PROFILED_TRAFFIC = {
         30_559_232, "profiles/walk_lists_kernel_bh_collision_1m.md"),
     ("allpairs_plummer_16k", None, 1, "lists", 16, 0.0): (
         296_960, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
+    # one-pass DRAM capture of the full 10M walk launch
+    ("bh_matched_10m", 5.0, 1, "lists", 32, 0.0045): (
+        566_170_000, "profiles/bh_step_launches_relative_10m.md"),
 }
 
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
@@ -1275,6 +1278,9 @@ def main(argv=None):
                     help="skip the matched-accuracy study of the Barnes-Hut workloads")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the sub-records of the other configurations")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the plugin-path measurement (one device context less, for "
+                         "profiling)")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--order", type=int, default=None, choices=[1, 2])
     ap.add_argument("--walk", default=None, choices=["lists", "stackless", "shared"])
@@ -1310,7 +1316,8 @@ def main(argv=None):
     sharded = wl["algorithm"] == "all_pairs_sharded" or wl.get("sharded", False)
     if sharded:
         config["parallelism"] = f"sharded x{world}"
-    r = run_workload(args, args.workload, wl, world, rank, local, args.steps, args.warmup)
+    r = run_workload(args, args.workload, wl, world, rank, local, args.steps, args.warmup,
+                     with_e2e=not args.no_e2e)
     if wl["algorithm"] == "ensemble":
         config["particles"] = (sum(ensemble_sizes(wl)) if wl.get("sharded")
                                else r["stats"]["particles"])

@@ -275,12 +275,16 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_openin
 
 /* No reference counterpart: the relative opening test (Springel 2001) on top of
  * the geometric one.  With alpha > 0 a cell of mass M and side 2h is accepted
- * for a target only when also  G M (2h)^2 / d^4 <= alpha |a_old|,  a_old the
- * target's acceleration in the state (the previous evaluation's, or what was
- * uploaded / passed in the view); targets with a_old = 0 use the geometric
- * test alone.  theta (with OFFSET, 1.0 keeps every target outside the cells it
- * accepts) becomes the safety bound.  0 (default) turns it off.  Not combined
- * with a learned correction, which keeps the geometric test it was trained on. */
+ * for a target only when also  G M (2h)^2 / d^4 <= alpha max(|a_old|, rms),
+ * a_old the target's acceleration in the state (the previous evaluation's, or
+ * what was uploaded / passed in the view) and rms the root mean square of
+ * |a_old| over the state.  theta becomes a geometric bound on top (the test
+ * is fastest at rms force error 1e-3 with a loose one, theta 5.0, and
+ * alpha 0.0045).  A state without previous accelerations (all a_old zero, or
+ * not finite) is evaluated with the geometric test alone at
+ * min(theta, 0.5), so its first evaluation is an ordinary Barnes-Hut one and
+ * the next reads its result.  0 (default) turns it off.  A learned correction
+ * still corrects the monopole of the cells the combined test accepts. */
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_opening(
     NBodySimProCudaContext* context, double alpha, NBodySimProError* error);
 

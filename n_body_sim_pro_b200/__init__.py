@@ -456,8 +456,10 @@ class CudaContext:
                                                                  C.byref(err)), err)
 
     def set_relative_opening(self, alpha: float) -> None:
-        """Relative opening test G M (2h)^2 / d^4 <= alpha |a_old| on top of the
-        geometric one (alpha 0: off)."""
+        """Relative opening test G M (2h)^2 / d^4 <= alpha max(|a_old|, rms |a_old|)
+        on top of the geometric one (alpha 0: off).  A state without previous
+        accelerations is evaluated with the geometric test alone at
+        min(theta, 0.5)."""
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_relative_opening(
             self.handle, float(alpha), C.byref(err)), err)

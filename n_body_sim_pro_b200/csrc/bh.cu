@@ -840,6 +840,10 @@ struct Opening {
   const uint64_t* keys;  // sorted Morton keys (a node's first key names its cell)
   const double* geometry;
   double inv_theta, inv_theta2;
+  // relative opening test on: a state without previous accelerations (rms
+  // |a_old| in geometry[7] zero or not finite) is opened at the start angle
+  double start_inv_theta, start_inv_theta2;
+  int relative;
   int criterion;         // NBSP_BH_OPENING_*
 };
 
@@ -866,10 +870,17 @@ __device__ void finish_node(const Tree& t, int node, const Moments& mo, int firs
     shift2 += d * d;
   }
   const double shift = sqrt(shift2);
+  // Without previous accelerations every target's relative test passes (its
+  // tolerance is +inf), so the geometric test alone decides: at the start
+  // angle, not at the loose bound the relative test runs under.
+  const double a_rms = o.geometry[7];
+  const bool start = o.relative && !(a_rms > 0.0 && a_rms < INFINITY);
+  const double it = start ? o.start_inv_theta : o.inv_theta;
+  const double it2 = start ? o.start_inv_theta2 : o.inv_theta2;
   // reference: accept when (2h)^2 < theta^2 d^2; offset: when 2h / theta + shift < d
   const double r2 = o.criterion == NBSP_BH_OPENING_OFFSET
-                        ? (side * o.inv_theta + shift) * (side * o.inv_theta + shift)
-                        : side * side * o.inv_theta2;
+                        ? (side * it + shift) * (side * it + shift)
+                        : side * side * it2;
   t.ropen2[node] = (float)r2;
   t.side[node] = (float)side;
   t.shift[node] = (float)shift;
@@ -2513,8 +2524,8 @@ void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree
 }
 
 void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const double* geometry,
-                     double theta, int opening, int quadrupoles, void* tree, int* status,
-                     cudaStream_t stream) {
+                     double theta, double start_theta, int opening, int quadrupoles, void* tree,
+                     int* status, cudaStream_t stream) {
   Tree t = tree_view(tree, n);
   const size_t nb = 2 * n - 1;
   Opening o;
@@ -2522,6 +2533,9 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
   o.geometry = geometry;
   o.inv_theta = theta > 0.0 ? 1.0 / theta : INFINITY;
   o.inv_theta2 = theta > 0.0 ? 1.0 / (theta * theta) : INFINITY;
+  o.relative = start_theta > 0.0;
+  o.start_inv_theta = o.relative ? 1.0 / start_theta : o.inv_theta;
+  o.start_inv_theta2 = o.relative ? 1.0 / (start_theta * start_theta) : o.inv_theta2;
   o.criterion = opening;
   size_t blocks = (nb + 255) / 256;  // grid-stride over the octree nodes (<= 2n - 1)
   if (blocks > 148 * 16) blocks = 148 * 16;

@@ -131,9 +131,18 @@ NBSP_HIDDEN void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity
  * with the cell's centre-of-mass offset added, 2h / theta + shift < d. */
 enum { NBSP_BH_OPENING_REFERENCE = 0, NBSP_BH_OPENING_OFFSET = 1 };
 
+/* start_theta > 0 (the relative opening test is on): when the state has no
+ * previous accelerations (rms |a_old| zero or not finite) the opening radii are
+ * those of start_theta instead of theta.  The relative test then passes for
+ * every target and the geometric test decides alone, so a fresh state is
+ * opened at an ordinary angle rather than at the loose geometric bound the
+ * relative test is run under. */
+#define NBSP_BH_START_THETA 0.5
+
 NBSP_HIDDEN void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n,
-                                 const double* geometry, double theta, int opening,
-                                 int quadrupoles, void* tree, int* status, cudaStream_t stream);
+                                 const double* geometry, double theta, double start_theta,
+                                 int opening, int quadrupoles, void* tree, int* status,
+                                 cudaStream_t stream);
 
 enum { NBSP_BH_WALK_STACKLESS = 0, NBSP_BH_WALK_LISTS = 1, NBSP_BH_WALK_SHARED = 2 };
 

@@ -203,7 +203,8 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
                    rel ? b->tol : NULL, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
-    nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta, p->opening,
+    nbsp_bh_moments(b->pos4, b->keys, n, b->geometry, p->theta,
+                    rel ? fmin(p->theta, NBSP_BH_START_THETA) : 0.0, p->opening,
                     p->multipole_order == 2 || p->correction != NULL || p->quadrupoles, b->tree,
                     status, stream);
     cudaEventRecord(b->events[5], stream);

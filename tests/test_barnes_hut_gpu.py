@@ -204,7 +204,9 @@ def test_headline_configuration_10m_accuracy(cuda, ctx):
     study chooses — the relative opening test at alpha 0.0045 with the
     geometric test at theta 5.0 as the bound, 32-particle buckets, evaluated
     twice so the test reads the previous forces as in a run — holds rms <= 1e-3,
-    and so does the plain walk at theta 0.5 it is compared with."""
+    and so does the plain walk at theta 0.5 it is compared with.  The first
+    evaluation of the fresh state (no previous forces: the geometric test at
+    the start angle 0.5) holds it too."""
     n = 10_000_000
     ctx.generate_plummer_collision(n, 42)
     s = cuda.ParticleSystem.zeros(n)
@@ -218,16 +220,20 @@ def test_headline_configuration_10m_accuracy(cuda, ctx):
     ctx.theta = 0.5
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
     a_plain = ctx.download_accelerations()[targets]
+    ctx.upload(s)  # the generated state again: accelerations zero
     ctx.theta = 5.0
     ctx.set_leaf_capacity(32)
     ctx.set_relative_opening(0.0045)
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+    a_first = ctx.download_accelerations()[targets]
     ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
     a_rel = ctx.download_accelerations()[targets]
     e_plain, e_rel = O.rms_relative_error(a_plain, ref), O.rms_relative_error(a_rel, ref)
+    e_first = O.rms_relative_error(a_first, ref)
     m_rel = float(np.max(np.linalg.norm(a_rel - ref, axis=1) / np.linalg.norm(ref, axis=1)))
-    print(f"10M: plain theta 0.5 rms={e_plain:.3e}; relative rms={e_rel:.3e} max={m_rel:.3e}")
-    assert e_plain <= 1e-3
+    print(f"10M: plain theta 0.5 rms={e_plain:.3e}; relative first={e_first:.3e} "
+          f"rms={e_rel:.3e} max={m_rel:.3e}")
+    assert e_plain <= 1e-3 and e_first <= 1e-3
     assert e_rel <= 1e-3 and m_rel < 0.05
 
 
@@ -297,24 +303,34 @@ def _resident(cuda, p, theta, opening=0, alpha=0.0, eps=0.01):
     return ctx
 
 
-def test_relative_opening_limits_are_the_geometric_walk(cuda):
-    """alpha -> infinity, or no previous accelerations at all (a_old = 0 and rms
-    |a_old| = 0): every relative test passes, the geometric test alone decides."""
+@pytest.mark.parametrize("opening", [0, 1])
+def test_relative_opening_limits_are_the_geometric_walk(cuda, opening):
+    """alpha -> infinity: every relative test passes and the geometric test at
+    theta alone decides.  No previous accelerations at all (a_old = 0, rms
+    |a_old| = 0): the geometric test alone decides at the start angle
+    min(theta, 0.5), so a fresh state under a loose bound (theta 1.0 or 5.0)
+    gets an ordinary first evaluation, and the next one reads it."""
     p = O.preset("plummer_collision", 100000, 42)
     g = cuda.gravity_init(1.0, 0.01)
-    with _resident(cuda, p, 1.0, opening=1) as ctx:
+
+    def geometric(theta):
+        with _resident(cuda, p, theta, opening=opening) as ctx:
+            ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+            return ctx.download_accelerations()
+
+    g10, g05, g04 = geometric(1.0), geometric(0.5), geometric(0.4)
+    assert not np.array_equal(g10, g05)
+    with _resident(cuda, p, 1.0, opening=opening) as ctx:
         ctx.set_relative_opening(1e30)
         ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old = 0 here
         first = ctx.download_accelerations()
         ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)  # a_old = first
         huge = ctx.download_accelerations()
-        ctx.set_relative_opening(0.0)
-        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
-        geometric = ctx.download_accelerations()
-    assert np.array_equal(first, geometric) and np.array_equal(huge, geometric)
-    with _resident(cuda, p, 1.0, opening=1, alpha=1e-3) as ctx:  # uploaded a = 0
-        ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
-        assert np.array_equal(ctx.download_accelerations(), geometric)
+    assert np.array_equal(first, g05) and np.array_equal(huge, g10)
+    for theta, expected in ((1.0, g05), (5.0, g05), (0.4, g04)):
+        with _resident(cuda, p, theta, opening=opening, alpha=1e-3) as ctx:  # uploaded a = 0
+            ctx.compute_acceleration(g, cuda.Algorithm.BARNES_HUT)
+            assert np.array_equal(ctx.download_accelerations(), expected), theta
 
 
 def test_relative_opening_trades_accuracy_for_work(cuda):
