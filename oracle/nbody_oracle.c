@@ -919,53 +919,68 @@ static void walk(const OTree* t, const double* root, double G, double eps2, doub
     }
 }
 
-int oracle_barnes_hut(const OracleView* v, double G, double eps, double theta, uint64_t* stats) {
+/* The reference's tree over the Morton-ordered particles (barnes_hut.c:145-253):
+ * buf holds x, y, z, m and three acceleration rows in Morton order, perm the
+ * input index of each Morton slot.  0 on success; the arrays are the caller's. */
+static int build_tree(const OracleView* v, OTree* t, double* root, double** buf_out,
+                      size_t** perm_out) {
     const size_t n = v->particle_count;
-    if (n == 0) return 1;
-    double root[4];
     uint64_t* keys;
     size_t* perm;
     if (morton_sorted(v, root, &keys, &perm)) return 2;
     free(keys);
     double* buf = (double*)malloc(7 * n * sizeof(double));
-    OTree t;
-    t.cap = 2 * n - 1;
-    t.nodes = (ONode*)malloc(t.cap * sizeof(ONode));
-    if (buf == NULL || t.nodes == NULL) {
+    t->cap = 2 * n - 1;
+    t->nodes = (ONode*)malloc(t->cap * sizeof(ONode));
+    if (buf == NULL || t->nodes == NULL) {
         free(buf);
-        free(t.nodes);
+        free(t->nodes);
         free(perm);
         return 2;
     }
     double *x = buf, *y = buf + n, *z = buf + 2 * n, *m = buf + 3 * n;
-    double *ax = buf + 4 * n, *ay = buf + 5 * n, *az = buf + 6 * n;
     for (size_t i = 0; i < n; ++i) {
         x[i] = v->positions_x[perm[i]];
         y[i] = v->positions_y[perm[i]];
         z[i] = v->positions_z[perm[i]];
         m[i] = v->masses[perm[i]];
     }
-    t.x = x;
-    t.y = y;
-    t.z = z;
-    t.m = m;
-    t.used = 0;
-    new_node(&t);
+    t->x = x;
+    t->y = y;
+    t->z = z;
+    t->m = m;
+    t->used = 0;
+    new_node(t);
     int status = 0;
     for (size_t i = 0; i < n && status == 0; ++i) {
-        if (t.nodes[0].count == 0) {
-            make_leaf(&t, 0, i);
+        if (t->nodes[0].count == 0) {
+            make_leaf(t, 0, i);
             continue;
         }
-        status = insert(&t, 0, i, root[0], root[1], root[2], root[3], 0);
+        status = insert(t, 0, i, root[0], root[1], root[2], root[3], 0);
     }
     if (status != 0) {
         free(buf);
-        free(t.nodes);
+        free(t->nodes);
         free(perm);
         return status;
     }
-    centres_of_mass(&t);
+    centres_of_mass(t);
+    *buf_out = buf;
+    *perm_out = perm;
+    return 0;
+}
+
+int oracle_barnes_hut(const OracleView* v, double G, double eps, double theta, uint64_t* stats) {
+    const size_t n = v->particle_count;
+    if (n == 0) return 1;
+    double root[4];
+    double* buf;
+    size_t* perm;
+    OTree t;
+    const int status = build_tree(v, &t, root, &buf, &perm);
+    if (status != 0) return status;
+    double *ax = buf + 4 * n, *ay = buf + 5 * n, *az = buf + 6 * n;
     uint64_t leaves = 0, internal = 0;
     for (size_t k = 0; k < t.used; ++k) {
         if (t.nodes[k].particle != -1) {
@@ -1000,6 +1015,133 @@ int oracle_barnes_hut(const OracleView* v, double G, double eps, double theta, u
         stats[4] = exact_total;
         stats[5] = depth_of(&t, 0);
     }
+    free(buf);
+    free(t.nodes);
+    free(perm);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Analysis, no reference counterpart: the monopole error of the walk above,  */
+/* split by how wide each accepted cell looks from the target                 */
+/* ------------------------------------------------------------------------- */
+
+/* The walk of barnes_hut.c:549-636 for one target; at every accepted cell (side
+ * 2h, distance d to its centre of mass) the cell's error -- its monopole term
+ * minus the exact softened sum over its particles (the target itself left
+ * out, as in the direct sum) -- is added to the bin of (2h / d) / theta, and the
+ * bin's cell count is raised.  Leaves are exact and add nothing, so the bins
+ * sum to the walk's force minus the direct sum. */
+static void residual_walk(const OTree* t, const int32_t* lo, const int32_t* hi, const double* root,
+                          double G, double eps2, double theta, size_t q, int bins, double* err,
+                          uint64_t* count) {
+    OEntry stack[1024];
+    int top = 1;
+    stack[0].node = 0;
+    stack[0].cx = root[0];
+    stack[0].cy = root[1];
+    stack[0].cz = root[2];
+    stack[0].h = root[3];
+    const double qx = t->x[q], qy = t->y[q], qz = t->z[q];
+    const double th2 = theta * theta;
+    while (top > 0) {
+        const OEntry e = stack[--top];
+        const ONode* n = &t->nodes[e.node];
+        if (n->count == 0 || n->particle != -1) continue;
+        const double dx = n->cx - qx;
+        const double dy = n->cy - qy;
+        const double dz = n->cz - qz;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double size2 = 4.0 * e.h * e.h;
+        if (d2 > 0.0 && size2 < th2 * d2) {
+            const double r2 = d2 + eps2;
+            const double s = G * n->mass / (r2 * sqrt(r2));
+            double ex = 0.0, ey = 0.0, ez = 0.0;
+            for (int32_t j = lo[e.node]; j <= hi[e.node]; ++j) {
+                if ((size_t)j == q) continue;
+                const double jx = t->x[j] - qx, jy = t->y[j] - qy, jz = t->z[j] - qz;
+                const double rj2 = jx * jx + jy * jy + jz * jz + eps2;
+                const double sj = G * t->m[j] / (rj2 * sqrt(rj2));
+                ex += sj * jx;
+                ey += sj * jy;
+                ez += sj * jz;
+            }
+            int b = (int)(sqrt(size2 / d2) / theta * bins);
+            b = b < 0 ? 0 : b >= bins ? bins - 1 : b;
+            err[3 * b + 0] += s * dx - ex;
+            err[3 * b + 1] += s * dy - ey;
+            err[3 * b + 2] += s * dz - ez;
+            ++count[b];
+            continue;
+        }
+        const double hh = 0.5 * e.h;
+        const double off = e.h * 0.5;
+        for (int c = 0; c < 8; ++c) {
+            const int32_t ch = n->child[c];
+            if (ch == -1) continue;
+            if (top >= 1024) break;
+            stack[top].node = ch;
+            stack[top].cx = e.cx + ((c & 1) ? off : -off);
+            stack[top].cy = e.cy + ((c & 2) ? off : -off);
+            stack[top].cz = e.cz + ((c & 4) ? off : -off);
+            stack[top].h = hh;
+            ++top;
+        }
+    }
+}
+
+int oracle_barnes_hut_residual_bands(const OracleView* v, double G, double eps, double theta,
+                                     const int64_t* targets, size_t n_targets, int bins,
+                                     double* err, uint64_t* count) {
+    const size_t n = v->particle_count;
+    if (n == 0 || bins < 1) return 1;
+    double root[4];
+    double* buf;
+    size_t* perm;
+    OTree t;
+    const int status = build_tree(v, &t, root, &buf, &perm);
+    if (status != 0) return status;
+    /* Morton-slot range of every node: nodes are created after their parents,
+     * and a cell's particles are consecutive in Morton order */
+    int32_t* lo = (int32_t*)malloc(t.used * sizeof(int32_t));
+    int32_t* hi = (int32_t*)malloc(t.used * sizeof(int32_t));
+    size_t* slot = (size_t*)malloc(n * sizeof(size_t));
+    if (lo == NULL || hi == NULL || slot == NULL) {
+        free(lo);
+        free(hi);
+        free(slot);
+        free(buf);
+        free(t.nodes);
+        free(perm);
+        return 2;
+    }
+    for (size_t k = t.used; k > 0; --k) {
+        const ONode* nd = &t.nodes[k - 1];
+        if (nd->particle != -1) {
+            lo[k - 1] = hi[k - 1] = nd->particle;
+            continue;
+        }
+        int32_t a = INT32_MAX, b = -1;
+        for (int c = 0; c < 8; ++c) {
+            const int32_t ch = nd->child[c];
+            if (ch == -1) continue;
+            if (lo[ch] < a) a = lo[ch];
+            if (hi[ch] > b) b = hi[ch];
+        }
+        lo[k - 1] = a;
+        hi[k - 1] = b;
+    }
+    for (size_t i = 0; i < n; ++i) slot[perm[i]] = i;
+    const double eps2 = eps * eps;
+    memset(err, 0, n_targets * (size_t)bins * 3 * sizeof(double));
+    memset(count, 0, n_targets * (size_t)bins * sizeof(uint64_t));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long k = 0; k < (long long)n_targets; ++k)
+        residual_walk(&t, lo, hi, root, G, eps2, theta, slot[targets[k]], bins,
+                      err + (size_t)k * bins * 3, count + (size_t)k * bins);
+    free(lo);
+    free(hi);
+    free(slot);
     free(buf);
     free(t.nodes);
     free(perm);

@@ -115,6 +115,17 @@ int oracle_morton_order(const OracleView* view, uint64_t* keys_sorted, uint64_t*
 int oracle_barnes_hut(const OracleView* view, double gravitational_constant,
                       double softening_length, double theta, uint64_t* stats);
 
+/* Analysis of the walk above (no reference counterpart): for each target (input
+ * index), the error of every accepted cell's monopole against the exact sum
+ * over the cell's particles, summed into `bins` bins of (2h / d) / theta
+ * (err[target][bin][3]), and the number of accepted cells per bin
+ * (count[target][bin]).  The bins of a target sum to its Barnes-Hut force minus
+ * the direct sum. */
+int oracle_barnes_hut_residual_bands(const OracleView* view, double gravitational_constant,
+                                     double softening_length, double theta,
+                                     const int64_t* targets, size_t n_targets, int bins,
+                                     double* err, uint64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -152,6 +152,8 @@ def lib() -> C.CDLL:
             "oracle_potential_energy_openmp": (d, [pv, d, d]),
             "oracle_morton_order": (C.c_int, [pv, C.POINTER(u64), C.POINTER(u64), C.POINTER(d)]),
             "oracle_barnes_hut": (C.c_int, [pv, d, d, d, C.POINTER(u64)]),
+            "oracle_barnes_hut_residual_bands": (C.c_int, [pv, d, d, d, i64p, sz, C.c_int,
+                                                           C.POINTER(d), C.POINTER(u64)]),
             "oracle_mix_seed": (u64, [u64, u64]),
         }
         for name, (res, args) in sig.items():
@@ -391,6 +393,25 @@ def barnes_hut(p: Particles, G: float, eps: float, theta: float):
     keys = ("node_count", "leaf_count", "internal_node_count", "accepted_approximations",
             "exact_interactions", "maximum_depth")
     return p.acc(), dict(zip(keys, (int(s) for s in stats)))
+
+
+def barnes_hut_residual_bands(p: Particles, G: float, eps: float, theta: float,
+                              targets: np.ndarray, bins: int):
+    """The monopole error of the reference's walk at `theta` on each target,
+    split by the apparent size (2h / d) / theta of the accepted cells:
+    err[t, b, 3] (monopole minus the exact sum over the cell's particles) and
+    count[t, b] (accepted cells).  err summed over the bins is the walk's force
+    minus the direct sum."""
+    tg = np.ascontiguousarray(targets, dtype=np.int64)
+    err = np.zeros((len(tg), bins, 3))
+    count = np.zeros((len(tg), bins), dtype=np.uint64)
+    v = p.view()
+    rc = lib().oracle_barnes_hut_residual_bands(
+        C.byref(v), G, eps, theta, tg.ctypes.data_as(C.POINTER(C.c_int64)), len(tg), bins,
+        err.ctypes.data_as(C.POINTER(C.c_double)), count.ctypes.data_as(C.POINTER(C.c_uint64)))
+    if rc != 0:
+        raise RuntimeError(f"oracle residual bands failed ({rc})")
+    return err, count
 
 
 def advance(p: Particles, G: float, eps: float, dt: float, steps: int, integrator: int = 1,
