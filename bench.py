@@ -824,8 +824,9 @@ def run_e2e(nb, wl, system, steps, m=None, correction=None):
     """The metric end to end through the reference-facing plugin call on pinned
     host arrays: a host leapfrog (integrator.c:47-85) whose force function is
     n_body_sim_pro_{barnes_hut_,gravity_}compute_acceleration_cuda through its C
-    ABI; each call copies positions and masses (and, under the relative opening
-    test, the previous accelerations) in and the accelerations out."""
+    ABI; each call copies positions and masses in and the accelerations out
+    (under the relative opening test the previous accelerations stay on the
+    device: the integrator passes each result back unchanged)."""
     import torch
 
     n = wl["n"]
@@ -836,6 +837,9 @@ def run_e2e(nb, wl, system, steps, m=None, correction=None):
     g = nb.gravity_init(1.0, wl["eps"])
     bh = wl["algorithm"] == "barnes_hut"
     c2 = make_context(nb, m, correction) if bh else nb.CudaContext()
+    rel = bh and m is not None and m["relative_alpha"] > 0.0
+    if rel:  # the integrator passes each result back unchanged: keep it on the device
+        c2.set_relative_source(nb.RelativeSource.FROM_CONTEXT)
     plugin = getattr(nb.library(), "n_body_sim_pro_barnes_hut_compute_acceleration_cuda"
                      if bh else "n_body_sim_pro_gravity_compute_acceleration_cuda")
     view, err = s.view(), nb.Error()
@@ -850,23 +854,32 @@ def run_e2e(nb, wl, system, steps, m=None, correction=None):
     tv = [torch.from_numpy(getattr(s, f)) for f in ("vx", "vy", "vz")]
     tx = [torch.from_numpy(getattr(s, f)) for f in ("x", "y", "z")]
     ta = [torch.from_numpy(getattr(s, f)) for f in ("ax", "ay", "az")]
+    in_force, on_device = 0.0, 0.0
     t0 = time.perf_counter()
     for _ in range(steps):
         for v, a in zip(tv, ta):
             v.add_(a, alpha=h)
         for x, v in zip(tx, tv):
             x.add_(v, alpha=dt)
+        f0 = time.perf_counter()
         force()
+        in_force += time.perf_counter() - f0
+        on_device += c2.timings()["total_ms"]
         for v, a in zip(tv, ta):
             v.add_(a, alpha=h)
     elapsed = time.perf_counter() - t0
     c2.close()
-    rel = bh and m is not None and m["relative_alpha"] > 0.0
     return {"value": n * steps / elapsed, "unit": "particle-steps/s",
-            "h2d_bytes_per_step": (4 + (3 if rel else 0)) * 8 * n,
+            "h2d_bytes_per_step": 4 * 8 * n,
             "d2h_bytes_per_step": 3 * 8 * n, "steps": steps,
+            "ms_per_step": round(1e3 * elapsed / steps, 3),
+            "plugin_ms_per_step": round(1e3 * in_force / steps, 3),
+            "host_integrator_ms_per_step": round(1e3 * (elapsed - in_force) / steps, 3),
+            "plugin_device_force_ms_per_step": round(on_device / steps, 3),
             "path": "host leapfrog (in-place, host threads) + the plugin force function "
-                    "through its C ABI on pinned host arrays",
+                    "through its C ABI on pinned host arrays" + (
+                        "; relative test's previous accelerations kept on the device "
+                        "(RELATIVE_FROM_CONTEXT)" if rel else ""),
             "timer": "host wall clock"}
 
 

@@ -288,6 +288,24 @@ N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_openin
 N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_opening(
     NBodySimProCudaContext* context, double alpha, NBodySimProError* error);
 
+/* No reference counterpart: where the plugin functions take the relative
+ * test's previous accelerations.  FROM_VIEW (default): the view's acceleration
+ * arrays, uploaded with every call (24 bytes per particle).  FROM_CONTEXT: the
+ * accelerations this context computed in its previous plugin call, kept on the
+ * device, when that call had the same particle count and the same acceleration
+ * arrays and no device-resident call came between; otherwise the view's, as
+ * with FROM_VIEW.  The reference's integrators pass the previous call's output
+ * back unchanged (integrator.c:47-85), so both give the same forces and
+ * FROM_CONTEXT saves the upload; a caller that edits the accelerations between
+ * calls wants FROM_VIEW. */
+typedef enum NBodySimProCudaRelativeSource {
+    N_BODY_SIM_PRO_CUDA_RELATIVE_FROM_VIEW = 0,
+    N_BODY_SIM_PRO_CUDA_RELATIVE_FROM_CONTEXT = 1
+} NBodySimProCudaRelativeSource;
+
+N_BODY_SIM_PRO_CUDA_API NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_source(
+    NBodySimProCudaContext* context, int source, NBodySimProError* error);
+
 /* Replaces n_body_sim_pro_barnes_hut_tree_stats (barnes_hut/barnes_hut.h:116-117):
  * 0 on success, non-zero when an argument is NULL. */
 N_BODY_SIM_PRO_CUDA_API int n_body_sim_pro_cuda_context_stats(

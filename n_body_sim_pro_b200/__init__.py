@@ -61,6 +61,13 @@ class Opening(IntEnum):
     OFFSET = 1
 
 
+class RelativeSource(IntEnum):
+    """NBodySimProCudaRelativeSource: where the plugin functions take the
+    relative opening test's previous accelerations."""
+    FROM_VIEW = 0
+    FROM_CONTEXT = 1
+
+
 class View(C.Structure):
     """NBodySimProParticleSystemView (include/n_body_sim_pro/core/particle_system.h:38-50)."""
 
@@ -179,6 +186,7 @@ EXPORTS = (
     "n_body_sim_pro_cuda_checkpoint_read", "n_body_sim_pro_cuda_context_set_opening",
     "n_body_sim_pro_cuda_shard_begin", "n_body_sim_pro_cuda_shard_end",
     "n_body_sim_pro_cuda_plummer_collision_generate", "n_body_sim_pro_cuda_correction_evaluate",
+    "n_body_sim_pro_cuda_context_set_relative_source",
 )
 
 # NBodySimProCudaMlpEngine
@@ -227,6 +235,7 @@ def library() -> C.CDLL:
         "n_body_sim_pro_cuda_context_set_walk": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_opening": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_set_relative_opening": (st, [vp, C.c_double, pe]),
+        "n_body_sim_pro_cuda_context_set_relative_source": (st, [vp, C.c_int, pe]),
         "n_body_sim_pro_cuda_context_stats": (C.c_int, [vp, C.POINTER(BarnesHutStats)]),
         "n_body_sim_pro_cuda_context_timings": (C.c_int, [vp, C.POINTER(Timings)]),
         "n_body_sim_pro_cuda_context_walk_restarts": (C.c_size_t, [vp]),
@@ -463,6 +472,14 @@ class CudaContext:
         err = Error()
         _check(library().n_body_sim_pro_cuda_context_set_relative_opening(
             self.handle, float(alpha), C.byref(err)), err)
+
+    def set_relative_source(self, source: int) -> None:
+        """Where the plugin functions take the relative test's previous
+        accelerations: RelativeSource.FROM_VIEW (default) or FROM_CONTEXT (this
+        context's previous plugin result, kept on the device)."""
+        err = Error()
+        _check(library().n_body_sim_pro_cuda_context_set_relative_source(
+            self.handle, int(source), C.byref(err)), err)
 
     def set_correction(self, correction: "CudaCorrection | None") -> None:
         err = Error()

@@ -108,6 +108,11 @@ struct NBodySimProCudaContext {
     int walk_mode;
     int opening;
     double tolerance; /* alpha of the relative opening test; 0: off */
+    int relative_source; /* NBodySimProCudaRelativeSource */
+    /* the last plugin call's result, still in ax/ay/az: its particle count and
+     * the view's acceleration array it was copied to (0 / NULL: none) */
+    size_t history_n;
+    const double* history_ax;
     const void* correction; /* device network of the learned correction, or NULL */
     int tree_quadrupoles; /* the next build keeps every cell's quadrupole (training reads them) */
     NbspBarnesHut* bh;
@@ -260,6 +265,17 @@ NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_opening(NBodySimProCu
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
                     "relative opening tolerance must be finite and >= 0");
     c->tolerance = alpha;
+    return N_BODY_SIM_PRO_STATUS_OK;
+}
+
+NBodySimProStatus n_body_sim_pro_cuda_context_set_relative_source(NBodySimProCudaContext* c,
+                                                                 int source,
+                                                                 NBodySimProError* error) {
+    if (c == NULL) return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "context must not be null");
+    if (source != N_BODY_SIM_PRO_CUDA_RELATIVE_FROM_VIEW &&
+        source != N_BODY_SIM_PRO_CUDA_RELATIVE_FROM_CONTEXT)
+        return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT, "unknown relative-test source");
+    c->relative_source = source;
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
@@ -614,12 +630,21 @@ static NBodySimProStatus view_force(const NBodySimProParticleSystemView* view,
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t n = view->particle_count;
     if (n == 0) return N_BODY_SIM_PRO_STATUS_OK;
+    /* Every other call that writes ax/ay/az needs or makes a resident state,
+     * so with none since the last plugin call its result is still there. */
+    const int reuse = algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT &&
+                      c->tolerance > 0.0 &&
+                      c->relative_source == N_BODY_SIM_PRO_CUDA_RELATIVE_FROM_CONTEXT &&
+                      !c->resident && c->history_n == n &&
+                      c->history_ax == view->accelerations_x;
+    c->history_n = 0;
+    c->history_ax = NULL;
     if ((st = ensure_capacity(c, n, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
     c->n = n;
     c->n_padded = round_up(n, 256);
     c->resident = 0; /* the plugin path only stages positions and masses */
     if ((st = copy_in(c, view, 0, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
-    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && c->tolerance > 0.0) {
+    if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT && c->tolerance > 0.0 && !reuse) {
         /* the relative opening test reads the view's previous accelerations */
         const size_t bytes = n * sizeof(double);
         double* dst[3] = {c->ax, c->ay, c->az};
@@ -639,6 +664,8 @@ static NBodySimProStatus view_force(const NBodySimProParticleSystemView* view,
     CUDA_TRY(cudaEventRecord(c->events[1], c->stream));
     if ((st = copy_accelerations_out(c, view, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
     if ((st = check_device_status(c, error)) != N_BODY_SIM_PRO_STATUS_OK) return st;
+    c->history_n = n;
+    c->history_ax = view->accelerations_x;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->events[0], c->events[1]);
     if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_ALL_PAIRS) {

@@ -174,11 +174,16 @@ __device__ __forceinline__ uint64_t spread3(uint64_t v) {
 // runs out.
 // ---------------------------------------------------------------------------
 
-constexpr int kSortThreads = 256;
+// 512 threads of 8 keys: twice the warps of 256 x 16 at the same tile (the
+// ranking chain per warp is half as long); at 10M keys 0.92 ms for the 8
+// passes against 1.10 with 256 x 16 (and 1.17 with 1024 x 4, one block per SM)
+constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
 constexpr int kRadix = 256;
+constexpr int kLookback = 8;  // predecessors' flags read at once in the look-back
+static_assert(kSortThreads >= kRadix, "one thread per digit");
 constexpr int kSortPasses = 8;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kCountMask = (1u << 30) - 1u;
 constexpr int kLookbackSpins = 1 << 22;  // ~ms per predecessor before the error flag
@@ -311,11 +316,15 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(
   uint32_t val[kSortItems];
   uint32_t rank[kSortItems];
 #pragma unroll
-  for (int it = 0; it < kSortItems; ++it) {
+  for (int it = 0; it < kSortItems; ++it) {  // every load of the tile in flight at once
     const size_t i = base_i + (size_t)it * 32 + lane;
     const bool valid = i < n;
     key[it] = valid ? keys_in[i] : 0ull;
     val[it] = valid ? vals_in[i] : 0u;
+  }
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const bool valid = base_i + (size_t)it * 32 + lane < n;
     const unsigned digit = valid ? ((unsigned)(key[it] >> shift) & 0xffu) : 0x100u;
     const unsigned peers = __match_any_sync(kFull, digit);
     uint32_t before = 0;
@@ -326,54 +335,63 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(
     rank[it] = before + __popc(peers & lt);
   }
   __syncthreads();
-  uint32_t count;  // this tile's keys with digit t
-  {
+  // threads t < 256: digit t — this tile's count, publish, look back, and the
+  // exclusive scan of the tile's digit totals (warp shuffles, then warp sums)
+  __shared__ uint32_t s_wsum[kRadix / 32];
+  if (t < kRadix) {
     uint32_t run = 0;
     for (int ww = 0; ww < kSortWarps; ++ww) {
       const uint32_t c = wc[ww * kRadix + t];
       wc[ww * kRadix + t] = run;
       run += c;
     }
-    start[t] = run;
-    count = run;
-  }
-  // publish, then look back for the keys with digit t in all earlier tiles
-  uint32_t* st = status + (size_t)tile * kRadix + t;
-  atomicExch(st, (tile == 0 ? kFlagP : kFlagA) | count);
-  uint32_t prefix = 0;
-  if (tile > 0) {
-    int j = tile - 1;
-    int spins = 0;
-    while (j >= 0) {
-      const uint32_t v = load_volatile(status + (size_t)j * kRadix + t);
-      const uint32_t flag = v & ~kCountMask;
-      if (flag == 0u) {
-        if (++spins > kLookbackSpins) {
+    const uint32_t count = run;  // this tile's keys with digit t
+    uint32_t* st = status + (size_t)tile * kRadix + t;
+    atomicExch(st, (tile == 0 ? kFlagP : kFlagA) | count);
+    uint32_t prefix = 0;
+    if (tile > 0) {
+      // kLookback predecessors at a time, nearest first: counts are added up
+      // to the first unpublished flag (read again) or the first inclusive one
+      int j = tile - 1, spins = 0;
+      for (;;) {
+        uint32_t v[kLookback];
+#pragma unroll
+        for (int k = 0; k < kLookback; ++k)
+          v[k] = j - k >= 0 ? load_volatile(status + (size_t)(j - k) * kRadix + t) : kFlagP;
+        int used = 0;
+        bool done = false;
+#pragma unroll
+        for (int k = 0; k < kLookback; ++k) {
+          if (done || used < k) continue;
+          const uint32_t flag = v[k] & ~kCountMask;
+          if (flag == 0u) continue;
+          prefix += v[k] & kCountMask;
+          used = k + 1;
+          if (flag == kFlagP) done = true;
+        }
+        if (done) break;
+        if (used == 0 && ++spins > kLookbackSpins) {
           atomicOr(err, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
           break;
         }
-        continue;
+        j -= used;
       }
-      prefix += v & kCountMask;
-      if (flag == kFlagP) break;
-      --j;
+      atomicExch(st, kFlagP | ((prefix + count) & kCountMask));
     }
-    atomicExch(st, kFlagP | ((prefix + count) & kCountMask));
-  }
-  gofs[t] = base[t] + prefix;
-  __syncthreads();
-  {  // exclusive scan of the tile's digit totals: warp shuffles, then the warp sums
-    __shared__ uint32_t s_wsum[kSortWarps];
-    uint32_t v = count;
+    gofs[t] = base[t] + prefix;
+    uint32_t x = count;
     for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t u = __shfl_up_sync(kFull, v, off);
-      if (lane >= off) v += u;
+      const uint32_t u = __shfl_up_sync(kFull, x, off);
+      if (lane >= off) x += u;
     }
-    if (lane == 31) s_wsum[w] = v;
-    __syncthreads();
+    if (lane == 31) s_wsum[w] = x;
+    start[t] = x - count;
+  }
+  __syncthreads();
+  if (t < kRadix) {
     uint32_t before = 0;
     for (int k = 0; k < w; ++k) before += s_wsum[k];
-    start[t] = before + v - count;
+    start[t] += before;
   }
   __syncthreads();
 #pragma unroll

@@ -97,6 +97,8 @@ def test_context_setters_validate_without_a_device():
         nb.Status.INVALID_ARGUMENT
     assert L.n_body_sim_pro_cuda_context_set_relative_opening(None, 0.01, C.byref(err)) == \
         nb.Status.INVALID_ARGUMENT
+    assert L.n_body_sim_pro_cuda_context_set_relative_source(None, 1, C.byref(err)) == \
+        nb.Status.INVALID_ARGUMENT
     assert L.n_body_sim_pro_cuda_context_stats(None, None) != 0
     assert L.n_body_sim_pro_cuda_context_theta(None) == 0.0
 

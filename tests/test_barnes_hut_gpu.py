@@ -388,6 +388,62 @@ def test_relative_opening_reads_the_views_accelerations(cuda):
     assert np.array_equal(b, a0)
 
 
+def test_relative_source_from_context_saves_the_upload(cuda):
+    """FROM_CONTEXT: the plugin function takes the previous accelerations from
+    the context's last result instead of uploading the view's.  Under a host
+    leapfrog that passes the result back unchanged (integrator.c:47-85) the
+    forces are bit-equal to FROM_VIEW's; the view's values are not read while
+    the context's result is current, and they are again after a different
+    acceleration array or a device-resident call."""
+    p = O.preset("plummer_collision", 100000, 42)
+    g = cuda.gravity_init(1.0, 0.01)
+    h, dt = 5e-4, 1e-3
+    systems, ctxs = [], []
+    for source in (cuda.RelativeSource.FROM_VIEW, cuda.RelativeSource.FROM_CONTEXT):
+        c = cuda.CudaContext(theta=1.0, leaf_capacity=32, relative_opening=0.003)
+        c.set_relative_source(source)
+        ctxs.append(c)
+        systems.append(to_system(cuda, p))
+    try:
+        for s, c in zip(systems, ctxs):
+            cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, c)
+        for step in range(3):
+            for s, c in zip(systems, ctxs):
+                for v, a in ((s.vx, s.ax), (s.vy, s.ay), (s.vz, s.az)):
+                    v += h * a
+                for x, v in ((s.x, s.vx), (s.y, s.vy), (s.z, s.vz)):
+                    x += dt * v
+                cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(s, g, c)
+                for v, a in ((s.vx, s.ax), (s.vy, s.ay), (s.vz, s.az)):
+                    v += h * a
+            assert np.array_equal(systems[0].acc(), systems[1].acc()), step
+        (sv, cv), (sc, cc) = zip(systems, ctxs)
+        again = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(sv, g, cv).copy()
+        for a in (sc.ax, sc.ay, sc.az):
+            a[:] = 0.0  # not read: the context's last result is current
+        assert np.array_equal(
+            cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(sc, g, cc), again)
+        # another acceleration array (zeros): the view's are read, a fresh start
+        fresh = to_system(cuda, p)
+        for f in ("x", "y", "z", "m"):
+            getattr(fresh, f)[:] = getattr(sc, f)
+        start = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(fresh, g, cc).copy()
+        with cuda.CudaContext(theta=0.5, leaf_capacity=32) as plain:
+            ref = cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(fresh, g, plain).copy()
+        assert np.array_equal(start, ref)
+        # a device-resident call in between: the view's are read again
+        cc.upload(fresh)
+        for a in (fresh.ax, fresh.ay, fresh.az):
+            a[:] = 0.0
+        assert np.array_equal(
+            cuda.n_body_sim_pro_barnes_hut_compute_acceleration_cuda(fresh, g, cc), ref)
+        with pytest.raises(cuda.CudaError):
+            cc.set_relative_source(2)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_opening_argument_checked(cuda, ctx):
     with pytest.raises(cuda.CudaError):
         ctx.set_opening(2)
