@@ -939,8 +939,12 @@ __device__ __forceinline__ void swap_if_greater(int& a, int& b) {
 // writes the sorted list back for the interaction-list walk.
 // QUAD: also the trace-free quadrupoles and the spread (the quadrupole walk,
 // the correction's features); the monopole walk reads neither.
+// Monopole pass at 6 blocks per SM (40 registers, a few spilled to L1): it is
+// bound by the latency of its loads and of the climb, and the extra warps hide
+// more of it (0.246 -> 0.228 ms at 10M); the quadrupole pass is left to the
+// compiler (its moments would spill hundreds of bytes per thread at 40 or 64)
 template <bool QUAD>
-__global__ void __launch_bounds__(256) moments_kernel(const float4* __restrict__ pos, Tree t,
+__global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4* __restrict__ pos, Tree t,
                                                       Opening open, int* status) {
   const int total = (int)t.offset[t.n];
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < total;
