@@ -789,8 +789,8 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
         # 8 LSD passes over (key 8 + index 4), read and written
         ("sort", "sort_ms", 8 * 24.0 * n),
         ("moments", "moments_ms", mom_bytes),
-        # unsort: inverse index 4 + one 32-byte double4 read, ax/ay/az 24 written
-        ("unsort", "integrate_ms", 60.0 * n),
+        # unsort: the walk's double4 (32 B, input order) read, ax/ay/az 24 written
+        ("unsort", "integrate_ms", 56.0 * n),
     ]
     stages = {}
     for name, key, nbytes in rows:
@@ -816,7 +816,7 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
                        "particle: bounds 32 (+24 relative), keys 32 read + 28 written (+28 "
                        "relative), sort 8 passes x (12 + 12), moments "
                        + ("2 x 16 + 264 per node" if quad else "16 + 116 per node")
-                       + ", unsort 4 + 32 read + 24 written, kick-drift 120 + kick 72")
+                       + ", unsort 32 read + 24 written, kick-drift 120 + kick 72")
     return stages
 
 

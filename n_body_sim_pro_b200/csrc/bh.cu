@@ -187,7 +187,7 @@ static_assert(kSortThreads >= kRadix, "one thread per digit");
 constexpr int kSortPasses = 8;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kCountMask = (1u << 30) - 1u;
 constexpr int kLookbackSpins = 1 << 22;  // ~ms per predecessor before the error flag
-constexpr int kKeysBlocks = 2 * 148;
+constexpr int kKeysBlocks = 4 * 148;  // 32 warps per SM: enough loads in flight for HBM
 
 // Sort scratch (32-bit words): hist[8][256] | base[8][256] | ticket[8] | status[8][tiles][256]
 struct SortScratch {
@@ -459,13 +459,12 @@ __global__ void duplicates_kernel(const uint64_t* __restrict__ keys,
 // gather / scatter
 // ---------------------------------------------------------------------------
 
-// pos[s] = unsorted[perm[s]]; inverse[perm[s]] = s (for the unsort); the
-// relative opening test's tolerances the same way when present.
+// pos[s] = unsorted[perm[s]]; the relative opening test's tolerances the same
+// way when present.
 __global__ void gather_kernel(const float4* __restrict__ unsorted,
                               const uint32_t* __restrict__ perm, size_t n,
-                              float4* __restrict__ pos, uint32_t* __restrict__ inverse,
-                              const float* __restrict__ unsorted_tol, float* __restrict__ tol,
-                              int* status) {
+                              float4* __restrict__ pos, const float* __restrict__ unsorted_tol,
+                              float* __restrict__ tol, int* status) {
   for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < n;
        s += (size_t)gridDim.x * blockDim.x) {
     const uint32_t i = perm[s];
@@ -475,20 +474,18 @@ __global__ void gather_kernel(const float4* __restrict__ unsorted,
       continue;
     }
     pos[s] = unsorted[i];
-    inverse[i] = (uint32_t)s;
     if (tol != nullptr) tol[s] = unsorted_tol[i];
   }
 }
 
-// a[i] = G * acc[inverse[i]]: random 32-byte reads, coalesced FP64 writes.
-__global__ void unsort_kernel(const double4* __restrict__ acc, const uint32_t* __restrict__ inverse,
-                              size_t n, double g, double* __restrict__ ax,
-                              double* __restrict__ ay, double* __restrict__ az) {
+// a[i] = G * acc[i]: the walk wrote each target's sum at its input index
+// (one aligned 32-byte record), so this pass is coalesced both ways.
+__global__ void unsort_kernel(const double4* __restrict__ acc, size_t n, double g,
+                              double* __restrict__ ax, double* __restrict__ ay,
+                              double* __restrict__ az) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t s = inverse[i];
-    if (s >= n) continue;  // only after the gather flagged a bad permutation
-    const double4 a = acc[s];
+    const double4 a = acc[i];
     ax[i] = g * a.x;
     ay[i] = g * a.y;
     az[i] = g * a.z;
@@ -958,13 +955,21 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
     Moments mo;
     {
       double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-#pragma unroll 4
-      for (int j = info.y; j < info.y + info.z; ++j) {
-        const float4 p = pos[j];
-        m += (double)p.w;
-        sx += (double)p.w * (double)p.x;
-        sy += (double)p.w * (double)p.y;
-        sz += (double)p.w * (double)p.z;
+      // eight particles' loads in flight at once (padding adds exact zeros, so
+      // the sums are those of the plain sequential loop)
+      const int end = info.y + info.z;
+      for (int j0 = info.y; j0 < end; j0 += 8) {
+        float4 q[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          q[k] = j0 + k < end ? pos[j0 + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          m += (double)q[k].w;
+          sx += (double)q[k].w * (double)q[k].x;
+          sy += (double)q[k].w * (double)q[k].y;
+          sz += (double)q[k].w * (double)q[k].z;
+        }
       }
       mo.m = m;
       mo.cx = m != 0.0 ? sx / m : (double)pos[info.y].x;
@@ -1227,13 +1232,20 @@ __device__ __forceinline__ void stackless_walk(const float4* __restrict__ pos, i
   out.exact = exact;
 }
 
-// The compensated (hi, lo) sums combined in FP64, in Morton order.
+// The compensated (hi, lo) sums combined in FP64, stored at the target's input
+// index perm[s]: one aligned 32-byte record per target, so the scattered store
+// writes whole sectors and the pass that scales them into the state's arrays is
+// coalesced.
 __device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active, int lane,
+                                           const uint32_t* __restrict__ perm, int n,
                                            double4* __restrict__ acc,
                                            unsigned long long* __restrict__ counters) {
-  if (active)
-    acc[s] = make_double4((double)a.hx + (double)a.lx, (double)a.hy + (double)a.ly,
-                          (double)a.hz + (double)a.lz, 0.0);
+  if (active) {
+    const uint32_t i = perm[s];
+    if (i < (uint32_t)n)  // (a bad permutation is flagged by the gather)
+      acc[i] = make_double4((double)a.hx + (double)a.lx, (double)a.hy + (double)a.ly,
+                            (double)a.hz + (double)a.lz, 0.0);
+  }
   unsigned long long ap = a.approx, ex = a.exact;
   for (int off = 16; off > 0; off >>= 1) {
     ap += __shfl_down_sync(kFull, ap, off);
@@ -1248,7 +1260,8 @@ __device__ __forceinline__ void store_walk(const WalkAcc& a, int s, bool active,
 template <int ORDER, bool REL>
 __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
-    double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status) {
+    const uint32_t* __restrict__ perm, double4* __restrict__ acc,
+    unsigned long long* __restrict__ counters, int* status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kWalkThreads + threadIdx.x) >> 5;
   if (warp * 32 >= n) return;
@@ -1258,7 +1271,7 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(
   const float tl = REL ? tol[active ? s : n - 1] : 0.f;
   WalkAcc a;
   stackless_walk<ORDER, REL>(pos, n, t, eps2, s, active, p, tl, lane, status, a);
-  store_walk(a, s, active, lane, acc, counters);
+  store_walk(a, s, active, lane, perm, n, acc, counters);
 }
 
 // Point sources (bucket particles and monopole cells) gathered per warp in
@@ -1772,7 +1785,8 @@ static_assert(kCtaStack + kFrontier <= 3 * kListStack, "frontier inside warp 2's
 template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED = false>
 __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
-    double4* __restrict__ acc, unsigned long long* __restrict__ counters, int* status,
+    const uint32_t* __restrict__ perm, double4* __restrict__ acc,
+    unsigned long long* __restrict__ counters, int* status,
     const nbsp_mlp::Net* __restrict__ net, NbspCorrectionLists lists) {
   static_assert(!SHARED || (ORDER == 1 && !CORR && STACK == kListStack), "shared top: monopole walk");
   __shared__ int s_stack[kListThreads / 32][STACK];
@@ -2217,7 +2231,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
     a.approx = approx;
     a.exact = exact;
   }
-  store_walk(a, s, active, lane, acc, counters);
+  store_walk(a, s, active, lane, perm, n, acc, counters);
 }
 
 // ---- the correction pipeline after a corrected walk ------------------------
@@ -2360,6 +2374,7 @@ __global__ void __launch_bounds__(nbsp_umma::kThreads) corr_rows_kernel(
 
 __global__ void __launch_bounds__(128) corr_apply_kernel(const float4* __restrict__ pos, int n,
                                                          Tree t, NbspCorrectionLists lists,
+                                                         const uint32_t* __restrict__ perm,
                                                          double4* __restrict__ acc) {
   const int lane = threadIdx.x & 31;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -2399,12 +2414,15 @@ __global__ void __launch_bounds__(128) corr_apply_kernel(const float4* __restric
     fold(hy, ly, ay);
     fold(hz, lz, az);
   }
-  if (active && cnt > 0) {
-    double4 a = acc[s];
-    a.x += (double)hx + (double)lx;
-    a.y += (double)hy + (double)ly;
-    a.z += (double)hz + (double)lz;
-    acc[s] = a;
+  if (active && cnt > 0) {  // the walk stored the target at its input index
+    const uint32_t i = perm[s];
+    if (i < (uint32_t)n) {
+      double4 a = acc[i];
+      a.x += (double)hx + (double)lx;
+      a.y += (double)hy + (double)ly;
+      a.z += (double)hz + (double)lz;
+      acc[i] = a;
+    }
   }
 }
 
@@ -2425,32 +2443,33 @@ int grid_for(size_t n, int threads) {
 template <bool REL>
 void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order, int mode,
                  const nbsp_mlp::Net* net, const NbspCorrectionLists* lists, float eps2,
-                 double4* out, unsigned long long* counters, int* status, cudaStream_t stream) {
+                 const uint32_t* perm, double4* out, unsigned long long* counters, int* status,
+                 cudaStream_t stream) {
   if (mode == NBSP_BH_WALK_LISTS || mode == NBSP_BH_WALK_SHARED || net != nullptr) {
     const unsigned blocks = (unsigned)((n + kListThreads - 1) / kListThreads);
     NbspCorrectionLists none{};
     if (net != nullptr && lists != nullptr) {  // the network corrects the monopole term
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, true, REL><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, net, *lists);
+          p, tol, (int)n, t, eps2, perm, out, counters, status, net, *lists);
     } else if (order == 1 && mode == NBSP_BH_WALK_SHARED) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL, true><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
+          p, tol, (int)n, t, eps2, perm, out, counters, status, nullptr, none);
     } else if (order == 2) {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
+          p, tol, (int)n, t, eps2, perm, out, counters, status, nullptr, none);
     } else {
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
-          p, tol, (int)n, t, eps2, out, counters, status, nullptr, none);
+          p, tol, (int)n, t, eps2, perm, out, counters, status, nullptr, none);
     }
     return;
   }
   const unsigned blocks = (unsigned)((n + kWalkThreads - 1) / kWalkThreads);
   if (order == 2) {
     NBSP_COUNT_LAUNCH(1), walk_kernel<2, REL><<<blocks, kWalkThreads, 0, stream>>>(
-        p, tol, (int)n, t, eps2, out, counters, status);
+        p, tol, (int)n, t, eps2, perm, out, counters, status);
   } else {
     NBSP_COUNT_LAUNCH(1), walk_kernel<1, REL><<<blocks, kWalkThreads, 0, stream>>>(
-        p, tol, (int)n, t, eps2, out, counters, status);
+        p, tol, (int)n, t, eps2, perm, out, counters, status);
   }
 }
 
@@ -2518,10 +2537,9 @@ void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, const double
 }
 
 void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
-                    uint32_t* inverse, const float* unsorted_tol, float* tol, int* status,
-                    cudaStream_t stream) {
+                    const float* unsorted_tol, float* tol, int* status, cudaStream_t stream) {
   NBSP_COUNT_LAUNCH(1), gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
-      (const float4*)unsorted, perm, n, (float4*)pos4, inverse, unsorted_tol, tol, status);
+      (const float4*)unsorted, perm, n, (float4*)pos4, unsorted_tol, tol, status);
 }
 
 size_t nbsp_bh_tree_bytes(size_t n) { return tree_bytes(n); }
@@ -2571,21 +2589,23 @@ void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const dou
 
 void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree, int order,
                   int mode, const void* correction, const NbspCorrectionLists* lists, float eps2,
-                  void* acc, unsigned long long* counters, int* status, cudaStream_t stream) {
+                  const uint32_t* perm, void* acc, unsigned long long* counters, int* status,
+                  cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
   const float4* p = (const float4*)pos4;
   double4* out = (double4*)acc;
   if (tol != nullptr)
-    launch_walk<true>(p, tol, n, t, order, mode, net, lists, eps2, out, counters, status, stream);
+    launch_walk<true>(p, tol, n, t, order, mode, net, lists, eps2, perm, out, counters, status,
+                      stream);
   else
-    launch_walk<false>(p, nullptr, n, t, order, mode, net, lists, eps2, out, counters, status,
-                       stream);
+    launch_walk<false>(p, nullptr, n, t, order, mode, net, lists, eps2, perm, out, counters,
+                       status, stream);
 }
 
 void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* correction,
-                     const NbspCorrectionLists* lists, void* acc, unsigned long long* counters,
-                     int* status, cudaStream_t stream) {
+                     const NbspCorrectionLists* lists, const uint32_t* perm, void* acc,
+                     unsigned long long* counters, int* status, cudaStream_t stream) {
   Tree t = tree_view(const_cast<void*>(tree), n);
   const nbsp_mlp::Net* net = (const nbsp_mlp::Net*)correction;
   const int groups = (int)((n + 31) / 32);
@@ -2598,13 +2618,13 @@ void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* c
   NBSP_COUNT_LAUNCH(1), corr_rows_kernel<<<148 * nbsp_umma::kCtasPerSm, nbsp_umma::kThreads, smem, stream>>>(
       net, t, *lists, groups, status);
   NBSP_COUNT_LAUNCH(1), corr_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
-      (const float4*)pos4, (int)n, t, *lists, (double4*)acc);
+      (const float4*)pos4, (int)n, t, *lists, perm, (double4*)acc);
 }
 
-void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n, double g, double* ax,
-                    double* ay, double* az, cudaStream_t stream) {
+void nbsp_bh_unsort(const void* acc, size_t n, double g, double* ax, double* ay, double* az,
+                    cudaStream_t stream) {
   NBSP_COUNT_LAUNCH(1), unsort_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
-      (const double4*)acc, inverse, n, g, ax, ay, az);
+      (const double4*)acc, n, g, ax, ay, az);
 }
 
 void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta, int opening,

@@ -114,10 +114,10 @@ NBSP_HIDDEN void nbsp_bh_duplicates(const uint64_t* keys, const uint32_t* perm, 
                                     const double* y, const double* z, size_t n, int* status,
                                     cudaStream_t stream);
 
-/* pos4[s] = unsorted[perm[s]] (Morton order); inverse[perm[s]] = s. */
+/* pos4[s] = unsorted[perm[s]] (Morton order), tol[s] = unsorted_tol[perm[s]]. */
 NBSP_HIDDEN void nbsp_bh_gather(const void* unsorted, const uint32_t* perm, size_t n, void* pos4,
-                                uint32_t* inverse, const float* unsorted_tol, float* tol,
-                                int* status, cudaStream_t stream);
+                                const float* unsorted_tol, float* tol, int* status,
+                                cudaStream_t stream);
 
 /* Device-side layout of the tree build scratch; sized by nbsp_bh_tree_bytes. */
 NBSP_HIDDEN size_t nbsp_bh_tree_bytes(size_t n);
@@ -166,9 +166,10 @@ typedef struct NbspCorrectionLists {
 NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, const void* tree,
                               int order, int mode, const void* correction,
                               const NbspCorrectionLists* lists, float softening_squared,
-                              void* acc, unsigned long long* counters, int* status,
-                              cudaStream_t stream);
-/* (tol != NULL: every opening test also takes the relative test with the
+                              const uint32_t* perm, void* acc, unsigned long long* counters,
+                              int* status, cudaStream_t stream);
+/* (acc: one double4 per particle, stored at the target's input index perm[s];
+ * tol != NULL: every opening test also takes the relative test with the
  * per-target tolerances tol, Morton order; correction != NULL: the monopole
  * walk lists cells into `lists` for nbsp_bh_correct) */
 
@@ -176,8 +177,8 @@ NBSP_HIDDEN void nbsp_bh_walk(const void* pos4, const float* tol, size_t n, cons
  * tcgen05 tensor cores and the corrections added to the walk's result acc. */
 NBSP_HIDDEN void nbsp_bh_correct(const void* pos4, size_t n, const void* tree,
                                  const void* correction, const NbspCorrectionLists* lists,
-                                 void* acc, unsigned long long* counters, int* status,
-                                 cudaStream_t stream);
+                                 const uint32_t* perm, void* acc, unsigned long long* counters,
+                                 int* status, cudaStream_t stream);
 
 /* Learned correction: training pairs (target, accepted cell) sampled with the
  * opening criterion `opening` at theta, their features and exact-sum labels, and
@@ -215,10 +216,10 @@ NBSP_HIDDEN const void* nbsp_correction_net(const NBodySimProCudaCorrection* cor
 NBSP_HIDDEN const void* nbsp_bh_positions(const NbspBarnesHut* bh);
 NBSP_HIDDEN const void* nbsp_bh_tree(const NbspBarnesHut* bh);
 
-/* a[i] = G * acc[inverse[i]] (acc: double4 per target in Morton order) */
-NBSP_HIDDEN void nbsp_bh_unsort(const void* acc, const uint32_t* inverse, size_t n,
-                                double gravitational_constant, double* ax, double* ay,
-                                double* az, cudaStream_t stream);
+/* a[i] = G * acc[i] (acc: double4 per particle in input order, as the walk
+ * stores it) */
+NBSP_HIDDEN void nbsp_bh_unsort(const void* acc, size_t n, double gravitational_constant,
+                                double* ax, double* ay, double* az, cudaStream_t stream);
 
 /* Copy node_count, leaf_count and depth of the tree to counters[2..4]. */
 NBSP_HIDDEN void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,

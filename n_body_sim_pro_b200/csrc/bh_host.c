@@ -28,9 +28,8 @@ struct NbspBarnesHut {
     uint32_t* hist;
     void* pos4;
     void* tree;
-    void* acc;          /* double4 per target, Morton order */
+    void* acc;          /* double4 per target, input order (the walk stores at perm[s]) */
     void* unsorted;     /* float4 positions in input order */
-    uint32_t* inverse;  /* Morton slot of each input particle */
     float* tol_unsorted; /* relative opening test: tolerance per particle, input order */
     float* tol;          /* the same in Morton order */
     NbspCorrectionLists lists;          /* corrected walk (allocated on first use) */
@@ -98,15 +97,14 @@ static NBodySimProStatus ensure_lists(NbspBarnesHut* b, size_t n, NBodySimProErr
 
 static void release_buffers(NbspBarnesHut* b) {
     void* buffers[] = {b->partial, b->geometry, b->keys, b->keys_alt, b->index, b->index_alt,
-                       b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->inverse,
-                       b->tol_unsorted, b->tol};
+                       b->hist, b->pos4, b->tree, b->acc, b->unsorted, b->tol_unsorted,
+                       b->tol};
     for (size_t k = 0; k < sizeof(buffers) / sizeof(buffers[0]); ++k) cudaFree(buffers[k]);
     b->partial = b->geometry = NULL;
     b->keys = b->keys_alt = NULL;
     b->index = b->index_alt = NULL;
     b->hist = NULL;
     b->pos4 = b->tree = b->acc = b->unsorted = NULL;
-    b->inverse = NULL;
     b->tol_unsorted = b->tol = NULL;
     b->capacity = 0;
 }
@@ -149,7 +147,6 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
     BH_TRY(cudaMalloc(&b->tree, nbsp_bh_tree_bytes(cap)));
     BH_TRY(cudaMalloc(&b->acc, cap * 32));
     BH_TRY(cudaMalloc(&b->unsorted, cap * 16));
-    BH_TRY(cudaMalloc((void**)&b->inverse, cap * sizeof(uint32_t)));
     BH_TRY(cudaMalloc((void**)&b->tol_unsorted, cap * sizeof(float)));
     BH_TRY(cudaMalloc((void**)&b->tol, cap * sizeof(float)));
     b->capacity = cap;
@@ -199,7 +196,7 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     const int rel = tol_scale > 0.0;
     morton(b, s, tol_scale, status, stream);
     nbsp_bh_duplicates(b->keys, b->index, s->x, s->y, s->z, n, status, stream);
-    nbsp_bh_gather(b->unsorted, b->index, n, b->pos4, b->inverse, rel ? b->tol_unsorted : NULL,
+    nbsp_bh_gather(b->unsorted, b->index, n, b->pos4, rel ? b->tol_unsorted : NULL,
                    rel ? b->tol : NULL, status, stream);
     nbsp_bh_build(b->keys, n, p->leaf_capacity, b->tree, status, stream);
     cudaEventRecord(b->events[4], stream);
@@ -210,13 +207,12 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
     cudaEventRecord(b->events[5], stream);
     nbsp_bh_walk(b->pos4, rel ? b->tol : NULL, n, b->tree, p->multipole_order, p->walk_mode,
                  p->correction, p->correction != NULL ? &b->lists : NULL,
-                 (float)p->softening_squared, b->acc, b->counters, status, stream);
+                 (float)p->softening_squared, b->index, b->acc, b->counters, status, stream);
     if (p->correction != NULL)
-        nbsp_bh_correct(b->pos4, n, b->tree, p->correction, &b->lists, b->acc, b->counters,
-                        status, stream);
+        nbsp_bh_correct(b->pos4, n, b->tree, p->correction, &b->lists, b->index, b->acc,
+                        b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
-    nbsp_bh_unsort(b->acc, b->inverse, n, p->gravitational_constant, s->ax, s->ay, s->az,
-                   stream);
+    nbsp_bh_unsort(b->acc, n, p->gravitational_constant, s->ax, s->ay, s->az, stream);
     nbsp_bh_tree_counts(b->tree, n, b->counters, stream);
     cudaEventRecord(b->events[7], stream);
     BH_TRY(cudaGetLastError());
