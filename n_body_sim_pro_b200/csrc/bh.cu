@@ -501,11 +501,10 @@ __global__ void unsort_kernel(const double4* __restrict__ acc, size_t n, double 
 struct Tree {
   int n;
   int2* range;        // [n-1] first, last of internal nodes
-  int2* child;        // [n-1] binary ids
+  int2* child;        // [n-1] binary ids of the two children
   int* delta;         // [n-1] common prefix length in bits
   int* parent;        // [2n-1] binary parent id (root: -1)
   int* cell;          // [2n-1] octree level of a cell node, -1 otherwise
-  int* kept;          // [2n-1] 1 if the node is in the bucketed octree
   int* oparent;       // [2n-1] octree parent (binary id) of a cell node, from keep_kernel
   uint32_t* mask;     // [n]   levels of kept nodes starting at particle k
   uint32_t* offset;   // [n+1] exclusive scan of popcounts; offset[n] = node count
@@ -551,7 +550,6 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.delta = carve<int>(p, ni);
   t.parent = carve<int>(p, nb);
   t.cell = carve<int>(p, nb);
-  t.kept = carve<int>(p, nb);
   t.oparent = carve<int>(p, nb);
   t.mask = carve<uint32_t>(p, n);
   t.offset = carve<uint32_t>(p, n + 1);
@@ -663,43 +661,81 @@ __device__ __forceinline__ int last_of(const Tree& t, int b) {
   return b < t.n - 1 ? t.range[b].y : b - (t.n - 1);
 }
 
-// Octree parent of a cell node: the nearest binary ancestor that is a cell.
-__device__ __forceinline__ int octree_parent(const Tree& t, int b, int* status) {
-  int p = t.parent[b];
-  for (int guard = 0; p >= 0 && t.cell[p] < 0; ++guard) {
-    if (guard > 96 || p >= t.n - 1) {
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-      return -1;
-    }
-    p = t.parent[p];
-  }
-  if (p >= t.n - 1) {
-    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-    return -1;
-  }
-  return p;
+// A splitting cell: an octree cell (binary node b with cell level >= 0) of
+// more than leaf_capacity particles above level 21 — an internal node of the
+// bucketed octree, whose octree children are all kept.  (A cell is kept when
+// its octree parent splits; the root always is.)
+__device__ __forceinline__ bool splits(const Tree& t, int b, int leaf_capacity) {
+  if (b >= t.n - 1) return false;  // a particle
+  const int lvl = t.cell[b];
+  if (lvl < 0 || lvl >= 21) return false;
+  const int2 r = t.range[b];
+  return r.y - r.x + 1 > leaf_capacity;
 }
 
+// The octree children of splitting cell b, in Morton order: the cells met
+// first below b in the binary tree.  The binary nodes passed on the way have
+// b's own level (they are not cells), at most 7 of them, so the descent is a
+// stack of at most 8 entries; visit(c) is called for each child cell c.
+template <typename Visit>
+__device__ __forceinline__ int octree_children(const Tree& t, int b, int* status, Visit visit) {
+  int stack[8];
+  int top = 0, kids = 0;
+  const int2 c0 = t.child[b];
+  stack[top++] = c0.y;  // right pushed first: the left subtree is visited first
+  stack[top++] = c0.x;
+  for (int guard = 0; top > 0; ++guard) {
+    const int c = stack[--top];
+    if (guard > 16 || c < 0 || c >= 2 * t.n - 1) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return kids;
+    }
+    if (t.cell[c] >= 0) {
+      if (kids == 8) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+        return kids;
+      }
+      visit(c, kids++);
+    } else if (c < t.n - 1 && top <= 6) {  // a binary node at b's level: its children
+      const int2 cc = t.child[c];
+      stack[top++] = cc.y;
+      stack[top++] = cc.x;
+    } else {  // a particle that is no cell, or a descent deeper than one octree level
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return kids;
+    }
+  }
+  return kids;
+}
+
+// The kept cells, marked in mask[first particle] at their level (the depth-
+// first numbering counts them): the root, and the octree children of every
+// splitting cell, found by the splitting cell's own thread, which also records
+// itself as their octree parent.  One thread per internal binary node; only
+// the splitting cells (~N / leaf capacity of them) do work.
 __global__ void keep_kernel(Tree t, int leaf_capacity, int* status) {
   const int n = t.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= 2 * n - 1) return;
-  int kept = 0;
-  const int lvl = t.cell[b];
-  if (lvl >= 0) {
-    int p = -1;
-    if (b == 0) {
-      kept = 1;
-    } else {
-      p = octree_parent(t, b, status);
-      kept = p >= 0 && (last_of(t, p) - first_of(t, p) + 1) > leaf_capacity;
+  if (b >= n - 1) return;
+  if (b == 0) {
+    t.oparent[0] = -1;
+    if (t.cell[0] < 0) {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      return;
     }
-    t.oparent[b] = p;  // place_kernel reads it instead of climbing again
-    if (kept) atomicOr(&t.mask[first_of(t, b)], 1u << lvl);
+    atomicOr(&t.mask[0], 1u << t.cell[0]);
   }
-  t.kept[b] = kept;
+  if (!splits(t, b, leaf_capacity)) return;
+  octree_children(t, b, status, [&](int c, int) {
+    t.oparent[c] = b;
+    const int f = first_of(t, c);
+    if (f >= 0 && f < n) {
+      atomicOr(&t.mask[f], 1u << t.cell[c]);
+    } else {
+      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+    }
+  });
 }
-
 // Exclusive scan of popc(mask[k]) into offset[0..n].
 __global__ void scan_reduce_kernel(Tree t) {
   __shared__ uint32_t sh[256];
@@ -790,46 +826,75 @@ __device__ __forceinline__ int dfs_index(const Tree& t, int begin, int lvl) {
   return (int)(t.offset[begin] + __popc(t.mask[begin] & ((1u << lvl) - 1u)));
 }
 
+// The record of kept cell b at depth-first index `node`: next (the first node
+// after its subtree), first particle, particle count (0: internal) and octree
+// parent (-1: the root).
+__device__ __forceinline__ void write_node(const Tree& t, int b, int node, int parent_node,
+                                           bool leaf, int total) {
+  const int begin = first_of(t, b), end = last_of(t, b) + 1;
+  const int next = end >= t.n ? total : (int)t.offset[end];
+  t.info[node] = make_int4(next, begin, leaf ? end - begin : 0, parent_node);
+  t.level[node] = t.cell[b];
+  t.arrive[node] = 0;
+  t.height[node] = 1;
+}
+
+// Octree records in depth-first order.  Every splitting cell writes its own
+// record, its children list (in Morton order, which is depth-first order) and
+// the records of its children that are buckets; a splitting child writes its
+// own.  One thread per internal binary node, like keep_kernel.
 __global__ void place_kernel(Tree t, int leaf_capacity, int* status) {
   const int n = t.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= 2 * n - 1 || !t.kept[b]) return;
-  const int lvl = t.cell[b];
-  const int begin = first_of(t, b), end = last_of(t, b) + 1;
-  const int count = end - begin;
-  const int node = dfs_index(t, begin, lvl);
   const int total = (int)t.offset[n];
-  if (node < 0 || node >= total || total > 2 * n - 1) {
-    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-    return;
+  int leaves = 0;
+  if (b < n - 1 && (total < 1 || total > 2 * n - 1)) {
+    if (b == 0) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+  } else if (b < n - 1) {
+    const bool split = splits(t, b, leaf_capacity);
+    if (b == 0 && !split) {  // the root is the only node: one bucket
+      if (total == 1) {
+        write_node(t, 0, 0, -1, true, total);
+        t.nchild[0] = 0;
+        leaves = 1;
+      } else {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      }
+    } else if (split) {
+      const int node = dfs_index(t, first_of(t, b), t.cell[b]);
+      int parent_node = -1;
+      bool ok = node >= 0 && node < total;
+      if (b != 0) {
+        const int p = t.oparent[b];  // keep_kernel: the splitting cell that found b
+        ok = ok && p >= 0 && p < n - 1;
+        if (ok) parent_node = dfs_index(t, first_of(t, p), t.cell[p]);
+        ok = ok && parent_node >= 0 && parent_node < node;  // parents precede children
+      }
+      if (!ok) {
+        atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+      } else {
+        write_node(t, b, node, parent_node, false, total);
+        const int kids = octree_children(t, b, status, [&](int c, int k) {
+          const int cn = dfs_index(t, first_of(t, c), t.cell[c]);
+          if (cn <= node || cn >= total) {
+            atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
+            t.children[8 * node + k] = -1;
+            return;
+          }
+          t.children[8 * node + k] = cn;
+          if (!splits(t, c, leaf_capacity)) {  // a bucket
+            write_node(t, c, cn, node, true, total);
+            t.nchild[cn] = 0;
+            ++leaves;
+          }
+        });
+        for (int k = kids; k < 8; ++k) t.children[8 * node + k] = -1;
+        t.nchild[node] = kids;
+      }
+    }
   }
-  const int next = end >= n ? total : (int)t.offset[end];
-  const bool leaf = b >= n - 1 || count <= leaf_capacity || lvl >= 21;
-  int parent_node = -1;
-  if (b != 0) {
-    const int p = t.oparent[b];  // kept nodes are cells: keep_kernel stored it
-    if (p < 0 || p >= n - 1) {
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-      return;
-    }
-    parent_node = dfs_index(t, first_of(t, p), t.cell[p]);
-    if (parent_node < 0 || parent_node >= node) {  // parents precede children in DFS order
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-      return;
-    }
-    // children in arrival order; the moments pass sorts them into depth-first order
-    const int slot = atomicAdd(&t.nchild[parent_node], 1);
-    if (slot < 8) {
-      t.children[8 * parent_node + slot] = node;
-    } else {
-      atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-    }
-  }
-  t.info[node] = make_int4(next, begin, leaf ? count : 0, parent_node);
-  t.level[node] = lvl;
-  t.arrive[node] = 0;
-  t.height[node] = 1;
-  if (leaf) atomicAdd(t.leaves, 1ull);
+  leaves = (int)__reduce_add_sync(kFull, (unsigned)leaves);
+  if ((threadIdx.x & 31) == 0 && leaves > 0) atomicAdd(t.leaves, (unsigned long long)leaves);
 }
 
 // Trace-free quadrupole accumulation helpers (FP64).
@@ -2555,12 +2620,17 @@ void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree
   if (n >= 2)
     NBSP_COUNT_LAUNCH(1), radix_tree_kernel<<<(unsigned)((n - 1 + 255) / 256), 256, 0, stream>>>(keys, t, status);
   NBSP_COUNT_LAUNCH(1), cells_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, status);
-  NBSP_COUNT_LAUNCH(1), keep_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
+  // keep and place: one thread per internal binary node (n >= 2: the caller
+  // handles a lone particle without a tree)
+  const unsigned internal_blocks = (unsigned)((n - 1 + 255) / 256);
+  if (internal_blocks > 0)
+    NBSP_COUNT_LAUNCH(1), keep_kernel<<<internal_blocks, 256, 0, stream>>>(t, leaf_capacity, status);
   const int blocks = (int)((n + kScanItems - 1) / kScanItems);
   NBSP_COUNT_LAUNCH(1), scan_reduce_kernel<<<blocks, 256, 0, stream>>>(t);
   NBSP_COUNT_LAUNCH(1), scan_blocks_kernel<<<1, 1024, 0, stream>>>(t, blocks);
   NBSP_COUNT_LAUNCH(1), scan_apply_kernel<<<blocks, 256, 0, stream>>>(t);
-  NBSP_COUNT_LAUNCH(1), place_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, leaf_capacity, status);
+  if (internal_blocks > 0)
+    NBSP_COUNT_LAUNCH(1), place_kernel<<<internal_blocks, 256, 0, stream>>>(t, leaf_capacity, status);
 }
 
 void nbsp_bh_moments(const void* pos4, const uint64_t* keys, size_t n, const double* geometry,
