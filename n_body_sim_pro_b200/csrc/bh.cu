@@ -502,8 +502,6 @@ struct Tree {
   int n;
   int2* range;        // [n-1] first, last of internal nodes
   int2* child;        // [n-1] binary ids of the two children
-  int* delta;         // [n-1] common prefix length in bits
-  int* parent;        // [2n-1] binary parent id (root: -1)
   int* cell;          // [2n-1] octree level of a cell node, -1 otherwise
   int* oparent;       // [2n-1] octree parent (binary id) of a cell node, from keep_kernel
   uint32_t* mask;     // [n]   levels of kept nodes starting at particle k
@@ -547,8 +545,6 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.n = (int)n_;
   t.range = carve<int2>(p, ni);
   t.child = carve<int2>(p, ni);
-  t.delta = carve<int>(p, ni);
-  t.parent = carve<int>(p, nb);
   t.cell = carve<int>(p, nb);
   t.oparent = carve<int>(p, nb);
   t.mask = carve<uint32_t>(p, n);
@@ -594,6 +590,15 @@ __device__ __forceinline__ int prefix(const uint64_t* __restrict__ keys, int n, 
   return 63 + __clz((unsigned)(i ^ j));
 }
 
+__device__ __forceinline__ int level_of_delta(int delta) { return min(delta / 3, 21); }
+
+// Karras's radix tree over the sorted keys, and which of its nodes are octree
+// cells: an internal node whose octree level (prefix length / 3) is deeper
+// than its parent's, the root, and a particle below a node above level 21.
+// The parent's prefix length is that of the node's range extended by one key
+// on the side with the longer common prefix, max(delta(first - 1, first),
+// delta(last, last + 1)), so each thread decides its own node and its leaf
+// children without reading another thread's results.
 __global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, Tree t, int* status) {
   const int n = t.n;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -625,34 +630,13 @@ __global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, Tree t, int
   const int right = last == gamma + 1 ? (n - 1) + gamma + 1 : gamma + 1;
   t.range[i] = make_int2(first, last);
   t.child[i] = make_int2(left, right);
-  t.delta[i] = dnode;
-  t.parent[left] = i;
-  t.parent[right] = i;
-  if (i == 0) t.parent[0] = -1;
+  const int lvl = level_of_delta(dnode);
+  const int pdelta = max(prefix(keys, n, first, first - 1), prefix(keys, n, last, last + 1));
+  t.cell[i] = (i == 0 || level_of_delta(pdelta) < lvl) ? lvl : -1;
+  if (left >= n - 1) t.cell[left] = lvl <= 20 ? 22 : -1;
+  if (right >= n - 1) t.cell[right] = lvl <= 20 ? 22 : -1;
 }
 
-__device__ __forceinline__ int level_of_delta(int delta) { return min(delta / 3, 21); }
-
-// Octree cell nodes among the binary nodes (see file comment).
-__global__ void cells_kernel(Tree t, int* status) {
-  const int n = t.n;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= 2 * n - 1) return;
-  int cell = -1;
-  const int p = t.parent[b];
-  if (b != 0 && (p < 0 || p >= n - 1)) {  // every non-root node has an internal parent
-    atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
-    t.cell[b] = -1;
-    return;
-  }
-  if (b < n - 1) {
-    const int lvl = level_of_delta(t.delta[b]);
-    if (b == 0 || level_of_delta(t.delta[p]) < lvl) cell = lvl;
-  } else {
-    if (level_of_delta(t.delta[p]) <= 20) cell = 22;
-  }
-  t.cell[b] = cell;
-}
 
 __device__ __forceinline__ int first_of(const Tree& t, int b) {
   return b < t.n - 1 ? t.range[b].x : b - (t.n - 1);
@@ -988,17 +972,10 @@ __device__ __forceinline__ int arrive_acq_rel(int* p) {
   return old;
 }
 
-__device__ __forceinline__ void swap_if_greater(int& a, int& b) {
-  const int lo = min(a, b), hi = max(a, b);
-  a = lo;
-  b = hi;
-}
-
 // Bottom-up moments: leaves sum their particles, the last child to finish
-// combines its parent.  place_kernel recorded the children in arrival order;
-// the combine sorts them into depth-first (= octant) order, so the sums run in
-// a fixed order and the result is deterministic, loads all of them at once and
-// writes the sorted list back for the interaction-list walk.
+// combines its parent.  place_kernel wrote each children list in depth-first
+// (= octant) order, so the combine's sums run in a fixed order and the result
+// is deterministic; it loads all the children at once.
 // QUAD: also the trace-free quadrupoles and the spread (the quadrupole walk,
 // the correction's features); the monopole walk reads neither.
 // Monopole pass at 6 blocks per SM (40 registers, a few spilled to L1): it is
@@ -1074,21 +1051,7 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
       const int4 pinfo = __ldcg(&t.info[parent]);
       const int4 ca = __ldcg(reinterpret_cast<const int4*>(t.children) + 2 * parent);
       const int4 cb = __ldcg(reinterpret_cast<const int4*>(t.children) + 2 * parent + 1);
-      int ch[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if (k >= nc) ch[k] = INT_MAX;
-      // sorting network for 8 keys (19 compare-exchanges)
-      swap_if_greater(ch[0], ch[2]); swap_if_greater(ch[1], ch[3]);
-      swap_if_greater(ch[4], ch[6]); swap_if_greater(ch[5], ch[7]);
-      swap_if_greater(ch[0], ch[4]); swap_if_greater(ch[1], ch[5]);
-      swap_if_greater(ch[2], ch[6]); swap_if_greater(ch[3], ch[7]);
-      swap_if_greater(ch[0], ch[1]); swap_if_greater(ch[2], ch[3]);
-      swap_if_greater(ch[4], ch[5]); swap_if_greater(ch[6], ch[7]);
-      swap_if_greater(ch[2], ch[4]); swap_if_greater(ch[3], ch[5]);
-      swap_if_greater(ch[1], ch[4]); swap_if_greater(ch[3], ch[6]);
-      swap_if_greater(ch[1], ch[2]); swap_if_greater(ch[3], ch[4]);
-      swap_if_greater(ch[5], ch[6]);
+      const int ch[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
       bool bad = false;
 #pragma unroll
       for (int k = 0; k < 8; ++k) bad |= k < nc && (ch[k] <= parent || ch[k] >= total);
@@ -1139,12 +1102,6 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
           pm.q[5] += __ldcg(&t.quad64[6 * c + 5]) + w * (3.0 * dz * dz - r2);
         }
       }
-      // the sorted children, -1 after the last (the walk pushes the first `kids`)
-      reinterpret_cast<int4*>(t.children)[2 * parent] =
-          make_int4(ch[0], nc > 1 ? ch[1] : -1, nc > 2 ? ch[2] : -1, nc > 3 ? ch[3] : -1);
-      reinterpret_cast<int4*>(t.children)[2 * parent + 1] =
-          make_int4(nc > 4 ? ch[4] : -1, nc > 5 ? ch[5] : -1, nc > 6 ? ch[6] : -1,
-                    nc > 7 ? ch[7] : -1);
       t.height[parent] = hmax + 1;
       finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open);
       parent = pinfo.w;
@@ -2612,14 +2569,10 @@ size_t nbsp_bh_tree_bytes(size_t n) { return tree_bytes(n); }
 void nbsp_bh_build(const uint64_t* keys, size_t n, int leaf_capacity, void* tree, int* status,
                    cudaStream_t stream) {
   Tree t = tree_view(tree, n);
-  const size_t nb = 2 * n - 1;
   cudaMemsetAsync(t.mask, 0, n * sizeof(uint32_t), stream);
-  cudaMemsetAsync(t.nchild, 0, nb * sizeof(int), stream);
   cudaMemsetAsync(t.leaves, 0, sizeof(unsigned long long), stream);
-  cudaMemsetAsync(t.parent, 0xff, nb * sizeof(int), stream);  // -1: not yet linked
   if (n >= 2)
     NBSP_COUNT_LAUNCH(1), radix_tree_kernel<<<(unsigned)((n - 1 + 255) / 256), 256, 0, stream>>>(keys, t, status);
-  NBSP_COUNT_LAUNCH(1), cells_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, stream>>>(t, status);
   // keep and place: one thread per internal binary node (n >= 2: the caller
   // handles a lone particle without a tree)
   const unsigned internal_blocks = (unsigned)((n - 1 + 255) / 256);
