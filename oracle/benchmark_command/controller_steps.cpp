@@ -7,7 +7,9 @@
 // library.
 //
 //   controller_steps PRESET N SEED ALGORITHM THETA SOFTENING TIMESTEP STEPS OUT
-//     ALGORITHM: cuda | barnes_hut_cuda | all_pairs | barnes_hut
+//     ALGORITHM: cuda | barnes_hut_cuda | all_pairs | barnes_hut, or
+//     cuda_resident | barnes_hut_cuda_resident: the controller's device-resident
+//     step, with no download before the checkpoint's own
 #include "simulation/SimulationController.hpp"
 
 #include <cstdio>
@@ -37,12 +39,14 @@ int main(int argc, char** argv) {
         n_body_sim_pro::SimulationController sim;
         sim.running = false;
         sim.use_cuda = std::strstr(algorithm, "cuda") != nullptr;
+        sim.cuda_resident = std::strstr(algorithm, "_resident") != nullptr;
         sim.barnes_hut_enabled = std::strncmp(algorithm, "barnes_hut", 10) == 0;
         sim.barnes_hut_theta = std::atof(argv[5]);
         sim.set_softening_length(std::atof(argv[6]));
         sim.timestep = std::atof(argv[7]);
         sim.apply_preset((NBodySimProSimulationPreset)preset, n, seed);
         const int steps = std::atoi(argv[8]);
+        sim.cuda_download_interval = steps + 1;  // (resident) the checkpoint downloads
         for (int s = 0; s < steps; ++s) sim.step();
         sim.save_checkpoint(argv[9]);
         std::printf("{\"steps\":%d,\"last_step_ms\":%.6f,\"force_evaluation_ms\":%.6f}\n", steps,

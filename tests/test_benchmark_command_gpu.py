@@ -83,11 +83,16 @@ def _read_checkpoint(path: str) -> dict:
 @pytest.mark.parametrize("algorithm,theta,acc_tol,pos_tol", [
     ("cuda", 0.7, 2e-6, 1e-10),          # all-pairs bars of tests/test_allpairs_gpu.py
     ("barnes_hut_cuda", 0.5, 1e-2, 1e-7),  # the reference's own theta-0.3 bar, at 0.5
+    ("cuda_resident", 0.7, 2e-6, 1e-10),
+    ("barnes_hut_cuda_resident", 0.5, 1e-2, 1e-7),
 ])
 def test_controller_steps_match_the_oracle(tmp_path, algorithm, theta, acc_tol, pos_tol):
-    """Three controller steps (the reference's host leapfrog, integrator.c:47-85,
-    with the device force function) against the oracle's FP64 leapfrog with the
-    exact all-pairs sum on the same sequential preset."""
+    """Three controller steps against the oracle's FP64 leapfrog with the exact
+    all-pairs sum on the same sequential preset: the reference's host leapfrog
+    (integrator.c:47-85) with the device force function, or (`_resident`) the
+    controller's device-resident step — the state uploaded once, advanced by
+    n_body_sim_pro_cuda_advance and downloaded only when the checkpoint is
+    written."""
     n, seed, eps, dt, steps = 4096, 42, 0.01, 1e-3, 3
     out = str(tmp_path / "state.ckpt")
     r = subprocess.run([STEPS_DRIVER, "globular_cluster", str(n), str(seed), algorithm,
