@@ -524,6 +524,9 @@ struct Tree {
   float* spread;      // sum m |x - com|^2 / (M side^2): the correction MLP's 10th feature
   float* shift;       // distance from the cell's geometric centre to its centre of mass
   float* kmass;       // M side^2: the relative opening test's cell term
+  // what the interaction-list walk reads of a node, in one 32-byte record:
+  // (com xyz, mass), (ropen2, kmass, first particle, particle count as int bits)
+  float4* wnode;      // 2 per node
   unsigned long long* leaves;  // [1]
 };
 
@@ -566,6 +569,7 @@ __host__ __device__ inline Tree tree_layout(uintptr_t p, size_t n_, uintptr_t* e
   t.spread = carve<float>(p, nb);
   t.shift = carve<float>(p, nb);
   t.kmass = carve<float>(p, nb);
+  t.wnode = carve<float4>(p, 2 * nb);
   t.leaves = carve<unsigned long long>(p, 1);
   if (end != nullptr) *end = p;
   return t;
@@ -913,7 +917,7 @@ struct Opening {
 
 template <bool QUAD>
 __device__ void finish_node(const Tree& t, int node, const Moments& mo, int first, int lvl,
-                            const Opening& o) {
+                            const Opening& o, int count) {
   t.mom[node] = make_double4(mo.m, mo.cx, mo.cy, mo.cz);
   if (QUAD) {
     for (int k = 0; k < 6; ++k) t.quad64[6 * node + k] = mo.q[k];
@@ -949,6 +953,9 @@ __device__ void finish_node(const Tree& t, int node, const Moments& mo, int firs
   t.side[node] = (float)side;
   t.shift[node] = (float)shift;
   t.kmass[node] = (float)(mo.m * side * side);
+  t.wnode[2 * node] = make_float4((float)mo.cx, (float)mo.cy, (float)mo.cz, (float)mo.m);
+  t.wnode[2 * node + 1] = make_float4((float)r2, (float)(mo.m * side * side), __int_as_float(first),
+                                      __int_as_float(count));
   if (QUAD) {
     t.spread[node] = mo.m > 0.0 ? (float)(mo.t2 / (mo.m * side * side)) : 0.f;
     t.quad[2 * node] = make_float4((float)mo.q[0], (float)mo.q[1], (float)mo.q[2], (float)mo.q[3]);
@@ -1034,7 +1041,7 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
         mo.q[5] += w * (3.0 * dz * dz - r2);
       }
     }
-    finish_node<QUAD>(t, node, mo, info.y, t.level[node], open);
+    finish_node<QUAD>(t, node, mo, info.y, t.level[node], open, info.z);
     int parent = info.w;
     for (int climb = 0; parent >= 0; ++climb) {
       if (climb > 64 || parent >= total) {  // octree depth <= 23 levels
@@ -1103,7 +1110,7 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
         }
       }
       t.height[parent] = hmax + 1;
-      finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open);
+      finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open, pinfo.z);
       parent = pinfo.w;
     }
   }
@@ -1906,10 +1913,11 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       }
       const bool valid = node >= 0;
       const int at = valid ? node : 0;
-      const int4 info = t.info[at];
-      const float4 c = t.com[at];
-      const float ro = t.ropen2[at];
-      const float km = REL ? t.kmass[at] : 0.f;
+      const float4 w0 = t.wnode[2 * at], w1 = t.wnode[2 * at + 1];
+      const int4 info = make_int4(0, __float_as_int(w1.z), __float_as_int(w1.w), 0);
+      const float4 c = w0;
+      const float ro = w1.x;
+      const float km = REL ? w1.y : 0.f;
       const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
       if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
       const bool ok = valid && !bad;
@@ -2048,10 +2056,14 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       {  // every lane loads a node (idle lanes the root) so no branch diverges
         const bool valid = node >= 0;
         const int at = valid ? node : 0;
-        info = t.info[at];
-        c = t.com[at];
-        ro = t.ropen2[at];
-        if (REL) km = t.kmass[at];
+        // one 32-byte record: the centre of mass and mass, the opening terms
+        // and the particle range (the node's next and parent links are not read)
+        const float4 w0 = t.wnode[2 * at], w1 = t.wnode[2 * at + 1];
+        c = w0;
+        ro = w1.x;
+        if (REL) km = w1.y;
+        info.y = __float_as_int(w1.z);
+        info.z = __float_as_int(w1.w);
         const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
         if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
         const bool ok = valid && !bad;
