@@ -2058,7 +2058,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
         const int at = valid ? node : 0;
         // one 32-byte record: the centre of mass and mass, the opening terms
         // and the particle range (the node's next and parent links are not read)
-        const float4 w0 = t.wnode[2 * at], w1 = t.wnode[2 * at + 1];
+        const float4 w0 = __ldg(&t.wnode[2 * at]), w1 = __ldg(&t.wnode[2 * at + 1]);
         c = w0;
         ro = w1.x;
         if (REL) km = w1.y;
@@ -2099,8 +2099,8 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       const bool open = (test || opened) && !accept;
       is_leaf = is_leaf || (open && info.z > 0);  // a failing bucket is summed exactly
       if (open && info.z == 0) {                   // an opened cell pushes its children
-        ca = reinterpret_cast<const int4*>(t.children)[2 * node];
-        cb = reinterpret_cast<const int4*>(t.children)[2 * node + 1];
+        ca = __ldg(reinterpret_cast<const int4*>(t.children) + 2 * node);
+        cb = __ldg(reinterpret_cast<const int4*>(t.children) + 2 * node + 1);
       }
       kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) + (cb.y >= 0) +
              (cb.z >= 0) + (cb.w >= 0);
