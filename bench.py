@@ -775,11 +775,16 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
     nodes = float(stats_acc[-1]["node_count"])
     rel = m["relative_alpha"] > 0.0
     quad = m["multipole_order"] == 2 or m["corrected"]
-    # moments: the monopole pass reads each particle once (16 B) and per node
-    # writes 64 B (FP64 moments, the walk's float4, opening terms) and reads 52
-    # (record, level, children's moments); the quadrupole pass reads the
-    # particles twice, writes 156 and reads 108 per node
-    mom_bytes = (32.0 * n + 264.0 * nodes) if quad else (16.0 * n + 116.0 * nodes)
+    # moments: the monopole pass reads each particle once (16 B); per node it
+    # writes 100 B (FP64 moments 32, the centre-of-mass float4 16, ropen2, side,
+    # shift and the cell term 16, the walk's 32-byte record, the height 4) and
+    # reads 76 (its record 16, level 4, first key 8; as a child, by its parent:
+    # FP64 moments 32, height 4, child count 4, the arrival counter 4; children
+    # lists 32 per internal node, ~4 per node), plus the 4-byte atomic write of
+    # its arrival: 180 B.  The quadrupole pass reads the particles twice and
+    # adds per node 92 B written (FP64 quadrupole and trace, the walk's
+    # quadrupole, the spread) and 56 read (the children's FP64 quadrupole and trace)
+    mom_bytes = (32.0 * n + 328.0 * nodes) if quad else (16.0 * n + 180.0 * nodes)
     rows = [
         # bounds: x, y, z, m (+ the previous accelerations for the relative test)
         ("bounds", "bounds_ms", (32.0 + (24.0 if rel else 0.0)) * n),
@@ -815,7 +820,7 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
     stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes per "
                        "particle: bounds 32 (+24 relative), keys 32 read + 28 written (+28 "
                        "relative), sort 8 passes x (12 + 12), moments "
-                       + ("2 x 16 + 264 per node" if quad else "16 + 116 per node")
+                       + ("2 x 16 + 328 per node" if quad else "16 + 180 per node")
                        + ", unsort 32 read + 24 written, kick-drift 120 + kick 72")
     return stages
 
