@@ -37,7 +37,7 @@ constexpr unsigned kFull = 0xffffffffu;
 // ---------------------------------------------------------------------------
 
 constexpr int kBoundsThreads = 256;
-constexpr int kBoundsBlocks = 1024;
+constexpr int kBoundsBlocks = 4 * 148;  // one wave at 4 blocks of 256 per SM (58 registers)
 constexpr int kBoundsVals = 11;  // min xyz, max xyz, m, mx, my, mz, |a|^2
 
 // The block's combined values in thread 0: each warp by shuffles, then the
@@ -187,7 +187,7 @@ static_assert(kSortThreads >= kRadix, "one thread per digit");
 constexpr int kSortPasses = 8;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kCountMask = (1u << 30) - 1u;
 constexpr int kLookbackSpins = 1 << 22;  // ~ms per predecessor before the error flag
-constexpr int kKeysBlocks = 4 * 148;  // 32 warps per SM: enough loads in flight for HBM
+constexpr int kKeysBlocks = 5 * 148;  // 40 warps per SM (48 registers): enough loads in flight
 
 // Sort scratch (32-bit words): hist[8][256] | base[8][256] | ticket[8] | status[8][tiles][256]
 struct SortScratch {
