@@ -785,17 +785,21 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
     # adds per node 92 B written (FP64 quadrupole and trace, the walk's
     # quadrupole, the spread) and 56 read (the children's FP64 quadrupole and trace)
     mom_bytes = (32.0 * n + 328.0 * nodes) if quad else (16.0 * n + 180.0 * nodes)
+    # The timed steps are device-resident leapfrog steps: the opening kick and
+    # drift run in the bounds pass and the closing kick in the pass that writes
+    # the accelerations (the phase events bracket them)
     rows = [
-        # bounds: x, y, z, m (+ the previous accelerations for the relative test)
-        ("bounds", "bounds_ms", (32.0 + (24.0 if rel else 0.0)) * n),
+        # bounds + kick-drift: read x, y, z, m 32, v 24, a 24; write x, v 48
+        ("bounds", "bounds_ms", (32.0 + 24.0 + 24.0 + 48.0) * n),
         # keys: read x, y, z, m; write key 8, index 4, the walk's float4 16
         # (+ read a_old 24, write the relative tolerance 4)
         ("keys", "keys_ms", (32.0 + 28.0 + (28.0 if rel else 0.0)) * n),
         # 8 LSD passes over (key 8 + index 4), read and written
         ("sort", "sort_ms", 8 * 24.0 * n),
         ("moments", "moments_ms", mom_bytes),
-        # unsort: the walk's double4 (32 B, input order) read, ax/ay/az 24 written
-        ("unsort", "integrate_ms", 56.0 * n),
+        # unsort + closing kick: read the walk's double4 (32 B, input order) and
+        # v 24; write ax/ay/az 24 and v 24
+        ("unsort", "integrate_ms", (32.0 + 24.0 + 24.0 + 24.0) * n),
     ]
     stages = {}
     for name, key, nbytes in rows:
@@ -804,24 +808,18 @@ def stage_bandwidth(phases, stats_acc, n, m, peaks, peak_kind):
         stages[name] = {"ms": round(ms, 4), "algorithmic_bytes": nbytes,
                         "gbs": round(gbs, 1) if gbs else None,
                         "frac_of_hbm": round(gbs / hbm, 4) if gbs else None}
-    # the two kick launches run outside the Barnes-Hut phase events: their time is
-    # the step's minus the phases'; opening kick-drift reads v, a, x (72 B) and
-    # writes v, x (48 B), the closing kick reads v, a (48 B) and writes v (24 B)
-    kick_ms = float(np.mean([ph["total_ms"] - sum(ph[k] for k in (
+    # what the phase events do not cover: the step's total minus the phases
+    # (the memsets and launch gaps between the passes; no kernel of its own)
+    gap_ms = float(np.mean([ph["total_ms"] - sum(ph[k] for k in (
         "bounds_ms", "keys_ms", "sort_ms", "build_ms", "moments_ms", "walk_ms", "integrate_ms"))
         for ph in phases]))
-    kick_bytes = 192.0 * n
-    gbs = kick_bytes / (kick_ms * 1e-3) / 1e9 if kick_ms > 0 else None
-    stages["kick_drift"] = {"ms": round(kick_ms, 4), "algorithmic_bytes": kick_bytes,
-                            "gbs": round(gbs, 1) if gbs else None,
-                            "frac_of_hbm": round(gbs / hbm, 4) if gbs else None,
-                            "timed_as": "step total minus the Barnes-Hut phases (includes "
-                                        "launch gaps)"}
+    stages["outside_phases"] = {"ms": round(gap_ms, 4),
+                                "timed_as": "step total minus the Barnes-Hut phases"}
     stages["_note"] = (f"HBM peak {hbm} GB/s ({peak_kind} MEASURED_PEAKS.json); bytes per "
-                       "particle: bounds 32 (+24 relative), keys 32 read + 28 written (+28 "
-                       "relative), sort 8 passes x (12 + 12), moments "
-                       + ("2 x 16 + 328 per node" if quad else "16 + 180 per node")
-                       + ", unsort 32 read + 24 written, kick-drift 120 + kick 72")
+                       "particle: bounds with the opening kick and drift 80 read + 48 written, "
+                       "keys 32 read + 28 written (+28 relative), sort 8 passes x (12 + 12), "
+                       "moments " + ("2 x 16 + 328 per node" if quad else "16 + 180 per node")
+                       + ", unsort with the closing kick 56 read + 48 written")
     return stages
 
 

@@ -523,11 +523,14 @@ static NBodySimProStatus pack_state(NBodySimProCudaContext* c, NBodySimProError*
     return N_BODY_SIM_PRO_STATUS_OK;
 }
 
-/* One force evaluation of the resident state with `algorithm`. */
-static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
-                                                const NBodySimProGravity* g,
-                                                NBodySimProCudaAlgorithm algorithm,
-                                                NBodySimProError* error) {
+/* One force evaluation of the resident state with `algorithm`; with a
+ * leapfrog fusion (Barnes-Hut only; NULL: none) the step's opening kick and
+ * drift and its closing kick run inside the evaluation's first and last passes. */
+static NBodySimProStatus resident_accelerations_fused(NBodySimProCudaContext* c,
+                                                      const NBodySimProGravity* g,
+                                                      NBodySimProCudaAlgorithm algorithm,
+                                                      const NbspLeapfrogFusion* leapfrog,
+                                                      NBodySimProError* error) {
     if (c->n == 0) return N_BODY_SIM_PRO_STATUS_OK;
     if (algorithm == N_BODY_SIM_PRO_CUDA_ALGORITHM_BARNES_HUT) {
         NbspBarnesHutParams p;
@@ -541,7 +544,9 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
         p.tolerance = c->tolerance;
         p.correction = c->correction;
         p.quadrupoles = c->tree_quadrupoles;
-        NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
+        NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n,
+                                {NULL, NULL, NULL, 0.0, 0.0}};
+        if (leapfrog != NULL) s.leapfrog = *leapfrog;
         c->bh_pending = 1;
         return nbsp_bh_accelerations(&c->bh, &s, &p, c->status, c->stream, &c->stats,
                                      &c->timings, error);
@@ -549,6 +554,14 @@ static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
     NBodySimProStatus st = pack_state(c, error);
     if (st != N_BODY_SIM_PRO_STATUS_OK) return st;
     return allpairs_accelerations(c, g, error);
+}
+
+/* One force evaluation of the resident state with `algorithm`. */
+static NBodySimProStatus resident_accelerations(NBodySimProCudaContext* c,
+                                                const NBodySimProGravity* g,
+                                                NBodySimProCudaAlgorithm algorithm,
+                                                NBodySimProError* error) {
+    return resident_accelerations_fused(c, g, algorithm, NULL, error);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -911,7 +924,16 @@ NBodySimProStatus n_body_sim_pro_cuda_advance(NBodySimProCudaContext* c,
         if ((st = advance_allpairs_kdk(c, gravity, dt, steps, error)) != N_BODY_SIM_PRO_STATUS_OK)
             return st;
     } else {
+        /* Barnes-Hut: the kicks and the drift ride in the evaluation's bounds
+         * pass and its last pass (a lone particle has no tree: plain kicks) */
+        const NbspLeapfrogFusion lf = {c->vx, c->vy, c->vz, h, dt};
         for (int step = 0; step < steps; ++step) {
+            if (n >= 2) {
+                if ((st = resident_accelerations_fused(c, gravity, algorithm, &lf, error)) !=
+                    N_BODY_SIM_PRO_STATUS_OK)
+                    return st;
+                continue;
+            }
             nbsp_kick_drift(c->x, c->y, c->z, c->vx, c->vy, c->vz, c->ax, c->ay, c->az, n, h, dt,
                             c->stream);
             if ((st = resident_accelerations(c, gravity, algorithm, error)) != N_BODY_SIM_PRO_STATUS_OK)
@@ -1115,7 +1137,8 @@ NBodySimProStatus n_body_sim_pro_cuda_morton_order(NBodySimProCudaContext* c, ui
         return FAIL(N_BODY_SIM_PRO_STATUS_INVALID_ARGUMENT,
                     "cannot build a Barnes-Hut tree for an empty system");
     CUDA_TRY(cudaSetDevice(c->device));
-    NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n};
+    NbspBarnesHutState s = {c->x, c->y, c->z, c->m, c->ax, c->ay, c->az, c->n,
+                                {NULL, NULL, NULL, 0.0, 0.0}};
     NBodySimProStatus st =
         nbsp_bh_morton(&c->bh, &s, c->status, c->stream, keys_sorted, permutation, root, error);
     if (st != N_BODY_SIM_PRO_STATUS_OK) return st;

@@ -72,11 +72,15 @@ __device__ __forceinline__ void bounds_block_reduce(double (&v)[kBoundsVals],
   }
 }
 
+// KICK: the opening kick and drift of a device-resident leapfrog step first
+// (kick_drift_kernel's arithmetic), the reductions then of the drifted state.
+template <bool KICK>
 __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
-    const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+    double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
     const double* __restrict__ m, size_t n, double* __restrict__ partial, int* status,
     const double* __restrict__ ax, const double* __restrict__ ay,
-    const double* __restrict__ az) {
+    const double* __restrict__ az, bool rms_of_a, double* __restrict__ vx,
+    double* __restrict__ vy, double* __restrict__ vz, double h, double dt) {
   __shared__ double sh[kBoundsVals][kBoundsThreads / 32];
   double v[kBoundsVals] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY,
                            0.0,      0.0,      0.0,      0.0,       0.0};
@@ -84,7 +88,22 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
 #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)kBoundsThreads + threadIdx.x; i < n;
        i += (size_t)gridDim.x * kBoundsThreads) {
-    const double px = x[i], py = y[i], pz = z[i], pm = m[i];
+    double px = x[i], py = y[i], pz = z[i];
+    const double pm = m[i];
+    if (KICK) {
+      const double u = __dadd_rn(vx[i], __dmul_rn(ax[i], h));
+      const double w = __dadd_rn(vy[i], __dmul_rn(ay[i], h));
+      const double q = __dadd_rn(vz[i], __dmul_rn(az[i], h));
+      vx[i] = u;
+      vy[i] = w;
+      vz[i] = q;
+      px = __dadd_rn(px, __dmul_rn(u, dt));
+      py = __dadd_rn(py, __dmul_rn(w, dt));
+      pz = __dadd_rn(pz, __dmul_rn(q, dt));
+      x[i] = px;
+      y[i] = py;
+      z[i] = pz;
+    }
     bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
     v[0] = fmin(v[0], px);
     v[1] = fmin(v[1], py);
@@ -96,7 +115,7 @@ __global__ void __launch_bounds__(kBoundsThreads) bounds_kernel(
     v[7] += pm * px;
     v[8] += pm * py;
     v[9] += pm * pz;
-    if (ax != nullptr) v[10] += ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i];
+    if (rms_of_a) v[10] += ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i];
   }
   if (bad) atomicOr(status, NBSP_DEVICE_ERROR_NONFINITE_POSITION);
   bounds_block_reduce(v, sh);
@@ -479,16 +498,26 @@ __global__ void gather_kernel(const float4* __restrict__ unsorted,
 }
 
 // a[i] = G * acc[i]: the walk wrote each target's sum at its input index
-// (one aligned 32-byte record), so this pass is coalesced both ways.
+// (one aligned 32-byte record), so this pass is coalesced both ways.  KICK:
+// the closing kick of a device-resident leapfrog step, v += h a, with
+// kick_drift_kernel's arithmetic on the accelerations just written.
+template <bool KICK>
 __global__ void unsort_kernel(const double4* __restrict__ acc, size_t n, double g,
                               double* __restrict__ ax, double* __restrict__ ay,
-                              double* __restrict__ az) {
+                              double* __restrict__ az, double* __restrict__ vx,
+                              double* __restrict__ vy, double* __restrict__ vz, double h) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const double4 a = acc[i];
-    ax[i] = g * a.x;
-    ay[i] = g * a.y;
-    az[i] = g * a.z;
+    const double gx = g * a.x, gy = g * a.y, gz = g * a.z;
+    ax[i] = gx;
+    ay[i] = gy;
+    az[i] = gz;
+    if (KICK) {
+      vx[i] = __dadd_rn(vx[i], __dmul_rn(gx, h));
+      vy[i] = __dadd_rn(vy[i], __dmul_rn(gy, h));
+      vz[i] = __dadd_rn(vz[i], __dmul_rn(gz, h));
+    }
   }
 }
 
@@ -2511,14 +2540,22 @@ void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order,
 
 extern "C" {
 
-void nbsp_bh_bounds(const double* x, const double* y, const double* z, const double* m, size_t n,
-                    double* partial, double* geometry, int* status, const double* ax,
-                    const double* ay, const double* az, cudaStream_t stream) {
+void nbsp_bh_bounds(double* x, double* y, double* z, const double* m, size_t n, double* partial,
+                    double* geometry, int* status, const double* ax, const double* ay,
+                    const double* az, int rms_of_a, const NbspLeapfrogFusion* leapfrog,
+                    cudaStream_t stream) {
   size_t blocks = (n + kBoundsThreads - 1) / kBoundsThreads;
   if (blocks < 1) blocks = 1;
   if (blocks > (size_t)kBoundsBlocks) blocks = kBoundsBlocks;
-  NBSP_COUNT_LAUNCH(1), bounds_kernel<<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(x, y, z, m, n, partial, status,
-                                                                   ax, ay, az);
+  if (leapfrog != nullptr && leapfrog->vx != nullptr) {
+    NBSP_COUNT_LAUNCH(1), bounds_kernel<true><<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(
+        x, y, z, m, n, partial, status, ax, ay, az, rms_of_a != 0, leapfrog->vx, leapfrog->vy,
+        leapfrog->vz, leapfrog->half_dt, leapfrog->dt);
+  } else {
+    NBSP_COUNT_LAUNCH(1), bounds_kernel<false><<<(unsigned)blocks, kBoundsThreads, 0, stream>>>(
+        x, y, z, m, n, partial, status, ax, ay, az, rms_of_a != 0, nullptr, nullptr, nullptr,
+        0.0, 0.0);
+  }
   NBSP_COUNT_LAUNCH(1), bounds_final_kernel<<<1, kBoundsThreads, 0, stream>>>(partial, (int)blocks,
                                                                             n, geometry);
 }
@@ -2657,9 +2694,15 @@ void nbsp_bh_correct(const void* pos4, size_t n, const void* tree, const void* c
 }
 
 void nbsp_bh_unsort(const void* acc, size_t n, double g, double* ax, double* ay, double* az,
-                    cudaStream_t stream) {
-  NBSP_COUNT_LAUNCH(1), unsort_kernel<<<grid_for(n, 256), 256, 0, stream>>>(
-      (const double4*)acc, n, g, ax, ay, az);
+                    const NbspLeapfrogFusion* leapfrog, cudaStream_t stream) {
+  if (leapfrog != nullptr && leapfrog->vx != nullptr) {
+    NBSP_COUNT_LAUNCH(1), unsort_kernel<true><<<grid_for(n, 256), 256, 0, stream>>>(
+        (const double4*)acc, n, g, ax, ay, az, leapfrog->vx, leapfrog->vy, leapfrog->vz,
+        leapfrog->half_dt);
+  } else {
+    NBSP_COUNT_LAUNCH(1), unsort_kernel<false><<<grid_for(n, 256), 256, 0, stream>>>(
+        (const double4*)acc, n, g, ax, ay, az, nullptr, nullptr, nullptr, 0.0);
+  }
 }
 
 void nbsp_bh_mlp_pairs(const void* pos4, size_t n, const void* tree, float theta, int opening,

@@ -44,10 +44,22 @@ typedef struct NbspBarnesHutParams {
                                (the correction's training reads them) */
 } NbspBarnesHutParams;
 
+/* The leapfrog of a device-resident step fused into an evaluation's first and
+ * last passes, with kick_drift_kernel's arithmetic (integrator.c:64-83): with
+ * vx set, the bounds pass first kicks v by half_dt * a (a: the accelerations in
+ * the state, the previous evaluation's) and drifts x by dt * v, and the pass
+ * that writes the new accelerations kicks v by half_dt * a.  vx NULL: none. */
+typedef struct NbspLeapfrogFusion {
+    double *vx, *vy, *vz;
+    double half_dt, dt;
+} NbspLeapfrogFusion;
+
 typedef struct NbspBarnesHutState {
-    const double *x, *y, *z, *m;
+    double *x, *y, *z;  /* written only by a fused drift */
+    const double* m;
     double *ax, *ay, *az;
     size_t n;
+    NbspLeapfrogFusion leapfrog;
 } NbspBarnesHutState;
 
 /* Enqueue one full Barnes-Hut force evaluation; accelerations into s->ax/ay/az.
@@ -79,12 +91,14 @@ NBSP_HIDDEN void nbsp_bh_destroy(NbspBarnesHut* bh);
 
 /* bbox + centre of mass: geometry[0..3] = root centre xyz + half size (bit-exact
  * with the reference), geometry[4..6] = centre of mass.  partial >= 1024*10 doubles. */
-NBSP_HIDDEN void nbsp_bh_bounds(const double* x, const double* y, const double* z,
-                                const double* m, size_t n, double* partial, double* geometry,
-                                int* status, const double* ax, const double* ay, const double* az,
-                                cudaStream_t stream);
-/* geometry: root centre [0..2], half side [3], centre of mass [4..6], and rms
- * |a| [7] of (ax, ay, az) when they are given (the relative test's floor) */
+NBSP_HIDDEN void nbsp_bh_bounds(double* x, double* y, double* z, const double* m, size_t n,
+                                double* partial, double* geometry, int* status, const double* ax,
+                                const double* ay, const double* az, int rms_of_a,
+                                const NbspLeapfrogFusion* leapfrog, cudaStream_t stream);
+/* geometry: root centre [0..2], half side [3], centre of mass [4..6], and with
+ * rms_of_a the rms |a| [7] of (ax, ay, az) (the relative test's floor); with a
+ * leapfrog fusion (NULL: none) the kick and drift come first and the rest is of
+ * the drifted positions */
 
 /* Morton keys, the identity index, the 8 digit histograms (into sort_scratch)
  * and the walk's float4 (x - c, y - c, z - c, m) with c the centre of mass, in
@@ -219,7 +233,9 @@ NBSP_HIDDEN const void* nbsp_bh_tree(const NbspBarnesHut* bh);
 /* a[i] = G * acc[i] (acc: double4 per particle in input order, as the walk
  * stores it) */
 NBSP_HIDDEN void nbsp_bh_unsort(const void* acc, size_t n, double gravitational_constant,
-                                double* ax, double* ay, double* az, cudaStream_t stream);
+                                double* ax, double* ay, double* az,
+                                const NbspLeapfrogFusion* leapfrog, cudaStream_t stream);
+/* (with a leapfrog fusion, NULL: none, v is then kicked by half_dt * a) */
 
 /* Copy node_count, leaf_count and depth of the tree to counters[2..4]. */
 NBSP_HIDDEN void nbsp_bh_tree_counts(const void* tree, size_t n, unsigned long long* counters,

@@ -157,8 +157,11 @@ static NBodySimProStatus ensure(NbspBarnesHut** handle, size_t n, NBodySimProErr
 static NBodySimProStatus morton(NbspBarnesHut* b, const NbspBarnesHutState* s, double tol_scale,
                                 int* status, cudaStream_t stream) {
     const int rel = tol_scale > 0.0;
+    const NbspLeapfrogFusion* lf = s->leapfrog.vx != NULL ? &s->leapfrog : NULL;
+    const int with_a = rel || lf != NULL;
     nbsp_bh_bounds(s->x, s->y, s->z, s->m, s->n, b->partial, b->geometry, status,
-                   rel ? s->ax : NULL, rel ? s->ay : NULL, rel ? s->az : NULL, stream);
+                   with_a ? s->ax : NULL, with_a ? s->ay : NULL, with_a ? s->az : NULL, rel, lf,
+                   stream);
     cudaEventRecord(b->events[1], stream);
     nbsp_bh_keys(s->x, s->y, s->z, s->m, s->n, b->geometry, b->keys, b->index, b->unsorted,
                  b->hist, s->ax, s->ay, s->az, tol_scale, rel ? b->tol_unsorted : NULL, stream);
@@ -212,7 +215,8 @@ NBodySimProStatus nbsp_bh_accelerations(NbspBarnesHut** handle, const NbspBarnes
         nbsp_bh_correct(b->pos4, n, b->tree, p->correction, &b->lists, b->index, b->acc,
                         b->counters, status, stream);
     cudaEventRecord(b->events[6], stream);
-    nbsp_bh_unsort(b->acc, n, p->gravitational_constant, s->ax, s->ay, s->az, stream);
+    nbsp_bh_unsort(b->acc, n, p->gravitational_constant, s->ax, s->ay, s->az,
+                   s->leapfrog.vx != NULL ? &s->leapfrog : NULL, stream);
     nbsp_bh_tree_counts(b->tree, n, b->counters, stream);
     cudaEventRecord(b->events[7], stream);
     BH_TRY(cudaGetLastError());
