@@ -743,9 +743,9 @@ def run_bh(args, wl, world, rank, local, steps, warmup, with_e2e=True):
                              f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz of {peak_kind} "
                              "MEASURED_PEAKS.json; it has no FP32 figure)",
                 "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None}
-    measured = PROFILED_TRAFFIC.get((args.workload, m["theta"], m["multipole_order"],
-                                     wl.get("walk", "lists"), m["leaf_capacity"],
-                                     m["relative_alpha"]))
+    measured = None if args.particles is not None else PROFILED_TRAFFIC.get(
+        (args.workload, m["theta"], m["multipole_order"], wl.get("walk", "lists"),
+         m["leaf_capacity"], m["relative_alpha"]))
     if measured is not None:
         roofline["traffic"] = measured[0]
         roofline["traffic_source"] = measured[1]
@@ -946,7 +946,8 @@ def run_allpairs(args, wl, world, rank, local, steps, warmup, with_e2e=True):
                              f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz of {peak_kind} "
                              "MEASURED_PEAKS.json; it has no FP32 figure)",
                 "flops_per_launch": flops, "launch_ms": round(kernel_ms, 4), "traffic": None}
-    measured = PROFILED_TRAFFIC.get((args.workload, None, 1, "lists", 16, 0.0))
+    measured = None if getattr(args, "particles", None) is not None else PROFILED_TRAFFIC.get(
+        (args.workload, None, 1, "lists", 16, 0.0))
     if measured is not None:
         roofline["traffic"] = measured[0]
         roofline["traffic_source"] = measured[1]
@@ -1218,6 +1219,7 @@ def secondary_record(args, name, world, rank, local):
     sub = argparse.Namespace(**vars(args))
     sub.workload = name
     sub.no_matched = True
+    sub.particles = None  # the sub-records run their own configurations' sizes
     t0 = time.time()
     r = run_workload(sub, name, wl, world, rank, local, wl["steps"], 3, with_e2e=False)
     rl = r["roofline"]
@@ -1303,11 +1305,18 @@ def main(argv=None):
     ap.add_argument("--leaf", type=int, default=None)
     ap.add_argument("--alpha", type=float, default=None,
                     help="relative opening test tolerance (with --no-matched)")
+    ap.add_argument("--particles", type=int, default=None,
+                    help="the workload's initial conditions at another particle count (with "
+                         "--no-matched; e.g. a smaller case of the same kernels for profiling)")
     args = ap.parse_args(argv)
     wl = dict(WORKLOADS[args.workload])
     for key in ("theta", "order", "walk", "leaf", "alpha"):
         if getattr(args, key) is not None:
             wl[key] = getattr(args, key)
+    if args.particles is not None:
+        if wl.get("n") is None or args.particles < 2:
+            ap.error("--particles needs a single-system workload and at least 2 particles")
+        wl["n"] = args.particles
     if args.steps is None:
         args.steps = wl["steps"]
     args.warmup = max(args.warmup, 3)
