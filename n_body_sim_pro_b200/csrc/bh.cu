@@ -554,7 +554,8 @@ struct Tree {
   float* shift;       // distance from the cell's geometric centre to its centre of mass
   float* kmass;       // M side^2: the relative opening test's cell term
   // what the interaction-list walk reads of a node, in one 32-byte record:
-  // (com xyz, mass), (ropen2, kmass, first particle, particle count as int bits)
+  // (com xyz, mass), (ropen2, kmass, first particle, count as int bits: the
+  // particle count of a bucket, minus the number of children of an internal node)
   float4* wnode;      // 2 per node
   unsigned long long* leaves;  // [1]
 };
@@ -1139,7 +1140,7 @@ __global__ void __launch_bounds__(256, QUAD ? 1 : 6) moments_kernel(const float4
         }
       }
       t.height[parent] = hmax + 1;
-      finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open, pinfo.z);
+      finish_node<QUAD>(t, parent, pm, pinfo.y, __ldcg(&t.level[parent]), open, -nc);
       parent = pinfo.w;
     }
   }
@@ -1950,7 +1951,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       const bool bad = valid && info.z > 0 && (info.y < 0 || info.y + info.z > n);
       if (bad) atomicOr(status, NBSP_DEVICE_ERROR_TREE_INCONSISTENT);
       const bool ok = valid && !bad;
-      bool all_accept = ok && info.z != 1, all_open = ok && info.z == 0;
+      bool all_accept = ok && info.z != 1, all_open = ok && info.z < 0;
 #pragma unroll
       for (int w = 0; w < kGroups; ++w) {
         if (!s_live[w]) continue;
@@ -2127,12 +2128,11 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       }
       const bool open = (test || opened) && !accept;
       is_leaf = is_leaf || (open && info.z > 0);  // a failing bucket is summed exactly
-      if (open && info.z == 0) {                   // an opened cell pushes its children
+      if (open && info.z < 0) {                    // an opened cell pushes its -info.z children
         ca = __ldg(reinterpret_cast<const int4*>(t.children) + 2 * node);
         cb = __ldg(reinterpret_cast<const int4*>(t.children) + 2 * node + 1);
+        kids = min(-info.z, 8);
       }
-      kids = (ca.x >= 0) + (ca.y >= 0) + (ca.z >= 0) + (ca.w >= 0) + (cb.x >= 0) + (cb.y >= 0) +
-             (cb.z >= 0) + (cb.w >= 0);
       unsigned m = __ballot_sync(kFull, is_leaf);
       if (is_leaf) leaves[nleaf + __popc(m & lt)] = make_int2(info.y, info.z);
       nleaf += __popc(m);
