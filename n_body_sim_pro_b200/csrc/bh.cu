@@ -2137,11 +2137,14 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       if (is_leaf) leaves[nleaf + __popc(m & lt)] = make_int2(info.y, info.z);
       nleaf += __popc(m);
       {  // targets whose own particle is in one of these buckets: one term fewer
+        // (only the group's own buckets overlap its targets: a vote first)
         const int lo = max(info.y - warp * 32, 0), hi = min(info.y + info.z - warp * 32, 32);
-        const unsigned span = hi >= 32 ? kFull : (1u << max(hi, 0)) - 1u;
-        const unsigned own = __reduce_or_sync(
-            kFull, is_leaf && hi > lo ? span & ~((1u << min(lo, 31)) - 1u) : 0u);
-        if (active && ((own >> lane) & 1u)) exact -= 1u;
+        if (__any_sync(kFull, is_leaf && hi > lo)) {
+          const unsigned span = hi >= 32 ? kFull : (1u << max(hi, 0)) - 1u;
+          const unsigned own = __reduce_or_sync(
+              kFull, is_leaf && hi > lo ? span & ~((1u << min(lo, 31)) - 1u) : 0u);
+          if (active && ((own >> lane) & 1u)) exact -= 1u;
+        }
       }
       m = __ballot_sync(kFull, accept);
       if (ORDER == 1) {
