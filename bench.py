@@ -134,7 +134,7 @@ PROFILED_TRAFFIC = {
         296_960, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
     # one-pass DRAM capture of the full 10M walk launch
     ("bh_matched_10m", 5.0, 1, "lists", 32, 0.0045): (
-        641_293_056, "profiles/bh_step_launches_relative_10m.md"),
+        622_074_624, "profiles/bh_step_launches_relative_10m.md"),
 }
 
 FP32_LANES_PER_SM = 128  # FFMA lanes per Blackwell SM
