@@ -129,7 +129,7 @@ DRIFT_STEPS = 10
 # capture of exactly this configuration (the file under profiles/ gives the command).
 PROFILED_TRAFFIC = {
     ("bh_collision_1m", 0.7, 1, "lists", 16, 0.0): (
-        30_559_232, "profiles/walk_lists_kernel_bh_collision_1m.md"),
+        31_626_240, "profiles/walk_lists_kernel_bh_collision_1m.md"),
     ("allpairs_plummer_16k", None, 1, "lists", 16, 0.0): (
         296_960, "profiles/allpairs_force_paired_kernel_plummer_16k.md"),
     # one-pass DRAM capture of the full 10M walk launch
