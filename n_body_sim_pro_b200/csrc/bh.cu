@@ -2013,7 +2013,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
         if (to_front) front[front0 + rf] = node;
         // cells every group accepts: into every live warp's source tile, in
         // rounds of what fits before the tiles are evaluated
-        approx += active ? (unsigned)na : 0u;
+        approx += (unsigned)na;
         for (int done = 0; done < na;) {
           const int put = min(kStage - staged, na - done);
           const int r = ra - done;
@@ -2063,7 +2063,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
   __syncwarp();
   // (staged > 0 with nothing left to walk: cells the shared phase staged; the
   // draining iteration evaluates them)
-  while (top > 0 || nleaf > 0 || staged > 0) {
+  for (;;) {  // until the stack, the bucket list and the tiles are drained
     if (top > 0) {
       if (++iters > total + 64) {  // every node is popped at most once
         if (lane == 0) atomicOr(status, NBSP_DEVICE_ERROR_WALK_LIMIT);
@@ -2178,7 +2178,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
         } else {
           staged += nacc;
         }
-        approx += active ? (unsigned)nacc : 0u;
+        approx += (unsigned)nacc;  // (warp-uniform; an idle lane's is dropped at the end)
       } else {  // a quadrupole cell goes into the QuadTile with its moments
         QuadTile& qt = s_quad[ORDER == 2 ? wib : 0];
         float4 qa = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -2198,7 +2198,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
         } else {
           qstaged += nacc;
         }
-        approx += active ? (unsigned)nacc : 0u;
+        approx += (unsigned)nacc;  // (warp-uniform; an idle lane's is dropped at the end)
       }
       int incl = kids;
       for (int off = 1; off < 32; off <<= 1) {
@@ -2277,6 +2277,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
       qstaged = 0;
     }
     __syncwarp();
+    if (drain) break;
   }
   if (CORR && lane == 0) {  // a group walked again keeps the plain monopole
     lists.count[warp] = overflow ? 0 : min(listed, lists.capacity);
@@ -2294,7 +2295,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_k
     a.lx = lx;
     a.ly = ly;
     a.lz = lz;
-    a.approx = approx;
+    a.approx = active ? approx : 0u;
     a.exact = exact;
   }
   store_walk(a, s, active, lane, perm, n, acc, counters);
