@@ -1796,6 +1796,9 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
+// the relative-test walk's stack: 896 ids per warp leave 24,064 B of shared
+// memory per block, so 9 blocks (at most 56 registers) fit an SM
+constexpr int kListStackRel = 896;
 // SHARED walk: the block's top-of-tree traversal keeps its stack and frontier
 // in the warps' stack space (it ends before any warp walks)
 constexpr int kCtaStack = 2048;    // warps 0 and 1's stacks
@@ -1842,7 +1845,7 @@ static_assert(kCtaStack + kFrontier <= 3 * kListStack, "frontier inside warp 2's
 // A block whose shared stack or frontier would overflow starts every group
 // from the root instead.
 template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED = false>
-__global__ void __launch_bounds__(kListThreads, ORDER == 1 ? 8 : 5) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, ORDER == 1 ? (STACK == kListStackRel ? 9 : 8) : 5) walk_lists_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
     const uint32_t* __restrict__ perm, double4* __restrict__ acc,
     unsigned long long* __restrict__ counters, int* status,
@@ -2525,7 +2528,8 @@ void launch_walk(const float4* p, const float* tol, size_t n, Tree t, int order,
       NBSP_COUNT_LAUNCH(1), walk_lists_kernel<2, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
           p, tol, (int)n, t, eps2, perm, out, counters, status, nullptr, none);
     } else {
-      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kListStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
+      constexpr int kStack = REL ? kListStackRel : kListStack;
+      NBSP_COUNT_LAUNCH(1), walk_lists_kernel<1, kStack, false, REL><<<blocks, kListThreads, 0, stream>>>(
           p, tol, (int)n, t, eps2, perm, out, counters, status, nullptr, none);
     }
     return;
