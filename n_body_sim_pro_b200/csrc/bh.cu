@@ -1796,9 +1796,15 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
-// the relative-test walk's stack: 896 ids per warp leave 24,064 B of shared
-// memory per block, so 9 blocks (at most 56 registers) fit an SM
+// the relative-test walk's stack: 896 ids per warp, so that its block (with
+// the tolerances' words, 23,040 B of shared memory) fits 9 times in an SM
 constexpr int kListStackRel = 896;
+// blocks per SM of the monopole list walks (at most 56 registers at 9): 9
+// where shared memory allows (the plain walk's block at 1024 ids is 24,576 B)
+template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED>
+constexpr int list_walk_blocks() {
+  return ORDER != 1 ? 5 : (!CORR && !SHARED && (REL ? STACK == kListStackRel : true)) ? 9 : 8;
+}
 // SHARED walk: the block's top-of-tree traversal keeps its stack and frontier
 // in the warps' stack space (it ends before any warp walks)
 constexpr int kCtaStack = 2048;    // warps 0 and 1's stacks
@@ -1845,7 +1851,7 @@ static_assert(kCtaStack + kFrontier <= 3 * kListStack, "frontier inside warp 2's
 // A block whose shared stack or frontier would overflow starts every group
 // from the root instead.
 template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED = false>
-__global__ void __launch_bounds__(kListThreads, ORDER == 1 ? (STACK == kListStackRel ? 9 : 8) : 5) walk_lists_kernel(
+__global__ void __launch_bounds__(kListThreads, (list_walk_blocks<ORDER, STACK, CORR, REL, SHARED>())) walk_lists_kernel(
     const float4* __restrict__ pos, const float* __restrict__ tol, int n, Tree t, float eps2,
     const uint32_t* __restrict__ perm, double4* __restrict__ acc,
     unsigned long long* __restrict__ counters, int* status,
@@ -1853,9 +1859,12 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? (STACK == kListStac
   static_assert(!SHARED || (ORDER == 1 && !CORR && STACK == kListStack), "shared top: monopole walk");
   __shared__ int s_stack[kListThreads / 32][STACK];
   __shared__ float s_probe_k[kListThreads / 32][REL ? 32 : 1];  // their M side^2
-  __shared__ float4 s_probe[kListThreads / 32][32];  // nodes awaiting per-target tests
+  // nodes awaiting per-target tests during a step; the same words hold the
+  // exclusive prefix of the bucket counts during a bucket flush (the two
+  // phases of an iteration never overlap: a __syncwarp ends each)
+  __shared__ float4 s_probe[kListThreads / 32][32];
+  static_assert(sizeof(s_probe[0]) >= kListCap * sizeof(int), "prefix fits the probe words");
   __shared__ int2 s_leaves[kListThreads / 32][kListCap];  // (first particle, count)
-  __shared__ int s_pref[kListThreads / 32][kListCap];     // exclusive prefix of the counts
   // ORDER 1: accepted cells are point masses in the source tile; ORDER 2:
   // cells fill a QuadTile
   static_assert(!(CORR && ORDER == 2), "the network corrects the monopole");
@@ -2227,7 +2236,7 @@ __global__ void __launch_bounds__(kListThreads, ORDER == 1 ? (STACK == kListStac
       // the bucket of its slot by binary search over the exclusive prefix of
       // the counts and loads its particles, all loads of a tile in flight at
       // once.  The target's own particle adds exactly 0 (d = 0).
-      int* pref = s_pref[wib];
+      int* pref = reinterpret_cast<int*>(s_probe[wib]);
       const int c0 = lane < nleaf ? leaves[lane].y : 0;
       const int c1 = lane + 32 < nleaf ? leaves[lane + 32].y : 0;
       int i0 = c0, i1 = c1;
