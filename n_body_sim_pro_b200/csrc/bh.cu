@@ -1800,10 +1800,11 @@ constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> sta
 // the tolerances' words, 23,040 B of shared memory) fits 9 times in an SM
 constexpr int kListStackRel = 896;
 // blocks per SM of the monopole list walks (at most 56 registers at 9): 9
-// where shared memory allows (the plain walk's block at 1024 ids is 24,576 B)
+// where shared memory allows (the plain and the corrected walk's block at
+// 1024 ids is 24,576 B)
 template <int ORDER, int STACK, bool CORR, bool REL, bool SHARED>
 constexpr int list_walk_blocks() {
-  return ORDER != 1 ? 5 : (!CORR && !SHARED && (REL ? STACK == kListStackRel : true)) ? 9 : 8;
+  return ORDER != 1 ? 5 : (!SHARED && (REL ? STACK == kListStackRel : true)) ? 9 : 8;
 }
 // SHARED walk: the block's top-of-tree traversal keeps its stack and frontier
 // in the warps' stack space (it ends before any warp walks)
