@@ -1796,9 +1796,9 @@ __device__ __forceinline__ int bucket_source(const int* pref, const int2* leaves
 constexpr int kListThreads = 128;  // 4 warps, one traversal group each
 constexpr int kListCap = 64;       // cells / leaves gathered before a flush (>= 32 + 32)
 constexpr int kListStack = 1024;   // node ids per warp (4 KiB); overflow -> stackless walk
-// the relative-test walk's stack: 896 ids per warp, so that its block (with
-// the tolerances' words, 23,040 B of shared memory) fits 9 times in an SM
-constexpr int kListStackRel = 896;
+// the relative-test walk's stack: 960 ids per warp, so that its block (with
+// the tolerances' words, 24,064 B of shared memory) fits 9 times in an SM
+constexpr int kListStackRel = 960;
 // blocks per SM of the monopole list walks (at most 56 registers at 9): 9
 // where shared memory allows (the plain and the corrected walk's block at
 // 1024 ids is 24,576 B)
